@@ -1,0 +1,287 @@
+"""Python host-side mirror of the reference's GridNode / Poisson call surface.
+
+Thin ctypes binding of lib/libamr_b200.so (include/amr_b200.h).  Method
+names follow the reference (grid/grid_node.h:46-80, poisson/poisson.h:44-69,
+euler/hydro_driver.h); every numerical call runs CUDA kernels in the library.
+There is no CPU fallback: when the library or a GPU is missing the
+constructor raises.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libamr_b200.so")
+
+PHYSICS_EULER = 0
+PHYSICS_EULER_GRAVITY = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+ERRORS = {
+    -1: "AMR_ERR_ARG", -2: "AMR_ERR_CUDA", -3: "AMR_ERR_RANGE", -4: "AMR_ERR_NOCONVERGE",
+    -5: "AMR_ERR_TIMEOUT", -6: "AMR_ERR_STATE", -7: "AMR_ERR_CAPACITY", -8: "AMR_ERR_NODEVICE",
+}
+
+
+class AmrConfig(ctypes.Structure):
+    _fields_ = [
+        ("bw", ctypes.c_int), ("nx", ctypes.c_int), ("nf", ctypes.c_int), ("physics", ctypes.c_int),
+        ("precision", ctypes.c_int), ("z_reflect", ctypes.c_int), ("mirror_refine_y", ctypes.c_int),
+        ("max_refine_level", ctypes.c_int), ("min_level", ctypes.c_int), ("min_grid_life", ctypes.c_int),
+        ("max_bricks", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("grid_dim", ctypes.c_double), ("origin", ctypes.c_double * 3), ("minmod_theta", ctypes.c_double),
+        ("cfl", ctypes.c_double), ("gamma", ctypes.c_double), ("rho_floor", ctypes.c_double),
+        ("ei_floor", ctypes.c_double), ("maxdtinc", ctypes.c_double), ("grav_g", ctypes.c_double),
+    ]
+
+
+class AmrError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERRORS.get(code, "AMR_ERR"), code, msg))
+        self.code = code
+
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    global _lib
+    if _lib is None:
+        if not os.path.exists(path):
+            raise ImportError("libamr_b200.so not built (run 3d-eulerian-amr_b200/build.py): %s" % path)
+        lib = ctypes.CDLL(path)
+        P, I, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        lib.amr_default_config.argtypes = [ctypes.POINTER(AmrConfig)]
+        lib.amr_create.argtypes = [ctypes.POINTER(AmrConfig), ctypes.POINTER(P)]
+        lib.amr_destroy.argtypes = [P]
+        lib.amr_last_error.argtypes = [P]
+        lib.amr_last_error.restype = ctypes.c_char_p
+        lib.amr_init_root.argtypes = [P]
+        lib.amr_load_tree.argtypes = [P, I, ip, ip, ip]
+        lib.amr_num_bricks.argtypes = [P]
+        lib.amr_get_tree.argtypes = [P, ip, ip, ip, ip, ip, ip, dp]
+        lib.amr_refine_from_flags.argtypes = [P, ctypes.POINTER(ctypes.c_ubyte), I, ip]
+        lib.amr_set_time.argtypes = [P, D]
+        lib.amr_get_time.argtypes = [P]
+        lib.amr_get_time.restype = D
+        lib.amr_zone_count.argtypes = [P]
+        lib.amr_zone_count.restype = ctypes.c_longlong
+        for name in ("amr_upload_state", "amr_download_state", "amr_upload_poisson", "amr_download_poisson",
+                     "amr_get_flow_off", "amr_set_flow_off"):
+            if hasattr(lib, name):
+                getattr(lib, name).argtypes = [P, dp]
+        for name in ("amr_synchronize", "amr_enforce_boundaries", "amr_store", "amr_restore",
+                     "amr_compute_fluxes", "amr_inject_from_children", "amr_poisson_set_source",
+                     "amr_poisson_boundaries", "amr_compute_forces", "amr_store_phi", "amr_restore_phi",
+                     "amr_restore_half_phi"):
+            if hasattr(lib, name):
+                getattr(lib, name).argtypes = [P]
+        lib.amr_add_difs.argtypes = [P, D, D]
+        lib.amr_max_dt.argtypes = [P, dp]
+        lib.amr_check_for_refine.argtypes = [P, D, I, ip]
+        lib.amr_state_max.argtypes = [P, I, dp]
+        lib.amr_sub_step.argtypes = [P, D, D]
+        lib.amr_hydro_step.argtypes = [P, D, D]
+        if hasattr(lib, "amr_vcycle"):
+            lib.amr_vcycle.argtypes = [P, dp]
+            lib.amr_poisson_solve.argtypes = [P, D, I, dp, ip]
+            lib.amr_grav_step.argtypes = [P, D, D, D, I]
+        _lib = lib
+    return _lib
+
+
+def default_config(**kw):
+    lib = load_library()
+    cfg = AmrConfig()
+    lib.amr_default_config(ctypes.byref(cfg))
+    for k, v in kw.items():
+        if k == "origin":
+            for d in range(3):
+                cfg.origin[d] = v[d]
+        else:
+            setattr(cfg, k, v)
+    return cfg
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _iptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+class AMR:
+    """One octree + device brick pool (amr_ctx)."""
+
+    def __init__(self, **cfg_kw):
+        self.lib = load_library()
+        self.cfg = default_config(**cfg_kw)
+        ptr = ctypes.c_void_p()
+        rc = self.lib.amr_create(ctypes.byref(self.cfg), ctypes.byref(ptr))
+        if rc != 0:
+            raise AmrError(rc, "amr_create failed (no GPU, or bad config)")
+        self.ctx = ptr
+        self.bw, self.nx, self.nf = self.cfg.bw, self.cfg.nx, self.cfg.nf
+        self.gnx = self.nx + 2 * self.bw
+        self.pnx = self.nx + 2
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.amr_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != 0:
+            raise AmrError(rc, self.lib.amr_last_error(self.ctx).decode(errors="replace"))
+        return rc
+
+    # ---- octree -----------------------------------------------------------
+    def init(self):
+        self._check(self.lib.amr_init_root(self.ctx))
+
+    def load_tree(self, level, loc, age=None):
+        level = np.ascontiguousarray(level, np.int32)
+        loc = np.ascontiguousarray(loc, np.int32).reshape(-1)
+        agep = _iptr(np.ascontiguousarray(age, np.int32)) if age is not None else None
+        if age is not None:
+            self._age_keep = np.ascontiguousarray(age, np.int32)
+            agep = _iptr(self._age_keep)
+        self._check(self.lib.amr_load_tree(self.ctx, len(level), _iptr(level), _iptr(loc), agep))
+
+    @property
+    def nbricks(self):
+        return self.lib.amr_num_bricks(self.ctx)
+
+    def get_tree(self):
+        n = self.nbricks
+        t = dict(level=np.zeros(n, np.int32), loc=np.zeros((n, 3), np.int32), offset=np.zeros((n, 3), np.int32),
+                 age=np.zeros(n, np.int32), child_mask=np.zeros(n, np.int32), refine_mask=np.zeros(n, np.int32),
+                 h=np.zeros(n, np.float64))
+        self._check(self.lib.amr_get_tree(self.ctx, _iptr(t["level"]), _iptr(t["loc"]), _iptr(t["offset"]),
+                                          _iptr(t["age"]), _iptr(t["child_mask"]), _iptr(t["refine_mask"]),
+                                          _dptr(t["h"])))
+        return t
+
+    def refine_from_flags(self, flags, clear=True):
+        f = np.ascontiguousarray(flags, np.uint8).reshape(-1)
+        ch = ctypes.c_int()
+        self._check(self.lib.amr_refine_from_flags(self.ctx, f.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)),
+                                                   int(clear), ctypes.byref(ch)))
+        return bool(ch.value)
+
+    def set_time(self, t):
+        self._check(self.lib.amr_set_time(self.ctx, float(t)))
+
+    def get_time(self):
+        return self.lib.amr_get_time(self.ctx)
+
+    def get_zone_cnt(self):
+        return self.lib.amr_zone_count(self.ctx)
+
+    # ---- state ------------------------------------------------------------
+    def upload_state(self, U):
+        U = np.ascontiguousarray(U, np.float64)
+        assert U.shape == (self.nbricks, self.nf, self.gnx, self.gnx, self.gnx), U.shape
+        self._check(self.lib.amr_upload_state(self.ctx, _dptr(U)))
+
+    def download_state(self):
+        U = np.zeros((self.nbricks, self.nf, self.gnx, self.gnx, self.gnx), np.float64)
+        self._check(self.lib.amr_download_state(self.ctx, _dptr(U)))
+        return U
+
+    def upload_poisson(self, P):
+        P = np.ascontiguousarray(P, np.float64)
+        assert P.shape == (8, self.nbricks, self.pnx, self.pnx, self.pnx), P.shape
+        self._check(self.lib.amr_upload_poisson(self.ctx, _dptr(P)))
+
+    def download_poisson(self):
+        P = np.zeros((8, self.nbricks, self.pnx, self.pnx, self.pnx), np.float64)
+        self._check(self.lib.amr_download_poisson(self.ctx, _dptr(P)))
+        return P
+
+    def flow_off(self):
+        fo = np.zeros(self.nf, np.float64)
+        self._check(self.lib.amr_get_flow_off(self.ctx, _dptr(fo)))
+        return fo
+
+    def set_flow_off(self, fo):
+        fo = np.ascontiguousarray(fo, np.float64)
+        self._check(self.lib.amr_set_flow_off(self.ctx, _dptr(fo)))
+
+    def synchronize(self):
+        self._check(self.lib.amr_synchronize(self.ctx))
+
+    # ---- GridNode call surface --------------------------------------------
+    def enforce_boundaries(self):
+        self._check(self.lib.amr_enforce_boundaries(self.ctx))
+
+    def store(self):
+        self._check(self.lib.amr_store(self.ctx))
+
+    def restore(self):
+        self._check(self.lib.amr_restore(self.ctx))
+
+    def compute_fluxes(self):
+        self._check(self.lib.amr_compute_fluxes(self.ctx))
+
+    def add_difs(self, dt, beta):
+        self._check(self.lib.amr_add_difs(self.ctx, float(dt), float(beta)))
+
+    def inject_from_children(self):
+        self._check(self.lib.amr_inject_from_children(self.ctx))
+
+    def max_dt(self):
+        v = ctypes.c_double()
+        self._check(self.lib.amr_max_dt(self.ctx, ctypes.byref(v)))
+        return v.value
+
+    def check_for_refine(self, min_refine_density, clear=True):
+        ch = ctypes.c_int()
+        self._check(self.lib.amr_check_for_refine(self.ctx, float(min_refine_density), int(clear), ctypes.byref(ch)))
+        return bool(ch.value)
+
+    def state_max(self, field=0):
+        v = ctypes.c_double()
+        self._check(self.lib.amr_state_max(self.ctx, int(field), ctypes.byref(v)))
+        return v.value
+
+    def sub_step(self, dt, beta):
+        self._check(self.lib.amr_sub_step(self.ctx, float(dt), float(beta)))
+
+    def hydro_step(self, dt, min_refine_density):
+        self._check(self.lib.amr_hydro_step(self.ctx, float(dt), float(min_refine_density)))
+
+    # ---- Poisson ------------------------------------------------------------
+    def vcycle(self):
+        v = ctypes.c_double()
+        self._check(self.lib.amr_vcycle(self.ctx, ctypes.byref(v)))
+        return v.value
+
+    def poisson_solve(self, tol, max_cycles=1000):
+        e = ctypes.c_double()
+        n = ctypes.c_int()
+        self._check(self.lib.amr_poisson_solve(self.ctx, float(tol), int(max_cycles), ctypes.byref(e),
+                                               ctypes.byref(n)))
+        return e.value, n.value
+
+    def compute_forces(self):
+        self._check(self.lib.amr_compute_forces(self.ctx))
+
+    def poisson_boundaries(self):
+        self._check(self.lib.amr_poisson_boundaries(self.ctx))
+
+    def grav_step(self, dt, tol, dynamic_range=1.0e6, step_index=0):
+        self._check(self.lib.amr_grav_step(self.ctx, float(dt), float(tol), float(dynamic_range),
+                                           int(step_index)))

@@ -1,0 +1,70 @@
+// Per-tree context: host octree, device brick pool and brick table.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "amr_internal.h"
+#include "octree.h"
+
+struct amr_ctx {
+    amr_config cfg{};
+    amr::Geom geom{};
+    amr::Octree tree;
+    std::string err;
+    double time = 0.0;
+    bool has_device = false;
+    cudaStream_t stream = nullptr;
+
+    // device pool
+    int cap = 0;
+    amr::DevState st{};
+    amr::BrickTable bt{};
+    double* d_fo = nullptr;      // FO[nf], FO0[nf] of the root
+    double* d_dt = nullptr;      // per-slot dt / scratch [cap]
+    double* d_red = nullptr;     // per-entry reduction scratch [cap]
+    unsigned char* d_flags = nullptr;  // [8*cap]
+    double* d_stage = nullptr;   // host<->device staging [stage_cap]
+    size_t stage_cap = 0;
+
+    // host mirror of the brick table
+    std::vector<int> h_level, h_off, h_ftype, h_fnbr, h_parent, h_cidx, h_child;
+    std::vector<double> h_h;
+    std::vector<int> free_slots;
+
+    // derived topology (rebuilt after every tree change)
+    std::vector<amr::Node*> order;              // DFS pre-order
+    std::vector<int> all_slots;                 // slots in DFS order
+    std::vector<std::vector<int>> level_slots;  // per level, DFS order
+    std::vector<std::vector<int>> parent_slots; // per level: bricks with >=1 child
+    std::vector<std::vector<amr::RefluxItem>> reflux;  // per coarse level
+    int* d_slots = nullptr;                     // all_slots | level lists | parent lists
+    std::vector<int> off_all, off_level, off_parent;
+    amr::RefluxItem* d_reflux = nullptr;
+    std::vector<int> off_reflux;
+    int d_slots_cap = 0, d_reflux_cap = 0;
+    std::vector<amr::Node*> pending_new;
+    int reflux_hazards = 0;
+
+    // Poisson
+    double* d_bphi = nullptr;   // [cap][6][pnx][pnx] domain-face potential tables
+    double* d_msrc = nullptr;   // [n][8][4] octant monopoles per DFS entry
+    int* d_allref = nullptr;    // [n] node fully covered by children
+    double* d_pres = nullptr;   // [cap] per-brick relax residual / L1 error
+    int* d_bfaces = nullptr;    // [nbf][2] (slot, face) of physical (non-mirror) faces
+    int* d_perr = nullptr;      // device error word (bad mirror index)
+    int n_bfaces = 0, msrc_cap = 0, bfaces_cap = 0;
+    std::vector<int> off_reflux_dir;  // [(maxl+1)*3+1] items sorted by (level, dir)
+    int vcycle_max_outer = 1000;
+    long long relax_calls = 0, relax_sweeps_total = 0;
+    bool topo_dirty = true;
+
+    amr_ctx(const amr::TreeParams& p) : tree(p) {}
+};
+
+namespace amr {
+int rebuild_topology(amr_ctx* c);
+int alloc_slot(amr_ctx* c);
+}  // namespace amr

@@ -1,0 +1,46 @@
+// Multigrid Poisson solver (poisson/poisson.cpp) on the device brick pool.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "amr_internal.h"
+
+struct amr_ctx;
+
+namespace amr {
+// New bricks: zero the Poisson arrays, then phi/phi0 piecewise constant from
+// the parent (Poisson::inject_from_parent, poisson.cpp:132-164).
+void launch_poisson_new_bricks(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                               cudaStream_t s);
+void launch_set_source(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);
+void launch_source_sums(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                        double* msrc, int* allref, cudaStream_t s);
+void launch_phys_bound(const Geom& g, const BrickTable& bt, const int* bfaces, int nbf, const int* order, int n,
+                       const double* msrc, const int* allref, double* bphi, cudaStream_t s);
+void launch_phi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,
+                           const int* slots, int n, cudaStream_t s);
+void launch_dphi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,
+                            const int* slots, int n, cudaStream_t s);
+void launch_phi_from_children(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                              cudaStream_t s);
+void launch_init_vcycle(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);
+void launch_vdown_a(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                    cudaStream_t s);
+void launch_adjust_dphi(const Geom& g, const BrickTable& bt, const DevState& st, const RefluxItem* items, int n,
+                        cudaStream_t s);
+void launch_vdown_c(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                    cudaStream_t s);
+int launch_relax(const Geom& g, const DevState& st, const int* slots, int n, double* out, int* sweeps,
+                 cudaStream_t s);
+void launch_coarse_correction(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                              cudaStream_t s);
+void launch_retire(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);
+void launch_forces(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                   cudaStream_t s);
+void launch_adjust_force(const Geom& g, const DevState& st, const RefluxItem* items, int n, cudaStream_t s);
+void launch_solution_error(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                           double* out, cudaStream_t s);
+void launch_phi_time(const Geom& g, const DevState& st, const int* slots, int n, int mode, cudaStream_t s);
+}  // namespace amr
+
+void amr_poisson_release(amr_ctx* c);

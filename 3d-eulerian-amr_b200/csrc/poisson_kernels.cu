@@ -1,0 +1,824 @@
+// Multigrid Poisson kernels, plain FP64 form (poisson/poisson.cpp and its
+// ghost proxies poisson_amr_bound.cpp / poisson_phys_bound.cpp).
+//
+// Poisson arrays live on the PNX^3 frame of every brick (PNX = nx + 2: the
+// interior plus one ghost layer); Poisson index p <-> grid index p + BW - 1.
+#include "context.h"
+#include "euler_state.cuh"
+#include "poisson.h"
+
+namespace amr {
+
+__device__ __forceinline__ int pidx(int pnx, int i, int j, int k) { return (k * pnx + j) * pnx + i; }
+
+// Grid::xf/yf/zf + h/2 (grid/grid.cpp:500-526) for grid index gi.
+__device__ __forceinline__ double cell_centre(const Geom& g, int axis, int off, double h, int gi) {
+    double f;
+    if (axis < 2) {
+        f = double(off + gi) * h - g.grid_dim - double(g.bw) * g.h0 - g.origin[axis];
+    } else if (g.z_reflect) {
+        f = double(off + gi) * h - double(g.bw) * g.h0 - g.origin[2];
+    } else {
+        f = double(off + gi) * h - g.grid_dim - double(g.bw) * g.h0;
+    }
+    return f + 0.5 * h;
+}
+
+// 1-D quadratic interpolation weights at +1/4 from the nodes -1, 0, +1;
+// their tensor product is the 27-point table of poisson_amr_bound.cpp:23-29
+// (every product is an exact dyadic double).
+__device__ __forceinline__ double w27(int l) { return l == 0 ? -0.09375 : (l == 1 ? 0.9375 : 0.15625); }
+
+// 4x4x4 restriction weights of poisson.cpp:12-15: 11 on the 2x2x2 core,
+// -1 where exactly one index is outside the core, 0 elsewhere.
+__device__ __forceinline__ double w64(int n, int o, int p) {
+    const int out = (n == 0 || n == 3) + (o == 0 || o == 3) + (p == 0 || p == 3);
+    return out == 0 ? 11.0 : (out == 1 ? -1.0 : 0.0);
+}
+
+// Array3d::divergence (array3d.h:139-150)
+__device__ __forceinline__ double divergence(const double* a, int pnx, int i, int j, int k) {
+    const int c = pidx(pnx, i, j, k);
+    return (a[c + 1] + a[c - 1] + a[c + pnx] + a[c - pnx] + a[c + pnx * pnx] + a[c - pnx * pnx]) - (a[c] * 6.0);
+}
+
+// Array3d::oct_avg (array3d.h:151-161)
+__device__ __forceinline__ double oct_avg(const double* a, int pnx, int i, int j, int k) {
+    const int c = pidx(pnx, i, j, k);
+    const int s = pnx * pnx;
+    return (a[c] + a[c + 1] + a[c + pnx] + a[c + pnx + 1] + a[c + s] + a[c + s + 1] + a[c + s + pnx] +
+            a[c + s + pnx + 1]) *
+           0.125;
+}
+
+// ---------------------------------------------------------------------------
+// sources and domain boundary
+// ---------------------------------------------------------------------------
+// Poisson::set_source (poisson.cpp:950-966): S = 4 pi G rho over PNX^3.
+__global__ void k_set_source(Geom g, DevState st, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx, gnx = g.gnx, off = g.bw - 1;
+    const double* R = st.U + (size_t)b * g.ucount;
+    double* S = st.S + (size_t)b * g.pnx3;
+    for (int t = threadIdx.x; t < g.pnx3; t += blockDim.x) {
+        const int i = t % pnx, j = (t / pnx) % pnx, k = t / (pnx * pnx);
+        const double rho = R[((k + off) * gnx + (j + off)) * gnx + (i + off)];
+        S[t] = 4.0 * M_PI * g.grav_g * rho;
+    }
+}
+
+// Octant monopoles of every brick (single/single.cpp:245-288, identical to
+// binary/binary.cpp:977-1019): per octant without a child, sums of S h^3 and
+// S x h^3 ... in the reference's cell order (k, j, i).  msrc[e][c] =
+// {src_0, src_x, src_y, src_z} for DFS entry e.
+__global__ void k_source_sums(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots,
+                              double* __restrict__ msrc, int* __restrict__ allref) {
+    const int e = blockIdx.x;
+    const int b = slots[e];
+    const int c = threadIdx.x;  // octant
+    const int pnx = g.pnx, half = (pnx - 2) / 2;
+    const double h = bt.h[b];
+    const double h3 = h * h * h;
+    __shared__ int uncovered;
+    if (c == 0) uncovered = 0;
+    __syncthreads();
+    double s0 = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+    if (c < 8 && bt.child[8 * b + c] < 0) {
+        atomicOr(&uncovered, 1);
+        const double* S = st.S + (size_t)b * g.pnx3;
+        const int ox = (c & 1) * half, oy = ((c >> 1) & 1) * half, oz = ((c >> 2) & 1) * half;
+        for (int k = 1 + oz; k <= half + oz; k++)
+            for (int j = 1 + oy; j <= half + oy; j++)
+                for (int i = 1 + ox; i <= half + ox; i++) {
+                    const double s = S[pidx(pnx, i, j, k)];
+                    s0 += s * h3;
+                    sx += s * cell_centre(g, 0, bt.off[3 * b + 0], h, i + g.bw - 1) * h3;
+                    sy += s * cell_centre(g, 1, bt.off[3 * b + 1], h, j + g.bw - 1) * h3;
+                    sz += s * cell_centre(g, 2, bt.off[3 * b + 2], h, k + g.bw - 1) * h3;
+                }
+    }
+    __syncthreads();
+    if (c < 8) {
+        const bool all_refined = uncovered == 0;
+        double* m = msrc + ((size_t)e * 8 + c) * 4;
+        if (!all_refined && s0 != 0.0) {
+            m[1] = sx / s0;
+            m[2] = sy / s0;
+            m[3] = sz / s0;
+            m[0] = s0 / (4.0 * M_PI);
+        } else {
+            m[0] = 0.0;
+            m[1] = m[2] = m[3] = 1.0;
+        }
+        if (c == 0) allref[e] = all_refined ? 1 : 0;
+    }
+}
+
+// Domain-face potential, PoissonPhysBound::compute_boundaries
+// (poisson_phys_bound.cpp:70-81) evaluating Single::compute_phi
+// (single/single.cpp:219-243): the recursive sum over all bricks of
+// -alpha m / r over their octant monopoles, with each brick's own sum formed
+// first and the children's sums added after it in child order.  One block per
+// boundary point: threads form the per-brick own sums of a chunk in parallel,
+// thread 0 accumulates them with the nesting of the recursion.
+__global__ void k_phys_bound(Geom g, BrickTable bt, const int* __restrict__ bfaces, const int* __restrict__ order,
+                             int n, const double* __restrict__ msrc, const int* __restrict__ allref,
+                             double* __restrict__ bphi) {
+    const int pnx = g.pnx;
+    const int fe = blockIdx.x / (pnx * pnx);
+    const int pt = blockIdx.x % (pnx * pnx);
+    const int b = bfaces[2 * fe], face = bfaces[2 * fe + 1];
+    const int a = pt / pnx, cc = pt % pnx;  // table[a][cc]: lower, higher transverse
+    const int ax = face >> 1;
+    int pi[3];
+    pi[ax] = (face & 1) ? pnx - 1 : 0;
+    pi[ax == 0 ? 1 : 0] = a;
+    pi[ax == 2 ? 1 : 2] = cc;
+    const double h = bt.h[b];
+    const double x = cell_centre(g, 0, bt.off[3 * b + 0], h, pi[0] + g.bw - 1);
+    const double y = cell_centre(g, 1, bt.off[3 * b + 1], h, pi[1] + g.bw - 1);
+    const double z = cell_centre(g, 2, bt.off[3 * b + 2], h, pi[2] + g.bw - 1);
+    const double alpha = g.z_reflect ? 2.0 : 1.0;
+    __shared__ double own[128];
+    __shared__ int lev[128];
+    double acc[16];
+    int depth = -1;
+    for (int base = 0; base < n; base += 128) {
+        const int e = base + threadIdx.x;
+        if (e < n) {
+            const double* m = msrc + (size_t)e * 32;
+            double sum = 0.0;
+            const bool ar = allref[e] != 0;
+            for (int q = 0; q < 8; q++) {
+                const double dx = x - m[4 * q + 1], dy = y - m[4 * q + 2], dz = z - m[4 * q + 3];
+                if (!ar) {
+                    sum -= alpha * m[4 * q + 0] / sqrt(dx * dx + dy * dy + dz * dz);
+                } else {
+                    sum = 0.0;
+                }
+            }
+            own[threadIdx.x] = sum;
+            lev[threadIdx.x] = bt.level[order[e]];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const int m = min(128, n - base);
+            for (int q = 0; q < m; q++) {
+                const int L = lev[q];
+                while (depth >= L) {
+                    acc[depth - 1] += acc[depth];
+                    depth--;
+                }
+                acc[L] = own[q];
+                depth = L;
+            }
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        while (depth > 0) {
+            acc[depth - 1] += acc[depth];
+            depth--;
+        }
+        bphi[((size_t)b * 6 + face) * pnx * pnx + a * pnx + cc] = acc[0];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// ghost values seen through a brick face: PoissonInterface::get_phi /
+// get_dphi of whatever sits there (a real brick, a PoissonAMRBound, a
+// PoissonPhysBound).
+// ---------------------------------------------------------------------------
+struct PoissonAux {
+    const double* bphi;  // [cap][6][pnx][pnx]
+    int* err;            // set when a mirrored ghost is asked for an index the reference aborts on
+};
+
+// PoissonAMRBound::get_phi (poisson_amr_bound.cpp:39-109).
+__device__ double amr_get_phi(const Geom& g, const BrickTable& bt, const DevState& st, int b, int face, int i, int j,
+                              int k) {
+    const int pnx = g.pnx;
+    const int p0 = bt.fnbr[6 * b + face];  // parent
+    const int ax = face >> 1;
+    const int v = (face & 1) ? 1 : -1;
+    int q[3] = {i, j, k}, par[3];
+    for (int d = 0; d < 3; d++) {
+        const int rel = bt.off[3 * b + d] + (d == ax ? v * (pnx - 2) : 0) - 2 * bt.off[3 * p0 + d] - (g.bw - 1);
+        const int t = rel + q[d];
+        par[d] = t % 2;
+        q[d] = t / 2;
+    }
+    int P = p0;
+    for (int d = 0; d < 3; d++) {
+        if (q[d] > pnx - 2) {
+            if (bt.ftype[6 * P + 2 * d + 1] != FACE_SIB) return 0.0;
+            P = bt.fnbr[6 * P + 2 * d + 1];
+            q[d] -= pnx - 2;
+        } else if (q[d] < 1) {
+            if (bt.ftype[6 * P + 2 * d] != FACE_SIB) return 0.0;
+            P = bt.fnbr[6 * P + 2 * d];
+            q[d] += pnx - 2;
+        }
+    }
+    const double* phi = st.phi + (size_t)P * g.pnx3;
+    double sum = 0.0;
+    for (int l = 0; l < 3; l++)
+        for (int n = 0; n < 3; n++)
+            for (int m = 0; m < 3; m++) {
+                const int i2 = q[0] + (l - 1) * (2 * par[0] - 1);
+                const int j2 = q[1] + (n - 1) * (2 * par[1] - 1);
+                const int k2 = q[2] + (m - 1) * (2 * par[2] - 1);
+                sum += (w27(l) * w27(n) * w27(m)) * phi[pidx(pnx, i2, j2, k2)];
+            }
+    return sum;
+}
+
+__device__ double get_phi_from(const Geom& g, const BrickTable& bt, const DevState& st, const PoissonAux& aux, int b,
+                               int face, int i, int j, int k) {
+    const int pnx = g.pnx;
+    const int kind = bt.ftype[6 * b + face];
+    if (kind == FACE_SIB) return st.phi[(size_t)bt.fnbr[6 * b + face] * g.pnx3 + pidx(pnx, i, j, k)];
+    if (kind == FACE_OUTFLOW) {
+        // PoissonPhysBound::get_phi (poisson_phys_bound.cpp:86-98): the face
+        // table indexed by the two transverse indices
+        const int ax = face >> 1;
+        const int idx[3] = {i, j, k};
+        const int a = idx[ax == 0 ? 1 : 0], c = idx[ax == 2 ? 1 : 2];
+        return aux.bphi[((size_t)b * 6 + face) * pnx * pnx + a * pnx + c];
+    }
+    if (kind == FACE_REFLECT) {
+        // mirrored plane z = 0 (poisson_phys_bound.cpp:99-126)
+        const double* phi = st.phi + (size_t)b * g.pnx3;
+        if (k == 1) return phi[pidx(pnx, i, j, pnx - 2)];
+        if (k == pnx - 2) return phi[pidx(pnx, i, j, 1)];
+        atomicExch(aux.err, 1);
+        return 0.0;
+    }
+    return amr_get_phi(g, bt, st, b, face, i, j, k);
+}
+
+// get_dphi: neighbour copy; PoissonAMRBound::get_dphi (poisson_amr_bound.cpp
+// :111-116) parent value without interpolation; 0 on a domain face; mirror.
+__device__ double get_dphi_from(const Geom& g, const BrickTable& bt, const DevState& st, const PoissonAux& aux, int b,
+                                int face, int i, int j, int k) {
+    const int pnx = g.pnx;
+    const int kind = bt.ftype[6 * b + face];
+    const int nbr = bt.fnbr[6 * b + face];
+    if (kind == FACE_SIB) return st.dphi[(size_t)nbr * g.pnx3 + pidx(pnx, i, j, k)];
+    if (kind == FACE_OUTFLOW) return 0.0;
+    if (kind == FACE_REFLECT) {
+        const double* d = st.dphi + (size_t)b * g.pnx3;
+        if (k == 1) return d[pidx(pnx, i, j, pnx - 2)];
+        if (k == pnx - 2) return d[pidx(pnx, i, j, 1)];
+        atomicExch(aux.err, 1);
+        return 0.0;
+    }
+    const int ax = face >> 1;
+    const int v = (face & 1) ? 1 : -1;
+    const int q[3] = {i, j, k};
+    int r[3];
+    for (int d = 0; d < 3; d++) {
+        const int rel = bt.off[3 * b + d] + (d == ax ? v * (pnx - 2) : 0) - 2 * bt.off[3 * nbr + d] - (g.bw - 1);
+        r[d] = (rel + q[d]) / 2;
+    }
+    return st.dphi[(size_t)nbr * g.pnx3 + pidx(pnx, r[0], r[1], r[2])];
+}
+
+// ---------------------------------------------------------------------------
+// ghost fills, Poisson::enforce_phi_boundaries (poisson.cpp:749-888) and
+// enforce_dphi_boundaries (poisson.cpp:890-929), one level at a time.
+// ---------------------------------------------------------------------------
+// faces: phi(0,j,k) = sib(XL).get_phi(PNX-2,j,k), phi(PNX-1,j,k) =
+// sib(XU).get_phi(1,j,k), ... over the transverse interior.
+__global__ void k_phi_faces(Geom g, BrickTable bt, DevState st, PoissonAux aux, const int* __restrict__ slots,
+                            int dphi_mode) {
+    const int b = slots[blockIdx.x];
+    const int face = blockIdx.y;
+    const int pnx = g.pnx, m = pnx - 2;
+    const int ax = face >> 1;
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+        const int t1 = t % m + 1, t2 = t / m + 1;
+        int dst[3], src[3];
+        dst[ax] = (face & 1) ? pnx - 1 : 0;
+        src[ax] = (face & 1) ? 1 : pnx - 2;
+        dst[ax == 0 ? 1 : 0] = src[ax == 0 ? 1 : 0] = t1;
+        dst[ax == 2 ? 1 : 2] = src[ax == 2 ? 1 : 2] = t2;
+        if (dphi_mode) {
+            const double v = get_dphi_from(g, bt, st, aux, b, face, src[0], src[1], src[2]);
+            st.dphi[(size_t)b * g.pnx3 + pidx(pnx, dst[0], dst[1], dst[2])] = v;
+        } else {
+            const double v = get_phi_from(g, bt, st, aux, b, face, src[0], src[1], src[2]);
+            st.phi[(size_t)b * g.pnx3 + pidx(pnx, dst[0], dst[1], dst[2])] = v;
+        }
+    }
+}
+
+// edges: Poisson::enforce_phi_boundaries_edge (poisson.cpp:788-842).
+__global__ void k_phi_edges(Geom g, BrickTable bt, DevState st, PoissonAux aux, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx, N = pnx - 1, M = pnx - 2;
+    const int k = threadIdx.x + 1;
+    if (k > M) return;
+    double* phi = st.phi + (size_t)b * g.pnx3;
+    auto phys = [&](int f) { const int t = bt.ftype[6 * b + f]; return t == FACE_OUTFLOW || t == FACE_REFLECT; };
+    auto gp = [&](int f, int i, int j, int kk) { return get_phi_from(g, bt, st, aux, b, f, i, j, kk); };
+    double v[12];
+    if (phys(XL) || phys(XU)) {
+        v[0] = gp(XL, M, 0, k);
+        v[1] = gp(XL, M, N, k);
+        v[2] = gp(XL, M, k, 0);
+        v[3] = gp(XL, M, k, N);
+        v[4] = gp(XU, 1, 0, k);
+        v[5] = gp(XU, 1, N, k);
+        v[6] = gp(XU, 1, k, 0);
+        v[7] = gp(XU, 1, k, N);
+    } else {
+        v[0] = gp(YL, 0, M, k);
+        v[4] = gp(YL, N, M, k);
+        v[1] = gp(YU, 0, 1, k);
+        v[5] = gp(YU, N, 1, k);
+        v[2] = gp(ZL, 0, k, M);
+        v[6] = gp(ZL, N, k, M);
+        v[3] = gp(ZU, 0, k, 1);
+        v[7] = gp(ZU, N, k, 1);
+    }
+    if (phys(YL) || phys(YU)) {
+        v[8] = gp(YL, k, M, 0);
+        v[9] = gp(YL, k, M, N);
+        v[10] = gp(YU, k, 1, 0);
+        v[11] = gp(YU, k, 1, N);
+    } else {
+        v[8] = gp(ZL, k, 0, M);
+        v[10] = gp(ZL, k, N, M);
+        v[9] = gp(ZU, k, 0, 1);
+        v[11] = gp(ZU, k, N, 1);
+    }
+    // edges read face ghosts only (this level's faces are complete)
+    phi[pidx(pnx, 0, 0, k)] = v[0];
+    phi[pidx(pnx, 0, N, k)] = v[1];
+    phi[pidx(pnx, 0, k, 0)] = v[2];
+    phi[pidx(pnx, 0, k, N)] = v[3];
+    phi[pidx(pnx, N, 0, k)] = v[4];
+    phi[pidx(pnx, N, N, k)] = v[5];
+    phi[pidx(pnx, N, k, 0)] = v[6];
+    phi[pidx(pnx, N, k, N)] = v[7];
+    phi[pidx(pnx, k, 0, 0)] = v[8];
+    phi[pidx(pnx, k, 0, N)] = v[9];
+    phi[pidx(pnx, k, N, 0)] = v[10];
+    phi[pidx(pnx, k, N, N)] = v[11];
+}
+
+// vertices: Poisson::enforce_phi_boundaries_vertex (poisson.cpp:844-888).
+__global__ void k_phi_vertices(Geom g, BrickTable bt, DevState st, PoissonAux aux, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx, N = pnx - 1, M = pnx - 2;
+    double* phi = st.phi + (size_t)b * g.pnx3;
+    auto phys = [&](int f) { const int t = bt.ftype[6 * b + f]; return t == FACE_OUTFLOW || t == FACE_REFLECT; };
+    auto gp = [&](int f, int i, int j, int kk) { return get_phi_from(g, bt, st, aux, b, f, i, j, kk); };
+    if (threadIdx.x != 0) return;
+    double v[8];  // index = x | y<<1 | z<<2 of the corner
+    if (phys(XL) || phys(XU)) {
+        v[0] = gp(XL, M, 0, 0);
+        v[2] = gp(XL, M, N, 0);
+        v[4] = gp(XL, M, 0, N);
+        v[6] = gp(XL, M, N, N);
+        v[1] = gp(XU, 1, 0, 0);
+        v[3] = gp(XU, 1, N, 0);
+        v[5] = gp(XU, 1, 0, N);
+        v[7] = gp(XU, 1, N, N);
+    } else if (phys(YL) || phys(YU)) {
+        v[0] = gp(YL, 0, M, 0);
+        v[1] = gp(YL, N, M, 0);
+        v[4] = gp(YL, 0, M, N);
+        v[5] = gp(YL, N, M, N);
+        v[2] = gp(YU, 0, 1, 0);
+        v[3] = gp(YU, N, 1, 0);
+        v[6] = gp(YU, 0, 1, N);
+        v[7] = gp(YU, N, 1, N);
+    } else {
+        v[0] = gp(ZL, 0, 0, M);
+        v[2] = gp(ZL, 0, N, M);
+        v[1] = gp(ZL, N, 0, M);
+        v[3] = gp(ZL, N, N, M);
+        v[4] = gp(ZU, 0, 0, 1);
+        v[6] = gp(ZU, 0, N, 1);
+        v[5] = gp(ZU, N, 0, 1);
+        v[7] = gp(ZU, N, N, 1);
+    }
+    for (int c = 0; c < 8; c++) phi[pidx(pnx, (c & 1) * N, ((c >> 1) & 1) * N, ((c >> 2) & 1) * N)] = v[c];
+}
+
+// ---------------------------------------------------------------------------
+// V-cycle pieces
+// ---------------------------------------------------------------------------
+// Poisson::phi_from_children (poisson.cpp:707-747): covered coarse phi :=
+// 64-point weighted child stencil / 64.  grid = (parents, 8 children).
+__global__ void k_phi_from_children(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
+    const int p = slots[blockIdx.x];
+    const int c = blockIdx.y;
+    const int ch = bt.child[8 * p + c];
+    if (ch < 0) return;
+    const int pnx = g.pnx, half = (pnx - 2) / 2;
+    const int t = threadIdx.x;
+    if (t >= half * half * half) return;
+    const int a = t % half, bb = (t / half) % half, cc = t / (half * half);
+    const int i = 2 * a + 1, j = 2 * bb + 1, k = 2 * cc + 1;
+    const int i0 = a + 1 + (c & 1) * half, j0 = bb + 1 + ((c >> 1) & 1) * half, k0 = cc + 1 + ((c >> 2) & 1) * half;
+    const double* C = st.phi + (size_t)ch * g.pnx3;
+    double sum = 0.0;
+    for (int n = -1; n < 3; n++)
+        for (int o = -1; o < 3; o++)
+            for (int q = -1; q < 3; q++) sum += w64(n + 1, o + 1, q + 1) * C[pidx(pnx, i + q, j + o, k + n)];
+    st.phi[(size_t)p * g.pnx3 + pidx(pnx, i0, j0, k0)] = sum / 64.0;
+}
+
+// Poisson::init_vcycle (poisson.cpp:931-948)
+__global__ void k_init_vcycle(Geom g, DevState st, const int* __restrict__ slots) {
+    const size_t base = (size_t)slots[blockIdx.x] * g.pnx3;
+    for (int t = threadIdx.x; t < g.pnx3; t += blockDim.x) {
+        st.dphi[base + t] = 0.0;
+        st.dphi1[base + t] = 0.0;
+    }
+}
+
+// Poisson::vcycle_down first part (poisson.cpp:989-1017): residual/6 on
+// uncovered cells, child averages of dphi and dphi1 on covered ones.
+__global__ void k_vdown_a(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx, nx = pnx - 2, half = nx / 2;
+    const double h = bt.h[b];
+    const double h2 = h * h;
+    const size_t base = (size_t)b * g.pnx3;
+    for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
+        const int i = t % nx + 1, j = (t / nx) % nx + 1, k = t / (nx * nx) + 1;
+        const int oc = ((i - 1) / half) | (((j - 1) / half) << 1) | (((k - 1) / half) << 2);
+        const int ch = bt.child[8 * b + oc];
+        const int c = pidx(pnx, i, j, k);
+        if (ch < 0) {
+            st.dphi[base + c] = (divergence(st.phi + base, pnx, i, j, k) - h2 * st.S[base + c]) * (1.0 / 6.0);
+        } else {
+            const int ci = 2 * (i - (oc & 1) * half) - 1;
+            const int cj = 2 * (j - ((oc >> 1) & 1) * half) - 1;
+            const int ck = 2 * (k - ((oc >> 2) & 1) * half) - 1;
+            const size_t cb = (size_t)ch * g.pnx3;
+            st.dphi1[base + c] = oct_avg(st.dphi1 + cb, pnx, ci, cj, ck);
+            st.dphi[base + c] = oct_avg(st.dphi + cb, pnx, ci, cj, ck);
+        }
+    }
+}
+
+// Poisson::adjust_{x,y,z}_dphi (poisson.cpp:249-443): coarse-fine
+// correction of dphi on uncovered cells next to a face refined on one side.
+// The items are the coarse-fine flux items of the hydro in the PNX frame.
+__global__ void k_adjust_dphi(Geom g, BrickTable bt, DevState st, const RefluxItem* __restrict__ items) {
+    const RefluxItem it = items[blockIdx.x];
+    const int pnx = g.pnx, half = (pnx - 2) / 2;
+    const int t = threadIdx.x;
+    if (t >= half * half) return;
+    const int a = t % half, cc = t / half;
+    const int j = 2 * a + 1, k = 2 * cc + 1;                          // child transverse (lower, higher)
+    const int j0 = a + 1 + it.cj * half, k0 = cc + 1 + it.ck * half;  // coarse transverse
+    const int i = it.ic - g.bw + 1, i0 = it.i0 - g.bw + 1;            // PNX frame
+    const int d = it.dir;
+    auto at = [&](int nrm, int t1, int t2) {
+        int q[3];
+        q[d] = nrm;
+        q[d == 0 ? 1 : 0] = t1;
+        q[d == 2 ? 1 : 2] = t2;
+        return pidx(pnx, q[0], q[1], q[2]);
+    };
+    const double* C = st.phi + (size_t)it.child * g.pnx3;
+    const size_t pb = (size_t)it.coarse * g.pnx3;
+    const double* P = st.phi + pb;
+    double v = +C[at(i, j, k)] - C[at(i - 1, j, k)];
+    v += C[at(i, j + 1, k)] - C[at(i - 1, j + 1, k)];
+    v += C[at(i, j, k + 1)] - C[at(i - 1, j, k + 1)];
+    v += C[at(i, j + 1, k + 1)] - C[at(i - 1, j + 1, k + 1)];
+    v *= 0.5;
+    const double dd = (P[at(i0, j0, k0)] - P[at(i0 - 1, j0, k0)] - v) * (1.0 / 6.0);
+    auto refined = [&](int cell) {
+        const int ci = cell % pnx, cj = (cell / pnx) % pnx, ck = cell / (pnx * pnx);
+        const int oc = (2 * ci / pnx) | ((2 * cj / pnx) << 1) | ((2 * ck / pnx) << 2);
+        return bt.child[8 * it.coarse + oc] >= 0;
+    };
+    const int c1 = at(i0, j0, k0), c0 = at(i0 - 1, j0, k0);
+    if (!refined(c1)) st.dphi[pb + c1] += dd;
+    if (!refined(c0)) st.dphi[pb + c0] -= dd;
+}
+
+// Poisson::vcycle_down last part (poisson.cpp:1021-1040): dphi1 = dphi on
+// uncovered cells.
+__global__ void k_vdown_c(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx, nx = pnx - 2, half = nx / 2;
+    const size_t base = (size_t)b * g.pnx3;
+    for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
+        const int i = t % nx + 1, j = (t / nx) % nx + 1, k = t / (nx * nx) + 1;
+        const int oc = ((i - 1) / half) | (((j - 1) / half) << 1) | (((k - 1) / half) << 2);
+        if (bt.child[8 * b + oc] < 0) st.dphi1[base + pidx(pnx, i, j, k)] = st.dphi[base + pidx(pnx, i, j, k)];
+    }
+}
+
+// Poisson::vcycle_relax (poisson.cpp:88-130): Jacobi sweeps on one brick
+// with its ghost dphi frozen, until the sweep's sum of squared updates drops
+// below half the first sweep's or 16 sweeps.  Block = one brick, thread per
+// interior cell, dphi staged in shared memory.  out[e] = last sweep's sum.
+template <int NX>
+__global__ void __launch_bounds__(NX* NX* NX) k_relax(Geom g, DevState st, const int* __restrict__ slots,
+                                                      double* __restrict__ out, int* __restrict__ sweeps_out) {
+    constexpr int P = NX + 2, P3 = P * P * P, NT = NX * NX * NX, NW = NT / 32;
+    __shared__ double d[P3];
+    __shared__ double red[NW];
+    __shared__ double total;
+    const int b = slots[blockIdx.x];
+    const size_t base = (size_t)b * P3;
+    for (int t = threadIdx.x; t < P3; t += NT) d[t] = st.dphi[base + t];
+    const int t = threadIdx.x;
+    const int i = t % NX + 1, j = (t / NX) % NX + 1, k = t / (NX * NX) + 1;
+    const int c = (k * P + j) * P + i;
+    const double d1 = st.dphi1[base + c];
+    __syncthreads();
+    double resid0 = 0.0, resid = 0.0;
+    int iters = 0;
+    bool first = true;
+    do {
+        const double div = (d[c + 1] + d[c - 1] + d[c + P] + d[c - P] + d[c + P * P] + d[c - P * P]) - (d[c] * 6.0);
+        const double tmp0 = d1 + div * (1.0 / 6.0);
+        __syncthreads();
+        d[c] += tmp0;
+        double sq = tmp0 * tmp0;
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        if ((t & 31) == 0) red[t >> 5] = sq;
+        __syncthreads();
+        if (t == 0) {
+            double s = 0.0;
+            for (int w = 0; w < NW; w++) s += red[w];
+            total = s;
+        }
+        __syncthreads();
+        resid = total;
+        if (first) {
+            resid0 = resid;
+            first = false;
+        }
+        iters++;
+    } while (resid / resid0 > 0.5 && iters < 16);
+    st.dphi[base + c] = d[c];
+    if (t == 0) {
+        out[b] = resid;
+        if (sweeps_out) atomicAdd(sweeps_out, iters);
+    }
+}
+
+// Poisson::vcycle_coarse_correction (poisson.cpp:17-51): child dphi +=
+// parent dphi - mean of the child's 2x2x2 group.
+__global__ void k_coarse_correction(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int p = bt.parent[b];
+    if (p < 0) return;
+    const int c = bt.cidx[b];
+    const int pnx = g.pnx, half = (pnx - 2) / 2;
+    const int t = threadIdx.x;
+    if (t >= half * half * half) return;
+    const int a = t % half, bb = (t / half) % half, cc = t / (half * half);
+    const int i = 2 * a + 1, j = 2 * bb + 1, k = 2 * cc + 1;
+    const int i0 = a + 1 + (c & 1) * half, j0 = bb + 1 + ((c >> 1) & 1) * half, k0 = cc + 1 + ((c >> 2) & 1) * half;
+    double* D = st.dphi + (size_t)b * g.pnx3;
+    const double av = st.dphi[(size_t)p * g.pnx3 + pidx(pnx, i0, j0, k0)] - oct_avg(D, pnx, i, j, k);
+    for (int o = 0; o < 8; o++) D[pidx(pnx, i + (o & 1), j + ((o >> 1) & 1), k + ((o >> 2) & 1))] += av;
+}
+
+// Poisson::vcycle_retire_dphi (poisson.cpp:1048-1067): phi += dphi.
+__global__ void k_retire(Geom g, DevState st, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx, nx = pnx - 2;
+    const size_t base = (size_t)b * g.pnx3;
+    for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
+        const int c = pidx(pnx, t % nx + 1, (t / nx) % nx + 1, t / (nx * nx) + 1);
+        st.phi[base + c] += st.dphi[base + c];
+    }
+}
+
+// Poisson::compute_forces (poisson.cpp:223-247): face forces -grad phi for
+// faces 1..PNX-1 on rows 1..PNX-1.
+__global__ void k_forces(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx, m = pnx - 1;
+    const double h = bt.h[b];
+    const size_t base = (size_t)b * g.pnx3;
+    const double* phi = st.phi + base;
+    for (int t = threadIdx.x; t < m * m * m; t += blockDim.x) {
+        const int i = t % m + 1, j = (t / m) % m + 1, k = t / (m * m) + 1;
+        const int c = pidx(pnx, i, j, k);
+        st.fx[base + c] = -(phi[c] - phi[c - 1]) / h;
+        st.fy[base + c] = -(phi[c] - phi[c - pnx]) / h;
+        st.fz[base + c] = -(phi[c] - phi[c - pnx * pnx]) / h;
+    }
+}
+
+// Poisson::adjust_{x,y,z}_force (poisson.cpp:445-635): coarse face force :=
+// mean of the child's four face forces.
+__global__ void k_adjust_force(Geom g, DevState st, const RefluxItem* __restrict__ items) {
+    const RefluxItem it = items[blockIdx.x];
+    const int pnx = g.pnx, half = (pnx - 2) / 2;
+    const int t = threadIdx.x;
+    if (t >= half * half) return;
+    const int a = t % half, cc = t / half;
+    const int j = 2 * a + 1, k = 2 * cc + 1;
+    const int j0 = a + 1 + it.cj * half, k0 = cc + 1 + it.ck * half;
+    const int i = it.ic - g.bw + 1, i0 = it.i0 - g.bw + 1;
+    const int d = it.dir;
+    auto at = [&](int nrm, int t1, int t2) {
+        int q[3];
+        q[d] = nrm;
+        q[d == 0 ? 1 : 0] = t1;
+        q[d == 2 ? 1 : 2] = t2;
+        return pidx(pnx, q[0], q[1], q[2]);
+    };
+    double* f = d == 0 ? st.fx : (d == 1 ? st.fy : st.fz);
+    const double* C = f + (size_t)it.child * g.pnx3;
+    double v = +C[at(i, j, k)];
+    v += C[at(i, j + 1, k)];
+    v += C[at(i, j, k + 1)];
+    v += C[at(i, j + 1, k + 1)];
+    f[(size_t)it.coarse * g.pnx3 + at(i0, j0, k0)] = v * 0.25;
+}
+
+// Poisson::solution_error (poisson.cpp:637-669): dphi := div f - S on
+// uncovered cells (0 on covered), per-brick sum of |dphi| h^3.
+__global__ void k_solution_error(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots,
+                                 double* __restrict__ out) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx, nx = pnx - 2, half = nx / 2;
+    const double h = bt.h[b];
+    const double h3 = h * h * h, hinv = 1.0 / h;
+    const size_t base = (size_t)b * g.pnx3;
+    __shared__ double red[32];
+    double sum = 0.0;
+    for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
+        const int i = t % nx + 1, j = (t / nx) % nx + 1, k = t / (nx * nx) + 1;
+        const int c = pidx(pnx, i, j, k);
+        const int oc = ((i - 1) / half) | (((j - 1) / half) << 1) | (((k - 1) / half) << 2);
+        if (bt.child[8 * b + oc] < 0) {
+            double df = -(st.fx[base + c + 1] - st.fx[base + c]) * hinv;
+            df -= (st.fy[base + c + pnx] - st.fy[base + c]) * hinv;
+            df -= (st.fz[base + c + pnx * pnx] - st.fz[base + c]) * hinv;
+            const double r = df - st.S[base + c];
+            st.dphi[base + c] = r;
+            sum += fabs(r) * h3;
+        } else {
+            st.dphi[base + c] = 0.0;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];
+        out[b] = s;
+    }
+}
+
+// Poisson::store_phi / restore_phi / restore_half_phi (poisson.cpp:166-221).
+__global__ void k_phi_time(Geom g, DevState st, const int* __restrict__ slots, int mode) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx, nx = pnx - 2;
+    const size_t base = (size_t)b * g.pnx3;
+    for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
+        const size_t c = base + pidx(pnx, t % nx + 1, (t / nx) % nx + 1, t / (nx * nx) + 1);
+        if (mode == 0) {
+            st.phi0[c] = st.phi[c];
+        } else if (mode == 1) {
+            st.phi[c] = st.phi0[c];
+        } else {
+            const double r = st.phi[c];
+            st.phi[c] = (st.phi[c] + st.phi0[c]) * 0.5;
+            st.phi0[c] = r;
+        }
+    }
+}
+
+// Poisson::Poisson() zeroes phi, dphi1, dphi, phi0 (poisson.cpp:671-685);
+// S and the forces are zeroed here too.  Then Poisson::inject_from_parent
+// (poisson.cpp:132-164): phi = phi0 = parent phi, piecewise constant.
+__global__ void k_poisson_new(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int pnx = g.pnx;
+    const size_t base = (size_t)b * g.pnx3;
+    for (int t = threadIdx.x; t < g.pnx3; t += blockDim.x) {
+        st.phi[base + t] = 0.0;
+        st.phi0[base + t] = 0.0;
+        st.dphi[base + t] = 0.0;
+        st.dphi1[base + t] = 0.0;
+        st.S[base + t] = 0.0;
+        st.fx[base + t] = 0.0;
+        st.fy[base + t] = 0.0;
+        st.fz[base + t] = 0.0;
+    }
+    __syncthreads();
+    const int p = bt.parent[b];
+    if (p < 0) return;
+    const int c = bt.cidx[b];
+    const int nx = pnx - 2, half = nx / 2;
+    const size_t pbase = (size_t)p * g.pnx3;
+    for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
+        const int i = t % nx + 1, j = (t / nx) % nx + 1, k = t / (nx * nx) + 1;
+        const int i0 = (i + 1) / 2 + (c & 1) * half;
+        const int j0 = (j + 1) / 2 + ((c >> 1) & 1) * half;
+        const int k0 = (k + 1) / 2 + ((c >> 2) & 1) * half;
+        const double u = st.phi[pbase + pidx(pnx, i0, j0, k0)];
+        st.phi[base + pidx(pnx, i, j, k)] = u;
+        st.phi0[base + pidx(pnx, i, j, k)] = u;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch wrappers
+// ---------------------------------------------------------------------------
+void launch_poisson_new_bricks(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                               cudaStream_t s) {
+    if (n <= 0) return;
+    k_poisson_new<<<n, 256, 0, s>>>(g, bt, st, slots);
+}
+
+}  // namespace amr
+
+namespace amr {
+
+void launch_set_source(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
+    if (n > 0) k_set_source<<<n, 256, 0, s>>>(g, st, slots);
+}
+void launch_source_sums(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                        double* msrc, int* allref, cudaStream_t s) {
+    if (n > 0) k_source_sums<<<n, 32, 0, s>>>(g, bt, st, slots, msrc, allref);
+}
+void launch_phys_bound(const Geom& g, const BrickTable& bt, const int* bfaces, int nbf, const int* order, int n,
+                       const double* msrc, const int* allref, double* bphi, cudaStream_t s) {
+    if (nbf > 0) k_phys_bound<<<nbf * g.pnx * g.pnx, 128, 0, s>>>(g, bt, bfaces, order, n, msrc, allref, bphi);
+}
+void launch_phi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,
+                           const int* slots, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    PoissonAux aux{bphi, err};
+    k_phi_faces<<<dim3(n, 6), 64, 0, s>>>(g, bt, st, aux, slots, 0);
+    k_phi_edges<<<n, g.pnx - 2, 0, s>>>(g, bt, st, aux, slots);
+    k_phi_vertices<<<n, 32, 0, s>>>(g, bt, st, aux, slots);
+}
+void launch_dphi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,
+                            const int* slots, int n, cudaStream_t s) {
+    if (n <= 0) return;
+    PoissonAux aux{bphi, err};
+    k_phi_faces<<<dim3(n, 6), 64, 0, s>>>(g, bt, st, aux, slots, 1);
+}
+void launch_phi_from_children(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                              cudaStream_t s) {
+    const int half = (g.pnx - 2) / 2;
+    if (n > 0) k_phi_from_children<<<dim3(n, 8), ((half * half * half + 31) / 32) * 32, 0, s>>>(g, bt, st, slots);
+}
+void launch_init_vcycle(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
+    if (n > 0) k_init_vcycle<<<n, 256, 0, s>>>(g, st, slots);
+}
+void launch_vdown_a(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                    cudaStream_t s) {
+    if (n > 0) k_vdown_a<<<n, 256, 0, s>>>(g, bt, st, slots);
+}
+void launch_adjust_dphi(const Geom& g, const BrickTable& bt, const DevState& st, const RefluxItem* items, int n,
+                        cudaStream_t s) {
+    if (n > 0) k_adjust_dphi<<<n, 32, 0, s>>>(g, bt, st, items);
+}
+void launch_vdown_c(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                    cudaStream_t s) {
+    if (n > 0) k_vdown_c<<<n, 256, 0, s>>>(g, bt, st, slots);
+}
+int launch_relax(const Geom& g, const DevState& st, const int* slots, int n, double* out, int* sweeps,
+                 cudaStream_t s) {
+    if (n <= 0) return 0;
+    if (g.nx != 8) return -1;
+    k_relax<8><<<n, 512, 0, s>>>(g, st, slots, out, sweeps);
+    return 0;
+}
+void launch_coarse_correction(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                              cudaStream_t s) {
+    const int half = (g.pnx - 2) / 2;
+    if (n > 0) k_coarse_correction<<<n, ((half * half * half + 31) / 32) * 32, 0, s>>>(g, bt, st, slots);
+}
+void launch_retire(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
+    if (n > 0) k_retire<<<n, 256, 0, s>>>(g, st, slots);
+}
+void launch_forces(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                   cudaStream_t s) {
+    if (n > 0) k_forces<<<n, 256, 0, s>>>(g, bt, st, slots);
+}
+void launch_adjust_force(const Geom& g, const DevState& st, const RefluxItem* items, int n, cudaStream_t s) {
+    if (n > 0) k_adjust_force<<<n, 32, 0, s>>>(g, st, items);
+}
+void launch_solution_error(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                           double* out, cudaStream_t s) {
+    if (n > 0) k_solution_error<<<n, 256, 0, s>>>(g, bt, st, slots, out);
+}
+void launch_phi_time(const Geom& g, const DevState& st, const int* slots, int n, int mode, cudaStream_t s) {
+    if (n > 0) k_phi_time<<<n, 256, 0, s>>>(g, st, slots, mode);
+}
+
+}  // namespace amr

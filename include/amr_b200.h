@@ -1,0 +1,161 @@
+/*
+ * amr_b200.h -- C ABI of the B200 octree-AMR hydro + gravity step.
+ *
+ * This is the drop-in boundary for the per-step hot path of
+ * STEllAR-GROUP/3d-eulerian-amr.  The reference has no FFI: its operator API
+ * is the C++ virtual call surface of the root octree node (GridNode,
+ * grid/grid_node.h:46-80; Grid, grid/grid.h:81-97; Poisson,
+ * poisson/poisson.h:44-69) driven by HydroDriver / BinaryDriver.  Each entry
+ * point below replaces one of those calls on the whole tree (the reference
+ * methods recurse from the root; these act on every brick of the tree).
+ *
+ * Conventions
+ *  - Every call returns int status: AMR_OK (0) or a negative AMR_ERR_*; the
+ *    reference printf()+abort()s instead (helmholtz/helmeos.cpp:216-221,
+ *    binary/binary_driver.cpp:320-324).  amr_last_error() gives the message.
+ *  - The library owns all device memory.  Host arrays are plain pointers.
+ *  - Bricks are addressed in depth-first pre-order (node, then children
+ *    0..7 with ChildIndex = x | y<<1 | z<<2, oct_node/child_index.cpp:13-15),
+ *    the order of OctNode::output_tree (oct_node/oct_node.cpp:163-170).
+ *  - State arrays are [brick][field][k][j][i], GNX = nx + 2*bw cells per edge
+ *    including ghosts, FP64.  Fields (Euler): d, sx, sy, sz, et, tau
+ *    (euler/state.cpp:12-17).
+ *  - Calls are asynchronous on the context's CUDA stream except those that
+ *    return host scalars or host arrays.
+ */
+#ifndef AMR_B200_H
+#define AMR_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AMR_OK 0
+#define AMR_ERR_ARG (-1)
+#define AMR_ERR_CUDA (-2)
+#define AMR_ERR_RANGE (-3)
+#define AMR_ERR_NOCONVERGE (-4)
+#define AMR_ERR_TIMEOUT (-5)
+#define AMR_ERR_STATE (-6)
+#define AMR_ERR_CAPACITY (-7)
+#define AMR_ERR_NODEVICE (-8)
+
+#define AMR_PHYSICS_EULER 0         /* euler/state.cpp, no gravity */
+#define AMR_PHYSICS_EULER_GRAVITY 1 /* Euler state + Poisson self-gravity */
+
+#define AMR_PREC_FP64 0  /* plain form: FP64 throughout, reference operation order */
+#define AMR_PREC_MIXED 1 /* FP32 flux/smoother inside FP64 state and defect correction */
+
+typedef struct amr_ctx amr_ctx;
+
+typedef struct amr_config {
+    int bw;               /* BW ghost width (euler/euler_defs.h:28) */
+    int nx;               /* interior cells per brick edge, GNX-2*BW (euler_defs.h:30) */
+    int nf;               /* STATE_NF (euler/state.h:16) */
+    int physics;          /* AMR_PHYSICS_* */
+    int precision;        /* AMR_PREC_* */
+    int z_reflect;        /* Z_REFLECT: domain z in [0, 2*GRID_DIM], mirror at z=0 */
+    int mirror_refine_y;  /* MIRROR_REFINE_Y (euler_defs.h:50) */
+    int max_refine_level; /* GridNode::max_refine_level */
+    int min_level;        /* MINLEVEL (defs.h:22) */
+    int min_grid_life;    /* MIN_GRID_LIFE (defs.h:23) */
+    int max_bricks;       /* device brick pool capacity; 0 = host-only context */
+    int reserved;
+    double grid_dim;      /* GRID_DIM */
+    double origin[3];     /* Grid::origin (grid/grid.h:23) */
+    double minmod_theta;  /* MINMOD_THETA (euler_defs.h:21) */
+    double cfl;           /* GRID_CFL_FACTOR (euler_defs.h:48) */
+    double gamma;         /* State::gamma (euler/state.cpp:9) */
+    double rho_floor;     /* State::rho_floor (euler/state.cpp:10) */
+    double ei_floor;      /* State::ei_floor (euler/state.cpp:11) */
+    double maxdtinc;      /* MAXDTINC (euler_defs.h:47) */
+    double grav_g;        /* G_CON (euler/state.h:14) */
+} amr_config;
+
+/* Fills the reference's EULER defaults (euler/euler_defs.h, defs.h). */
+int amr_default_config(amr_config* cfg);
+
+/* Context: one per tree, one CUDA stream.  cfg->max_bricks == 0 gives a
+ * host-only context for octree/refinement logic (every device call then
+ * returns AMR_ERR_NODEVICE). */
+int amr_create(const amr_config* cfg, amr_ctx** out);
+int amr_destroy(amr_ctx* ctx);
+const char* amr_last_error(const amr_ctx* ctx);
+
+/* ---- octree (host) ------------------------------------------------------ */
+/* GridNode::init (grid/grid_node.cpp:1410-1418): a lone root brick whose six
+ * faces are physical boundaries. */
+int amr_init_root(amr_ctx* ctx);
+/* Rebuild the tree from a depth-first pre-order node list (the order of
+ * GridNode::read, grid/grid_node.cpp:45-57): level[n], loc[3n], age[n]. */
+int amr_load_tree(amr_ctx* ctx, int n, const int* level, const int* loc, const int* age);
+int amr_num_bricks(const amr_ctx* ctx);
+/* Tree description in DFS pre-order; any pointer may be NULL. */
+int amr_get_tree(const amr_ctx* ctx, int* level, int* loc, int* offset, int* age, int* child_mask,
+                 int* refine_mask, double* h);
+/* Refinement decision of GridNode::check_for_refine (grid_node.cpp:957-1033)
+ * given per-brick octant density flags: flags[8*b+c] != 0 when some interior
+ * cell of brick b in octant c has rho > min_refine_density.  Host only;
+ * creates/destroys nodes (prolongation of new bricks happens on the device
+ * when the context has one).  *changed = use_refine_flags() result. */
+int amr_refine_from_flags(amr_ctx* ctx, const unsigned char* flags, int clear, int* changed);
+/* Grid::set_time on the whole tree (grid_node.cpp:547-556); t == 0 resets ages. */
+int amr_set_time(amr_ctx* ctx, double t);
+double amr_get_time(const amr_ctx* ctx);
+/* Leaf cells (GridNode::get_zone_cnt, grid_node.cpp:1276-1288). */
+long long amr_zone_count(const amr_ctx* ctx);
+
+/* ---- state transfer ------------------------------------------------------ */
+int amr_upload_state(amr_ctx* ctx, const double* U);   /* [n][nf][gnx^3] */
+int amr_download_state(amr_ctx* ctx, double* U);
+/* Poisson arrays phi, phi0, dphi, dphi1, S, fx, fy, fz: [8][n][pnx^3],
+ * pnx = nx + 2 (poisson/poisson.h:4). */
+int amr_upload_poisson(amr_ctx* ctx, const double* P);
+int amr_download_poisson(amr_ctx* ctx, double* P);
+/* Root flow-off accumulator FO[nf] (Grid::flow_off, grid/grid.cpp:346). */
+int amr_get_flow_off(amr_ctx* ctx, double* fo);
+int amr_set_flow_off(amr_ctx* ctx, const double* fo);
+int amr_synchronize(amr_ctx* ctx);
+
+/* ---- GridNode call surface (whole tree) --------------------------------- */
+int amr_enforce_boundaries(amr_ctx* ctx);          /* grid_node.cpp:59-112 + grid_amr_bound/grid_phys_bound */
+int amr_store(amr_ctx* ctx);                       /* grid.cpp:173-186, grid_node.cpp:495-515 */
+int amr_restore(amr_ctx* ctx);                     /* grid.cpp:188-199 */
+/* compute_{x,y,z}_flux + adjust_{x,y,z}_flux (grid.cpp:215-302,
+ * grid_node.cpp:1076-1274). */
+int amr_compute_fluxes(amr_ctx* ctx);
+/* clear_difs + sum_{x,y,z}_difs (+ flow-off at the root) + add_difs(dt,beta)
+ * (grid.cpp:201-213,304-420; grid_node.cpp:337-357,517-551). */
+int amr_add_difs(amr_ctx* ctx, double dt, double beta);
+int amr_inject_from_children(amr_ctx* ctx);        /* grid_node.cpp:1035-1074 */
+int amr_max_dt(amr_ctx* ctx, double* dt);          /* grid.cpp:422-483, grid_node.cpp:163-174 */
+/* check_for_refine with the density test on the device. */
+int amr_check_for_refine(amr_ctx* ctx, double min_refine_density, int clear, int* changed);
+/* GridNode::state_max (grid_node.cpp:1529-1558) for one field. */
+int amr_state_max(amr_ctx* ctx, int field, double* vmax);
+
+/* ---- driver sequences ----------------------------------------------------- */
+/* HydroDriver::sub_step (euler/hydro_driver.cpp:200-214). */
+int amr_sub_step(amr_ctx* ctx, double dt, double beta);
+/* HydroDriver::step (euler/hydro_driver.cpp:171-194): store, RK3 substeps
+ * with restriction, boundaries, regrid (min_refine_density), time += dt. */
+int amr_hydro_step(amr_ctx* ctx, double dt, double min_refine_density);
+
+/* ---- Poisson (poisson/poisson.h:44-69) ------------------------------------ */
+int amr_poisson_set_source(amr_ctx* ctx);                  /* poisson.cpp:950-966 */
+int amr_poisson_boundaries(amr_ctx* ctx);                  /* source sums + multipole phys bounds */
+int amr_compute_forces(amr_ctx* ctx);                      /* poisson.cpp:223-247 + adjust_*_force */
+int amr_vcycle(amr_ctx* ctx, double* l1_error);            /* poisson.cpp:1069-1074 */
+int amr_poisson_solve(amr_ctx* ctx, double tol, int max_cycles, double* l1_error, int* cycles);
+int amr_store_phi(amr_ctx* ctx);                           /* poisson.cpp:166-181 */
+int amr_restore_phi(amr_ctx* ctx);                         /* poisson.cpp:183-198 */
+int amr_restore_half_phi(amr_ctx* ctx);                    /* poisson.cpp:200-221 */
+/* Self-gravitating RK3 step (binary/binary_driver.cpp:346-459 sequence on the
+ * Euler state): per substep hydro + gravity sources, phi time level, solve;
+ * regrid every 8 steps at state_max/dynamic_range. */
+int amr_grav_step(amr_ctx* ctx, double dt, double tol, double dynamic_range, int step_index);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,105 @@
+"""Generate the golden fixtures in tests/golden/ from the reference itself.
+
+Runs the reference oracle harness (oracle/_ref/*_harness, built from the
+reference sources by oracle/build_ref.py) on small cases and stores, per
+case, the initial and final octree and the interior cells of every brick
+(ghost slabs are recomputed from interiors), the per-step dt sequence and the
+root flow-off accumulator.  Re-running this script must reproduce the
+committed files bit for bit (tests/test_oracle_ref.py checks that).
+
+    python tests/golden/make_golden.py [case ...]
+"""
+
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+from dumpio import read_dump  # noqa: E402
+
+# name: (variant, mode, argv after mode)
+CASES = {
+    "hydro_blast_L2": ("g05", "hydro", ["blast", 2, 20, 1e-6]),
+    "hydro_bump_L2": ("g05", "hydro", ["bump", 2, 5, 3.0]),
+    "hydro_bump_L3": ("g05", "hydro", ["bump", 3, 4, 3.0]),
+    "hydro_bump_zr_L3": ("zr", "hydro", ["bump", 3, 4, 3.0]),
+    "poisson_poly_L2": ("g05", "poisson", ["polytrope", 2, 4]),
+    "poisson_poly_L3": ("g05", "poisson", ["polytrope", 3, 3]),
+    "grav_poly_L2": ("g05", "grav", ["polytrope", 2, 3, 1e-6]),
+}
+# cases whose full state would make a large fixture keep only the tree and
+# per-brick, per-field sums and absolute sums of the interior cells
+SUMMARY_ONLY = {"hydro_blast_L2", "hydro_bump_L3", "poisson_poly_L3"}
+# for these the final conserved state is kept as sums only (the potential in
+# full): the initial state is needed in full to start from the same data
+FINAL_SUMMARY = {"grav_poly_L2"}
+
+
+def interior(d, U):
+    b = d.bw
+    return U[:, :, b:-b, b:-b, b:-b].copy()
+
+
+def pack(prefix, d, summary):
+    U = interior(d, d.U)
+    out = {
+        prefix + "level": d.level, prefix + "loc": d.loc, prefix + "age": d.age,
+        prefix + "child_mask": d.child_mask, prefix + "refine_mask": d.refine_mask,
+        prefix + "FO": d.FO, prefix + "time": np.float64(d.time),
+        prefix + "Usum": U.reshape(U.shape[0], U.shape[1], -1).sum(axis=2),
+        prefix + "Uabs": np.abs(U).reshape(U.shape[0], U.shape[1], -1).sum(axis=2),
+    }
+    if not summary:
+        out[prefix + "U"] = U
+    if d.P is not None and not summary:
+        out[prefix + "phi"] = d.P["phi"]
+    if d.P is not None:
+        out[prefix + "phisum"] = d.P["phi"][:, 1:-1, 1:-1, 1:-1].reshape(d.nnodes, -1).sum(axis=1)
+    return out
+
+
+def run_case(name, workdir):
+    variant, mode, args = CASES[name]
+    exe = os.path.join(ROOT, "oracle", "_ref", variant + "_harness")
+    out = os.path.join(workdir, name + ".bin")
+    env = dict(os.environ, OMP_NUM_THREADS="1")
+    r = subprocess.run([exe, mode] + [str(a) for a in args] + [out], cwd=workdir, env=env,
+                       capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(r.stdout + r.stderr)
+    d0 = read_dump(out + ".init")
+    summ = name in SUMMARY_ONLY
+    res = {"variant": np.array(variant), "mode": np.array(mode), "args": np.array([str(a) for a in args]),
+           "bw": np.int32(d0.bw), "nx": np.int32(d0.gnx - 2 * d0.bw)}
+    res.update(pack("init_", d0, summ))
+    if mode == "poisson":
+        ncyc = int(args[2])
+        for c in range(ncyc):
+            dc = read_dump(out + ".%d" % c)
+            res.update(pack("cycle%d_" % c, dc, summ))
+            res["extra"] = dc.extra
+    else:
+        d1 = read_dump(out)
+        res["extra"] = d1.extra
+        res.update(pack("final_", d1, summ or name in FINAL_SUMMARY))
+        if name in FINAL_SUMMARY:
+            res["final_phi"] = d1.P["phi"]
+    return res
+
+
+def main(names):
+    with tempfile.TemporaryDirectory() as td:
+        for n in names:
+            res = run_case(n, td)
+            path = os.path.join(HERE, n + ".npz")
+            np.savez_compressed(path, **res)
+            print(n, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:] or list(CASES))
