@@ -87,6 +87,14 @@ def load_library(path=LIB_PATH):
         lib.amr_state_max.argtypes = [P, I, dp]
         lib.amr_sub_step.argtypes = [P, D, D]
         lib.amr_hydro_step.argtypes = [P, D, D]
+        lib.amr_get_stream.argtypes = [P, ctypes.POINTER(ctypes.c_void_p)]
+        lib.amr_profile_enable.argtypes = [P, I]
+        lib.amr_profile_reset.argtypes = [P]
+        lib.amr_profile_get.argtypes = [P, I, dp, ctypes.POINTER(ctypes.c_longlong),
+                                        ctypes.POINTER(ctypes.c_char_p)]
+        lib.amr_stats.argtypes = [P, ctypes.POINTER(ctypes.c_longlong), ip, ip, ip]
+        lib.amr_profile_units.argtypes = [P, I, ctypes.POINTER(ctypes.c_longlong)]
+        lib.amr_launch_count.argtypes = [P, ctypes.POINTER(ctypes.c_longlong)]
         if hasattr(lib, "amr_vcycle"):
             lib.amr_vcycle.argtypes = [P, dp]
             lib.amr_poisson_solve.argtypes = [P, D, I, dp, ip]
@@ -262,6 +270,43 @@ class AMR:
 
     def hydro_step(self, dt, min_refine_density):
         self._check(self.lib.amr_hydro_step(self.ctx, float(dt), float(min_refine_density)))
+
+    # ---- instrumentation ----------------------------------------------------
+    def stream_handle(self):
+        s = ctypes.c_void_p()
+        self._check(self.lib.amr_get_stream(self.ctx, ctypes.byref(s)))
+        return s.value
+
+    def profile(self, on=True):
+        self._check(self.lib.amr_profile_enable(self.ctx, int(on)))
+
+    def profile_reset(self):
+        self._check(self.lib.amr_profile_reset(self.ctx))
+
+    def profile_get(self):
+        out = {}
+        for cls in range(19):
+            ms = ctypes.c_double()
+            n = ctypes.c_longlong()
+            name = ctypes.c_char_p()
+            self._check(self.lib.amr_profile_get(self.ctx, cls, ctypes.byref(ms), ctypes.byref(n),
+                                                 ctypes.byref(name)))
+            u = ctypes.c_longlong()
+            self._check(self.lib.amr_profile_units(self.ctx, cls, ctypes.byref(u)))
+            out[name.value.decode()] = dict(ms=ms.value, launches=n.value, units=u.value)
+        return out
+
+    def launch_count(self):
+        n = ctypes.c_longlong()
+        self._check(self.lib.amr_launch_count(self.ctx, ctypes.byref(n)))
+        return n.value
+
+    def stats(self):
+        rc = ctypes.c_longlong()
+        hz, nb, ml = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.amr_stats(self.ctx, ctypes.byref(rc), ctypes.byref(hz), ctypes.byref(nb),
+                                       ctypes.byref(ml)))
+        return dict(relax_calls=rc.value, reflux_hazards=hz.value, nbricks=nb.value, max_level=ml.value)
 
     # ---- Poisson ------------------------------------------------------------
     def vcycle(self):

@@ -10,6 +10,7 @@
 #include <functional>
 
 #include "context.h"
+#include "profiler.h"
 #include "kernels.h"
 #include "poisson.h"
 
@@ -282,7 +283,10 @@ int finish_refine(amr_ctx* c) {
     int* d;
     CUDA_TRY(cudaMalloc(&d, sizeof(int) * slots.size()));
     CUDA_TRY(cudaMemcpyAsync(d, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice, c->stream));
-    launch_prolong(c->geom, c->bt, c->st, d, (int)slots.size(), c->stream);
+    {
+        ProfScope ps_(c->prof, KC_PROLONG, c->stream);
+        launch_prolong(c->geom, c->bt, c->st, d, (int)slots.size(), c->stream);
+    }
     if (c->cfg.physics == AMR_PHYSICS_EULER_GRAVITY)
         launch_poisson_new_bricks(c->geom, c->bt, c->st, d, (int)slots.size(), c->stream);
     TRY(check_launch(c));
@@ -632,7 +636,10 @@ int amr_synchronize(amr_ctx* c) {
 int amr_enforce_boundaries(amr_ctx* c) {
     NEED_DEVICE(c);
     for (int l = 0; l <= c->tree.prm.max_level; l++)
-        launch_ghost_fill(c->geom, c->bt, c->st, dslots_level(c, l), (int)c->level_slots[l].size(), c->stream);
+        {
+            ProfScope ps_(c->prof, KC_GHOST, c->stream, (long long)c->level_slots[l].size());
+            launch_ghost_fill(c->geom, c->bt, c->st, dslots_level(c, l), (int)c->level_slots[l].size(), c->stream);
+        }
     return check_launch(c);
 }
 
@@ -663,10 +670,16 @@ int amr_restore(amr_ctx* c) {
 // level upward so a corrected child face is final before its parent uses it.
 int amr_compute_fluxes(amr_ctx* c) {
     NEED_DEVICE(c);
-    launch_flux(c->geom, c->st, dslots_all(c), (int)c->all_slots.size(), c->stream);
+    {
+        ProfScope ps_(c->prof, KC_FLUX, c->stream, (long long)c->all_slots.size());
+        launch_flux(c->geom, c->st, dslots_all(c), (int)c->all_slots.size(), c->stream);
+    }
     for (int l = c->tree.prm.max_level; l >= 0; l--) {
         const int n = c->off_reflux[l + 1] - c->off_reflux[l];
-        launch_reflux(c->geom, c->st, c->d_reflux + c->off_reflux[l], n, c->stream);
+        {
+            ProfScope ps_(c->prof, KC_REFLUX, c->stream);
+            launch_reflux(c->geom, c->st, c->d_reflux + c->off_reflux[l], n, c->stream);
+        }
     }
     return check_launch(c);
 }
@@ -674,8 +687,14 @@ int amr_compute_fluxes(amr_ctx* c) {
 int amr_add_difs(amr_ctx* c, double dt, double beta) {
     NEED_DEVICE(c);
     const int grav = c->cfg.physics == AMR_PHYSICS_EULER_GRAVITY;
-    launch_flow_off(c->geom, c->st, c->tree.root()->slot, c->tree.root()->h, dt, beta, c->d_fo, c->stream);
-    launch_add_difs(c->geom, c->st, dslots_all(c), (int)c->all_slots.size(), c->bt.h, dt, beta, grav, c->stream);
+    {
+        ProfScope ps_(c->prof, KC_ADD_DIFS, c->stream);
+        launch_flow_off(c->geom, c->st, c->tree.root()->slot, c->tree.root()->h, dt, beta, c->d_fo, c->stream);
+    }
+    {
+        ProfScope ps_(c->prof, KC_ADD_DIFS, c->stream, (long long)c->all_slots.size());
+        launch_add_difs(c->geom, c->st, dslots_all(c), (int)c->all_slots.size(), c->bt.h, dt, beta, grav, c->stream);
+    }
     for (Node* n : c->order) n->age++;  // GridNode::add_difs, grid_node.cpp:338
     return check_launch(c);
 }
@@ -684,7 +703,10 @@ int amr_add_difs(amr_ctx* c, double dt, double beta) {
 int amr_inject_from_children(amr_ctx* c) {
     NEED_DEVICE(c);
     for (int l = c->tree.prm.max_level; l >= 0; l--)
-        launch_inject(c->geom, c->bt, c->st, dslots_parent(c, l), (int)c->parent_slots[l].size(), c->stream);
+        {
+            ProfScope ps_(c->prof, KC_INJECT, c->stream);
+            launch_inject(c->geom, c->bt, c->st, dslots_parent(c, l), (int)c->parent_slots[l].size(), c->stream);
+        }
     return check_launch(c);
 }
 
@@ -694,7 +716,10 @@ int amr_max_dt(amr_ctx* c, double* dt) {
     NEED_DEVICE(c);
     if (!dt) return AMR_ERR_ARG;
     const int n = (int)c->all_slots.size();
-    launch_max_dt(c->geom, c->st, dslots_all(c), n, c->bt.h, c->d_dt, c->stream);
+    {
+        ProfScope ps_(c->prof, KC_MAX_DT, c->stream, (long long)n);
+        launch_max_dt(c->geom, c->st, dslots_all(c), n, c->bt.h, c->d_dt, c->stream);
+    }
     TRY(check_launch(c));
     std::vector<double> per(c->cap);
     int maxslot = 0;
@@ -719,7 +744,10 @@ int amr_max_dt(amr_ctx* c, double* dt) {
 int amr_check_for_refine(amr_ctx* c, double min_refine_density, int clear, int* changed) {
     NEED_DEVICE(c);
     const int n = (int)c->all_slots.size();
-    launch_refine_flags(c->geom, c->st, dslots_all(c), n, min_refine_density, c->d_flags, c->stream);
+    {
+        ProfScope ps_(c->prof, KC_REFINE, c->stream);
+        launch_refine_flags(c->geom, c->st, dslots_all(c), n, min_refine_density, c->d_flags, c->stream);
+    }
     TRY(check_launch(c));
     std::vector<unsigned char> fl(8 * (size_t)n);
     CUDA_TRY(cudaMemcpyAsync(fl.data(), c->d_flags, fl.size(), cudaMemcpyDeviceToHost, c->stream));
@@ -735,7 +763,10 @@ int amr_state_max(amr_ctx* c, int field, double* vmax) {
     NEED_DEVICE(c);
     if (field < 0 || field >= c->geom.nf || !vmax) return AMR_ERR_ARG;
     const int n = (int)c->all_slots.size();
-    launch_state_max(c->geom, c->bt, c->st, dslots_all(c), n, field, c->d_red, c->stream);
+    {
+        ProfScope ps_(c->prof, KC_OTHER, c->stream);
+        launch_state_max(c->geom, c->bt, c->st, dslots_all(c), n, field, c->d_red, c->stream);
+    }
     TRY(check_launch(c));
     std::vector<double> v(n);
     CUDA_TRY(cudaMemcpyAsync(v.data(), c->d_red, sizeof(double) * n, cudaMemcpyDeviceToHost, c->stream));
@@ -769,6 +800,71 @@ int amr_hydro_step(amr_ctx* c, double dt, double min_refine_density) {
     TRY(amr_enforce_boundaries(c));
     TRY(amr_check_for_refine(c, min_refine_density, 1, nullptr));
     TRY(amr_set_time(c, c->time + dt));
+    return AMR_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// instrumentation
+// ---------------------------------------------------------------------------
+extern "C" {
+
+static const char* kClassNames[amr::KC_COUNT] = {
+    "ghost_fill", "flux", "reflux", "add_difs", "inject", "max_dt", "refine_flags", "prolong",
+    "relax", "vcycle_down", "phi_boundaries", "dphi_boundaries", "forces", "solution_error",
+    "source", "phys_boundary", "coarse_correction", "phi_time", "other"};
+
+int amr_get_stream(amr_ctx* c, void** stream) {
+    NEED_DEVICE(c);
+    if (!stream) return AMR_ERR_ARG;
+    *stream = (void*)c->stream;
+    return AMR_OK;
+}
+
+int amr_profile_enable(amr_ctx* c, int on) {
+    NEED_DEVICE(c);
+    c->prof.collect();
+    c->prof.on = on != 0;
+    return AMR_OK;
+}
+
+int amr_profile_reset(amr_ctx* c) {
+    NEED_DEVICE(c);
+    c->prof.reset();
+    return AMR_OK;
+}
+
+int amr_profile_get(amr_ctx* c, int cls, double* ms, long long* launches, const char** name) {
+    NEED_DEVICE(c);
+    if (cls < 0 || cls >= amr::KC_COUNT) return AMR_ERR_ARG;
+    c->prof.collect();
+    if (ms) *ms = c->prof.ms[cls];
+    if (launches) *launches = c->prof.launches[cls];
+    if (name) *name = kClassNames[cls];
+    return AMR_OK;
+}
+
+int amr_launch_count(amr_ctx* c, long long* kernels) {
+    if (!c || !kernels) return AMR_ERR_ARG;
+    *kernels = c->prof.kernels;
+    return AMR_OK;
+}
+
+int amr_profile_units(amr_ctx* c, int cls, long long* units) {
+    NEED_DEVICE(c);
+    if (cls < 0 || cls >= amr::KC_COUNT || !units) return AMR_ERR_ARG;
+    c->prof.collect();
+    *units = c->prof.units[cls];
+    return AMR_OK;
+}
+
+int amr_stats(amr_ctx* c, long long* relax_calls, int* reflux_hazards, int* nbricks, int* max_level) {
+    if (!c) return AMR_ERR_ARG;
+    if (relax_calls) *relax_calls = c->relax_calls;
+    if (reflux_hazards) *reflux_hazards = c->reflux_hazards;
+    if (nbricks) *nbricks = (int)c->order.size();
+    if (max_level) *max_level = c->tree.max_level_present();
     return AMR_OK;
 }
 

@@ -8,6 +8,7 @@
 
 #include "amr_internal.h"
 #include "octree.h"
+#include "profiler.h"
 
 struct amr_ctx {
     amr_config cfg{};
@@ -60,6 +61,7 @@ struct amr_ctx {
     int vcycle_max_outer = 1000;
     long long relax_calls = 0, relax_sweeps_total = 0;
     bool topo_dirty = true;
+    amr::Profiler prof;
 
     amr_ctx(const amr::TreeParams& p) : tree(p) {}
 };

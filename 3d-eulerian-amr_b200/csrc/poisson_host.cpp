@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "context.h"
+#include "profiler.h"
 #include "kernels.h"
 #include "poisson.h"
 
@@ -97,17 +98,28 @@ double nested_tree_sum(const Node* n, const std::vector<double>& per) {
 }
 
 int phi_boundaries(amr_ctx* c, int l) {
-    launch_phi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), c->stream);
+    {
+        ProfScope ps_(c->prof, KC_PHI_BOUND, c->stream, nlvl(c, l));
+        launch_phi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), c->stream);
+    }
     return check_launch(c);
 }
 
 int dphi_boundaries(amr_ctx* c, int l) {
-    launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), c->stream);
+    {
+        ProfScope ps_(c->prof, KC_DPHI_BOUND, c->stream, nlvl(c, l));
+        launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), c->stream);
+    }
     return check_launch(c);
 }
 
 int relax(amr_ctx* c, int l, double* resid) {
-    if (launch_relax(c->geom, c->st, lvl(c, l), nlvl(c, l), c->d_pres, nullptr, c->stream)) {
+    int bad;
+    {
+        ProfScope ps_(c->prof, KC_RELAX, c->stream, nlvl(c, l));
+        bad = launch_relax(c->geom, c->st, lvl(c, l), nlvl(c, l), c->d_pres, nullptr, c->stream);
+    }
+    if (bad) {
         c->err = "relaxation kernel built for nx == 8 only";
         return AMR_ERR_ARG;
     }
@@ -147,44 +159,74 @@ int max_level_present(amr_ctx* c) {
 int vcycle0(amr_ctx* c) {
     const int maxlevel = max_level_present(c);
     for (int l = maxlevel - 1; l >= 0; l--)  // phi_from_children: children first
-        launch_phi_from_children(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l],
-                                 (int)c->parent_slots[l].size(), c->stream);
+        {
+            ProfScope ps_(c->prof, KC_VDOWN, c->stream);
+            launch_phi_from_children(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l],
+                                     (int)c->parent_slots[l].size(), c->stream);
+        }
     TRY(check_launch(c));
     for (int l = 0; l <= maxlevel; l++) TRY(phi_boundaries(c, l));
-    launch_init_vcycle(c->geom, c->st, all(c), nall(c), c->stream);
+    {
+        ProfScope ps_(c->prof, KC_VDOWN, c->stream);
+        launch_init_vcycle(c->geom, c->st, all(c), nall(c), c->stream);
+    }
     for (int l = maxlevel; l >= 0; l--) {
         TRY(dphi_boundaries(c, l));
-        launch_vdown_a(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->stream);
+        {
+            ProfScope ps_(c->prof, KC_VDOWN, c->stream);
+            launch_vdown_a(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->stream);
+        }
         for (int dir = 0; dir < 3; dir++) {
             const int a = c->off_reflux_dir[3 * l + dir], b = c->off_reflux_dir[3 * l + dir + 1];
-            launch_adjust_dphi(c->geom, c->bt, c->st, c->d_reflux + a, b - a, c->stream);
+            {
+                ProfScope ps_(c->prof, KC_VDOWN, c->stream);
+                launch_adjust_dphi(c->geom, c->bt, c->st, c->d_reflux + a, b - a, c->stream);
+            }
         }
-        launch_vdown_c(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->stream);
+        {
+            ProfScope ps_(c->prof, KC_VDOWN, c->stream);
+            launch_vdown_c(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->stream);
+        }
         TRY(check_launch(c));
         TRY(relax_until(c, l, 1.0));
     }
     for (int l = 0; l <= maxlevel; l++) {
         TRY(dphi_boundaries(c, l));
-        if (l > 0) launch_coarse_correction(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->stream);
+        if (l > 0) {
+            ProfScope ps_(c->prof, KC_CORRECT, c->stream);
+            launch_coarse_correction(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->stream);
+        }
         TRY(check_launch(c));
         TRY(relax_until(c, l, 0.05));
-        launch_retire(c->geom, c->st, lvl(c, l), nlvl(c, l), c->stream);
+        {
+            ProfScope ps_(c->prof, KC_CORRECT, c->stream);
+            launch_retire(c->geom, c->st, lvl(c, l), nlvl(c, l), c->stream);
+        }
         TRY(phi_boundaries(c, l));
     }
     return AMR_OK;
 }
 
 int compute_forces(amr_ctx* c) {
-    launch_forces(c->geom, c->bt, c->st, all(c), nall(c), c->stream);
+    {
+        ProfScope ps_(c->prof, KC_FORCES, c->stream);
+        launch_forces(c->geom, c->bt, c->st, all(c), nall(c), c->stream);
+    }
     for (int l = c->tree.prm.max_level; l >= 0; l--) {
         const int n = c->off_reflux[l + 1] - c->off_reflux[l];
-        launch_adjust_force(c->geom, c->st, c->d_reflux + c->off_reflux[l], n, c->stream);
+        {
+            ProfScope ps_(c->prof, KC_FORCES, c->stream);
+            launch_adjust_force(c->geom, c->st, c->d_reflux + c->off_reflux[l], n, c->stream);
+        }
     }
     return check_launch(c);
 }
 
 int solution_error(amr_ctx* c, double* err) {
-    launch_solution_error(c->geom, c->bt, c->st, all(c), nall(c), c->d_pres, c->stream);
+    {
+        ProfScope ps_(c->prof, KC_ERROR, c->stream);
+        launch_solution_error(c->geom, c->bt, c->st, all(c), nall(c), c->d_pres, c->stream);
+    }
     TRY(check_launch(c));
     std::vector<double> per;
     TRY(fetch_per_slot(c, per));
@@ -255,7 +297,10 @@ int amr_download_poisson(amr_ctx* c, double* P) {
 
 int amr_poisson_set_source(amr_ctx* c) {
     TRY(need_gravity(c));
-    launch_set_source(c->geom, c->st, all(c), nall(c), c->stream);
+    {
+        ProfScope ps_(c->prof, KC_SOURCE, c->stream);
+        launch_set_source(c->geom, c->st, all(c), nall(c), c->stream);
+    }
     return check_launch(c);
 }
 
@@ -263,9 +308,15 @@ int amr_poisson_set_source(amr_ctx* c) {
 int amr_poisson_boundaries(amr_ctx* c) {
     TRY(need_gravity(c));
     TRY(amr_poisson_set_source(c));
-    launch_source_sums(c->geom, c->bt, c->st, all(c), nall(c), c->d_msrc, c->d_allref, c->stream);
-    launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, all(c), nall(c), c->d_msrc, c->d_allref, c->d_bphi,
-                      c->stream);
+    {
+        ProfScope ps_(c->prof, KC_SOURCE, c->stream);
+        launch_source_sums(c->geom, c->bt, c->st, all(c), nall(c), c->d_msrc, c->d_allref, c->stream);
+    }
+    {
+        ProfScope ps_(c->prof, KC_PHYS_BOUND, c->stream);
+        launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, all(c), nall(c), c->d_msrc, c->d_allref, c->d_bphi,
+                          c->stream);
+    }
     return check_launch(c);
 }
 
@@ -313,19 +364,28 @@ int amr_poisson_solve(amr_ctx* c, double tol, int max_cycles, double* l1_error, 
 
 int amr_store_phi(amr_ctx* c) {
     TRY(need_gravity(c));
-    launch_phi_time(c->geom, c->st, all(c), nall(c), 0, c->stream);
+    {
+        ProfScope ps_(c->prof, KC_PHI_TIME, c->stream);
+        launch_phi_time(c->geom, c->st, all(c), nall(c), 0, c->stream);
+    }
     return check_launch(c);
 }
 
 int amr_restore_phi(amr_ctx* c) {
     TRY(need_gravity(c));
-    launch_phi_time(c->geom, c->st, all(c), nall(c), 1, c->stream);
+    {
+        ProfScope ps_(c->prof, KC_PHI_TIME, c->stream);
+        launch_phi_time(c->geom, c->st, all(c), nall(c), 1, c->stream);
+    }
     return check_launch(c);
 }
 
 int amr_restore_half_phi(amr_ctx* c) {
     TRY(need_gravity(c));
-    launch_phi_time(c->geom, c->st, all(c), nall(c), 2, c->stream);
+    {
+        ProfScope ps_(c->prof, KC_PHI_TIME, c->stream);
+        launch_phi_time(c->geom, c->st, all(c), nall(c), 2, c->stream);
+    }
     return check_launch(c);
 }
 

@@ -155,6 +155,25 @@ int amr_restore_half_phi(amr_ctx* ctx);                    /* poisson.cpp:200-22
  * regrid every 8 steps at state_max/dynamic_range. */
 int amr_grav_step(amr_ctx* ctx, double dt, double tol, double dynamic_range, int step_index);
 
+/* ---- instrumentation ------------------------------------------------------
+ * The reference times steps with omp_get_wtime (binary_driver.cpp:115,303);
+ * here device time per kernel class comes from CUDA events on the context
+ * stream.  Classes 0..18: ghost_fill flux reflux add_difs inject max_dt
+ * refine_flags prolong relax vcycle_down phi_boundaries dphi_boundaries
+ * forces solution_error source phys_boundary coarse_correction phi_time other.
+ */
+int amr_get_stream(amr_ctx* ctx, void** stream);  /* the context's cudaStream_t */
+int amr_profile_enable(amr_ctx* ctx, int on);
+int amr_profile_reset(amr_ctx* ctx);
+int amr_profile_get(amr_ctx* ctx, int cls, double* ms, long long* launches, const char** name);
+/* bricks (or correction items) processed by a class's launches */
+int amr_profile_units(amr_ctx* ctx, int cls, long long* units);
+/* kernels this context has launched so far */
+int amr_launch_count(amr_ctx* ctx, long long* kernels);
+/* relaxation calls so far, coarse-fine corrections whose depth-first order
+ * would matter in the reference (0 under proper nesting), bricks, deepest level */
+int amr_stats(amr_ctx* ctx, long long* relax_calls, int* reflux_hazards, int* nbricks, int* max_level);
+
 #ifdef __cplusplus
 }
 #endif

@@ -519,13 +519,26 @@ int main(int argc, char* argv[]) {
         std::vector<double> extra;
         if (mode == "grav") dump((std::string(out) + ".init").c_str(), root, root, root->get_time(), extra);
         double last_dt = 0.0;
-        std::vector<double> dts;
+        std::vector<double> dts, step_secs;
+        std::vector<int> step_cycles;
         const double t0 = omp_get_wtime();
         for (int s = 0; s < nsteps; s++) {
             const double dt = next_dt(root, s, last_dt);
             last_dt = dt;
             dts.push_back(dt);
+            const double ts = omp_get_wtime();
+            const size_t nv0 = drv.vcycle_errors.size();
             drv.step(dt, tol);
+            step_secs.push_back(omp_get_wtime() - ts);
+            int cyc = 0;
+            for (size_t q = nv0; q < drv.vcycle_errors.size(); q++)
+                if (drv.vcycle_errors[q] >= 0.0) cyc++;
+            step_cycles.push_back(cyc);
+            if (mode == "time_grav") {
+                printf("{\"step\": %d, \"seconds\": %.6f, \"vcycles\": %d, \"bricks\": %d}\n", s, step_secs.back(),
+                       cyc, root->get_node_cnt());
+                fflush(stdout);
+            }
         }
         const double t1 = omp_get_wtime();
         if (mode == "grav") {
@@ -540,6 +553,49 @@ int main(int argc, char* argv[]) {
                    nsteps, t1 - t0, leaf, root->get_node_cnt(), omp_get_max_threads(),
                    (int)drv.vcycle_errors.size());
         }
+        return 0;
+    }
+    if (mode == "sample_grav") {
+        // Bounded CPU sample of the self-gravitating step: one RK3 hydro step
+        // with gravity sources (the substep sequence without its solves) and
+        // `nvc` V-cycles, timed separately on the full tree.
+        if (argc < 5) return 2;
+        g_ic = argv[2];
+        g_maxlevel = atoi(argv[3]);
+        const int nvc = atoi(argv[4]);
+        GravNode* root = build_tree<GravNode>(1.0e-6);
+        GravDriver drv;
+        drv.root = root;
+        root->compute_source_sums();
+        root->compute_physical_boundaries(root);
+        root->compute_forces();
+        root->vcycle();
+        const double dt = root->max_dt();
+        const double t0 = omp_get_wtime();
+        root->store();
+        const double betas[3] = {1.0, 0.25, 2.0 / 3.0};
+        for (int rk = 0; rk < 3; rk++) {
+            root->enforce_boundaries();
+            root->clear_difs();
+            root->compute_x_flux();
+            root->adjust_x_flux();
+            root->sum_x_difs();
+            root->compute_y_flux();
+            root->adjust_y_flux();
+            root->sum_y_difs();
+            root->compute_z_flux();
+            root->adjust_z_flux();
+            root->sum_z_difs();
+            root->error_from_parent();
+            root->add_difs(dt, betas[rk]);
+        }
+        const double t1 = omp_get_wtime();
+        for (int c = 0; c < nvc; c++) root->vcycle();
+        const double t2 = omp_get_wtime();
+        printf("{\"mode\": \"sample_grav\", \"hydro_rk3_seconds\": %.6f, \"vcycles\": %d, \"vcycle_seconds\": %.6f, "
+               "\"leaf_cells\": %ld, \"bricks\": %d, \"threads\": %d}\n",
+               t1 - t0, nvc, (t2 - t1) / nvc, (long)root->get_zone_cnt(), root->get_node_cnt(),
+               omp_get_max_threads());
         return 0;
     }
     if (mode == "poisson") {
