@@ -99,6 +99,8 @@ def load_library(path=LIB_PATH):
             lib.amr_vcycle.argtypes = [P, dp]
             lib.amr_poisson_solve.argtypes = [P, D, I, dp, ip]
             lib.amr_grav_step.argtypes = [P, D, D, D, I]
+            lib.amr_graph_solve.argtypes = [P, D, I, dp, ip]
+            lib.amr_graph_grav_step.argtypes = [P, D, D, I, dp]
         _lib = lib
     return _lib
 
@@ -326,6 +328,19 @@ class AMR:
 
     def poisson_boundaries(self):
         self._check(self.lib.amr_poisson_boundaries(self.ctx))
+
+    def graph_solve(self, tol, max_cycles=1000):
+        e = ctypes.c_double()
+        n = ctypes.c_int()
+        self._check(self.lib.amr_graph_solve(self.ctx, float(tol), int(max_cycles), ctypes.byref(e),
+                                             ctypes.byref(n)))
+        return e.value, n.value
+
+    def graph_grav_step(self, tol, dynamic_range=1.0e6, step_index=0):
+        dt = ctypes.c_double()
+        self._check(self.lib.amr_graph_grav_step(self.ctx, float(tol), float(dynamic_range), int(step_index),
+                                                 ctypes.byref(dt)))
+        return dt.value
 
     def grav_step(self, dt, tol, dynamic_range=1.0e6, step_index=0):
         self._check(self.lib.amr_grav_step(self.ctx, float(dt), float(tol), float(dynamic_range),

@@ -261,6 +261,7 @@ int rebuild_topology(amr_ctx* c) {
     // host vectors may be rewritten before the async copies finish
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->topo_dirty = false;
+    c->topo_version++;  // captured graphs embed the slot lists: rebuild them
     return AMR_OK;
 }
 
@@ -484,6 +485,7 @@ int amr_destroy(amr_ctx* c) {
         for (void* p : ptrs)
             if (p) cudaFree(p);
         amr_poisson_release(c);
+        amr::graph_release(c);
         cudaStreamDestroy(c->stream);
     }
     delete c;

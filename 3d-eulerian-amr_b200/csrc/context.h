@@ -61,7 +61,9 @@ struct amr_ctx {
     int vcycle_max_outer = 1000;
     long long relax_calls = 0, relax_sweeps_total = 0;
     bool topo_dirty = true;
+    long long topo_version = 0;  // bumped by every rebuild_topology
     amr::Profiler prof;
+    struct GraphState* gs = nullptr;  // captured step/solve graphs (graph_host.cpp)
 
     amr_ctx(const amr::TreeParams& p) : tree(p) {}
 };
@@ -69,4 +71,5 @@ struct amr_ctx {
 namespace amr {
 int rebuild_topology(amr_ctx* c);
 int alloc_slot(amr_ctx* c);
+void graph_release(amr_ctx* c);
 }  // namespace amr

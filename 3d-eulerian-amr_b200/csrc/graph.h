@@ -1,0 +1,47 @@
+// Graph-captured step: device-side loop control and its kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "amr_internal.h"
+
+namespace amr {
+
+constexpr int MAX_LEVELS = 16;
+
+// Per-level brick lists in depth-first order (device pointers + counts).
+struct LevelLists {
+    const int* slots;  // packed lists
+    const int* all;    // all bricks, DFS order
+    int nall;
+    int off[MAX_LEVELS];
+    int cnt[MAX_LEVELS];
+};
+
+// Loop state shared between graph kernels and the host.
+struct Control {
+    double r0[MAX_LEVELS];  // first-pass residual of the current relaxation loop per level
+    int outer[MAX_LEVELS];  // relaxation passes in the current loop
+    double err;             // last L1 error of the solve loop
+    double dt, last_dt;     // CFL step of the graph-driven step
+    int cycles;             // V-cycles in the current solve
+    int max_cycles;
+    int max_outer;
+    int status;             // 0 ok, 1 relaxation loop cap, 2 V-cycle cap
+    long long relax_calls;
+    long long cycles_total;  // V-cycles since the context started
+    int steps;
+    int pad;
+};
+
+void launch_relax_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int level,
+                      int mode, double ratio, cudaGraphConditionalHandle cond, Control* ctl, double* pres,
+                      double* nest, unsigned int* counter, cudaStream_t s);
+void launch_error_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int nlevels,
+                      double tol, cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest,
+                      unsigned int* counter, cudaStream_t s);
+void launch_open_loop(cudaGraphConditionalHandle cond, Control* ctl, int reset_cycles, cudaStream_t s);
+void launch_dt_reduce(const BrickTable& bt, const LevelLists& L, int nlevels, const double* per, double* nest,
+                      Control* ctl, double maxdtinc, cudaStream_t s);
+
+}  // namespace amr

@@ -1,0 +1,471 @@
+// Graph-captured self-gravitating step.
+//
+// The whole RK3 step -- CFL step, store, three substeps of hydro + gravity
+// sources, each followed by a multigrid solve whose V-cycle loop and
+// relaxation loops are CUDA-graph WHILE nodes decided on the device -- is
+// captured once per topology and replayed every step; the graph is
+// re-instantiated only after a regrid changes the tree.  The kernels and the
+// order of every floating-point operation are those of the plain path, so
+// the graph form reproduces it bit for bit.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstddef>
+#include <functional>
+#include <string>
+#include <vector>
+
+#include "context.h"
+#include "graph.h"
+#include "kernels.h"
+#include "poisson.h"
+
+using namespace amr;
+
+#define CUDA_TRY(call)                                                                        \
+    do {                                                                                      \
+        cudaError_t e__ = (call);                                                             \
+        if (e__ != cudaSuccess) {                                                             \
+            c->err = std::string("CUDA error: ") + cudaGetErrorString(e__) + " at " + #call; \
+            return AMR_ERR_CUDA;                                                              \
+        }                                                                                     \
+    } while (0)
+
+#define TRY(x)                 \
+    do {                       \
+        int rc__ = (x);        \
+        if (rc__) return rc__; \
+    } while (0)
+
+struct GraphState {
+    Control* d_ctl = nullptr;
+    Control* h_ctl = nullptr;  // pinned mirror
+    double* d_nest = nullptr;
+    unsigned int* d_counter = nullptr;
+    int* h_steps = nullptr;     // pinned scalar staging
+    cudaGraphExec_t step_exec = nullptr;
+    long long step_version = -1;
+    double step_tol = -1.0;
+    cudaGraphExec_t solve_exec = nullptr;
+    long long solve_version = -1;
+    double solve_tol = -1.0;
+    int solve_max = -1;
+    std::vector<cudaStream_t> streams;  // capture streams of nested bodies
+    LevelLists L{};
+    // kernel nodes of the captured graphs: top level of the step / solve
+    // graph, one V-cycle body (outside its relaxation loops); a relaxation
+    // loop body holds 2 (ghost fill + relax)
+    long long k_step = 0, k_solve = 0, k_vbody = 0;
+    int nlevels_captured = 0;
+    long long last_cycles = 0, last_relax = 0;  // device counters at the last read
+};
+
+namespace {
+
+int ensure_state(amr_ctx* c) {
+    if (c->gs) return AMR_OK;
+    GraphState* g = new GraphState;
+    c->gs = g;
+    CUDA_TRY(cudaMalloc(&g->d_ctl, sizeof(Control)));
+    CUDA_TRY(cudaMemsetAsync(g->d_ctl, 0, sizeof(Control), c->stream));
+    CUDA_TRY(cudaMallocHost(&g->h_ctl, sizeof(Control)));
+    CUDA_TRY(cudaMallocHost(&g->h_steps, sizeof(int) * 4));
+    CUDA_TRY(cudaMalloc(&g->d_nest, sizeof(double) * c->cap));
+    CUDA_TRY(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
+    CUDA_TRY(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned int) * 4, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return AMR_OK;
+}
+
+int max_level_present(amr_ctx* c) {
+    int m = 0;
+    for (Node* n : c->order) m = std::max(m, n->level);
+    return m;
+}
+
+void fill_lists(amr_ctx* c) {
+    LevelLists& L = c->gs->L;
+    L.slots = c->d_slots;
+    L.all = c->d_slots + c->off_all[0];
+    L.nall = (int)c->all_slots.size();
+    for (int m = 0; m < MAX_LEVELS; m++) {
+        const bool ok = m < (int)c->level_slots.size();
+        L.off[m] = ok ? c->off_level[m] : 0;
+        L.cnt[m] = ok ? (int)c->level_slots[m].size() : 0;
+    }
+}
+
+cudaStream_t body_stream(amr_ctx* c, int depth) {
+    GraphState* g = c->gs;
+    while ((int)g->streams.size() <= depth) {
+        cudaStream_t s;
+        cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+        g->streams.push_back(s);
+    }
+    return g->streams[depth];
+}
+
+long long kernel_nodes(cudaGraph_t g);
+
+// At the current capture point of s: run pre(s, h), then add a WHILE node on
+// handle h whose body is captured from body(s2, h) on a side stream.
+int add_while(amr_ctx* c, cudaStream_t s, int depth, const std::function<int(cudaStream_t, cudaGraphConditionalHandle)>& pre,
+              const std::function<int(cudaStream_t, cudaGraphConditionalHandle)>& body,
+              long long* body_kernels = nullptr) {
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    CUDA_TRY(cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, &deps, &ndeps));
+    if (status != cudaStreamCaptureStatusActive) {
+        c->err = "add_while outside an active capture";
+        return AMR_ERR_STATE;
+    }
+    cudaGraphConditionalHandle h;
+    CUDA_TRY(cudaGraphConditionalHandleCreate(&h, graph, 0, 0));
+    TRY(pre(s, h));
+    CUDA_TRY(cudaStreamGetCaptureInfo(s, &status, nullptr, &graph, &deps, &ndeps));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = h;
+    p.conditional.type = cudaGraphCondTypeWhile;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CUDA_TRY(cudaGraphAddNode(&node, graph, deps, ndeps, &p));
+    cudaGraph_t bodyg = p.conditional.phGraph_out[0];
+    CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+    cudaStream_t s2 = body_stream(c, depth);
+    CUDA_TRY(cudaStreamBeginCaptureToGraph(s2, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    const int rc = body(s2, h);
+    cudaGraph_t out;
+    const cudaError_t e = cudaStreamEndCapture(s2, &out);
+    if (rc) return rc;
+    if (e != cudaSuccess) {
+        c->err = std::string("body capture failed: ") + cudaGetErrorString(e);
+        return AMR_ERR_CUDA;
+    }
+    if (body_kernels) *body_kernels = kernel_nodes(bodyg);
+    return AMR_OK;
+}
+
+long long kernel_nodes(cudaGraph_t g) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    cudaGraphGetNodes(g, nodes.data(), &n);
+    long long k = 0;
+    for (auto nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
+}
+
+int launched(amr_ctx* c) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        c->err = std::string("CUDA launch error: ") + cudaGetErrorString(e);
+        return AMR_ERR_CUDA;
+    }
+    return AMR_OK;
+}
+
+const int* lvl(amr_ctx* c, int l) { return c->d_slots + c->off_level[l]; }
+int nlvl(amr_ctx* c, int l) { return (int)c->level_slots[l].size(); }
+const int* all(amr_ctx* c) { return c->d_slots + c->off_all[0]; }
+int nall(amr_ctx* c) { return (int)c->all_slots.size(); }
+
+int rec_relax_until(amr_ctx* c, cudaStream_t s, int l, double ratio, int depth) {
+    GraphState* g = c->gs;
+    launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
+    return add_while(
+        c, s, depth,
+        [&](cudaStream_t q, cudaGraphConditionalHandle h) {
+            launch_relax_dev(c->geom, c->bt, c->st, g->L, l, 0, ratio, h, g->d_ctl, c->d_pres, g->d_nest,
+                             g->d_counter, q);
+            return launched(c);
+        },
+        [&](cudaStream_t q, cudaGraphConditionalHandle h) {
+            launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), q);
+            launch_relax_dev(c->geom, c->bt, c->st, g->L, l, 1, ratio, h, g->d_ctl, c->d_pres, g->d_nest,
+                             g->d_counter, q);
+            return launched(c);
+        });
+}
+
+int rec_forces(amr_ctx* c, cudaStream_t s) {
+    launch_forces(c->geom, c->bt, c->st, all(c), nall(c), s);
+    for (int l = c->tree.prm.max_level; l >= 0; l--) {
+        const int n = c->off_reflux[l + 1] - c->off_reflux[l];
+        launch_adjust_force(c->geom, c->st, c->d_reflux + c->off_reflux[l], n, s);
+    }
+    return launched(c);
+}
+
+// Poisson::vcycle (poisson.cpp:1069-1074) ending in the loop decision.
+int rec_vcycle(amr_ctx* c, cudaStream_t s, int depth, cudaGraphConditionalHandle hsolve, double tol) {
+    GraphState* g = c->gs;
+    const int maxlevel = max_level_present(c);
+    launch_set_source(c->geom, c->st, all(c), nall(c), s);
+    for (int l = maxlevel - 1; l >= 0; l--)
+        launch_phi_from_children(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l], (int)c->parent_slots[l].size(),
+                                 s);
+    for (int l = 0; l <= maxlevel; l++)
+        launch_phi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
+    launch_init_vcycle(c->geom, c->st, all(c), nall(c), s);
+    TRY(launched(c));
+    for (int l = maxlevel; l >= 0; l--) {
+        launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
+        launch_vdown_a(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
+        for (int dir = 0; dir < 3; dir++) {
+            const int a = c->off_reflux_dir[3 * l + dir], b = c->off_reflux_dir[3 * l + dir + 1];
+            launch_adjust_dphi(c->geom, c->bt, c->st, c->d_reflux + a, b - a, s);
+        }
+        launch_vdown_c(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
+        TRY(launched(c));
+        TRY(rec_relax_until(c, s, l, 1.0, depth));
+    }
+    for (int l = 0; l <= maxlevel; l++) {
+        launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
+        if (l > 0) launch_coarse_correction(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
+        TRY(launched(c));
+        TRY(rec_relax_until(c, s, l, 0.05, depth));
+        launch_retire(c->geom, c->st, lvl(c, l), nlvl(c, l), s);
+        launch_phi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
+    }
+    TRY(rec_forces(c, s));
+    launch_error_dev(c->geom, c->bt, c->st, g->L, maxlevel + 1, tol, hsolve, g->d_ctl, c->d_pres, g->d_nest,
+                     g->d_counter, s);
+    return launched(c);
+}
+
+// solve(): boundaries, forces, V-cycles while the L1 error > tol, restriction.
+int rec_solve(amr_ctx* c, cudaStream_t s, double tol, int depth) {
+    GraphState* g = c->gs;
+    launch_set_source(c->geom, c->st, all(c), nall(c), s);
+    launch_source_sums(c->geom, c->bt, c->st, all(c), nall(c), c->d_msrc, c->d_allref, s);
+    launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, all(c), nall(c), c->d_msrc, c->d_allref, c->d_bphi,
+                      s);
+    TRY(rec_forces(c, s));
+    TRY(add_while(
+        c, s, depth,
+        [&](cudaStream_t q, cudaGraphConditionalHandle h) {
+            launch_open_loop(h, g->d_ctl, 1, q);
+            return launched(c);
+        },
+        [&](cudaStream_t q, cudaGraphConditionalHandle h) { return rec_vcycle(c, q, depth + 1, h, tol); },
+        &g->k_vbody));
+    for (int l = c->tree.prm.max_level; l >= 0; l--)
+        launch_inject(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l], (int)c->parent_slots[l].size(), s);
+    return launched(c);
+}
+
+int rec_enforce_boundaries(amr_ctx* c, cudaStream_t s) {
+    for (int l = 0; l <= c->tree.prm.max_level; l++)
+        launch_ghost_fill(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
+    return launched(c);
+}
+
+int maxslot(amr_ctx* c) {
+    int m = 0;
+    for (int sl : c->all_slots) m = std::max(m, sl + 1);
+    return m;
+}
+
+// One RK3 step of the self-gravitating driver (binary_driver.cpp:346-459 on
+// the Euler state) with the CFL step reduced on the device.
+int rec_step(amr_ctx* c, cudaStream_t s, double tol) {
+    GraphState* g = c->gs;
+    double* dtp = &g->d_ctl->dt;
+    launch_max_dt(c->geom, c->st, all(c), nall(c), c->bt.h, c->d_dt, s);
+    launch_dt_reduce(c->bt, g->L, max_level_present(c) + 1, c->d_dt, g->d_nest, g->d_ctl, c->cfg.maxdtinc, s);
+    CUDA_TRY(cudaMemcpyAsync(c->st.U0, c->st.U, sizeof(double) * (size_t)maxslot(c) * c->geom.ucount,
+                             cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(c->d_fo + c->geom.nf, c->d_fo, sizeof(double) * c->geom.nf, cudaMemcpyDeviceToDevice, s));
+    const double betas[3] = {1.0, 0.25, 2.0 / 3.0};
+    for (int rk = 0; rk < 3; rk++) {
+        TRY(rec_enforce_boundaries(c, s));
+        launch_flux(c->geom, c->st, all(c), nall(c), s);
+        for (int l = c->tree.prm.max_level; l >= 0; l--) {
+            const int n = c->off_reflux[l + 1] - c->off_reflux[l];
+            launch_reflux(c->geom, c->st, c->d_reflux + c->off_reflux[l], n, s);
+        }
+        launch_flow_off(c->geom, c->st, c->tree.root()->slot, c->tree.root()->h, 0.0, betas[rk], c->d_fo, s, dtp);
+        launch_add_difs(c->geom, c->st, all(c), nall(c), c->bt.h, 0.0, betas[rk], 1, s, dtp);
+        launch_phi_time(c->geom, c->st, all(c), nall(c), rk == 0 ? 0 : (rk == 1 ? 2 : 1), s);
+        TRY(launched(c));
+        TRY(rec_solve(c, s, tol, 0));
+    }
+    return rec_enforce_boundaries(c, s);
+}
+
+int capture(amr_ctx* c, const std::function<int(cudaStream_t)>& rec, cudaGraphExec_t* exec, long long* kernels) {
+    if (*exec) {
+        cudaGraphExecDestroy(*exec);
+        *exec = nullptr;
+    }
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    const int rc = rec(c->stream);
+    cudaGraph_t graph;
+    const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    if (rc) {
+        if (e == cudaSuccess) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) {
+        c->err = std::string("capture failed: ") + cudaGetErrorString(e);
+        return AMR_ERR_CUDA;
+    }
+    *kernels = kernel_nodes(graph);
+    const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess) {
+        c->err = std::string("graph instantiation failed: ") + cudaGetErrorString(ei);
+        *exec = nullptr;
+        return AMR_ERR_CUDA;
+    }
+    return AMR_OK;
+}
+
+int set_limits(amr_ctx* c, int max_cycles, int steps) {
+    GraphState* g = c->gs;
+    int* hs = g->h_steps;
+    hs[0] = max_cycles;
+    hs[1] = c->vcycle_max_outer;
+    hs[2] = 0;
+    hs[3] = steps;
+    CUDA_TRY(cudaMemcpyAsync(&g->d_ctl->max_cycles, &hs[0], sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(&g->d_ctl->max_outer, &hs[1], sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(&g->d_ctl->status, &hs[2], sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    if (steps >= 0)
+        CUDA_TRY(cudaMemcpyAsync(&g->d_ctl->steps, &hs[3], sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    return AMR_OK;
+}
+
+int read_ctl(amr_ctx* c) {
+    GraphState* g = c->gs;
+    CUDA_TRY(cudaMemcpyAsync(g->h_ctl, g->d_ctl, sizeof(Control), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return AMR_OK;
+}
+
+// Kernels executed by the replay just read back: the graph's top-level kernel
+// nodes, one V-cycle body per V-cycle, two kernels per relaxation pass beyond
+// the first of each loop (the first is part of the V-cycle body).
+void count_replay(amr_ctx* c, long long top_kernels) {
+    GraphState* g = c->gs;
+    const long long dc = g->h_ctl->cycles_total - g->last_cycles;
+    const long long dr = g->h_ctl->relax_calls - g->last_relax;
+    const long long loops = dr - dc * 2LL * g->nlevels_captured;
+    c->prof.kernels += top_kernels + dc * g->k_vbody + 2LL * loops;
+    c->relax_calls += dr;
+    g->last_cycles = g->h_ctl->cycles_total;
+    g->last_relax = g->h_ctl->relax_calls;
+}
+
+int need(amr_ctx* c) {
+    if (!c) return AMR_ERR_ARG;
+    if (!c->has_device) return AMR_ERR_NODEVICE;
+    if (c->cfg.physics != AMR_PHYSICS_EULER_GRAVITY) {
+        c->err = "graph step needs AMR_PHYSICS_EULER_GRAVITY";
+        return AMR_ERR_ARG;
+    }
+    if (c->geom.nx != 8) {
+        c->err = "graph step built for nx == 8";
+        return AMR_ERR_ARG;
+    }
+    TRY(amr_poisson_set_source(c));  // allocates the Poisson scratch on first use
+    TRY(ensure_state(c));
+    return AMR_OK;
+}
+
+}  // namespace
+
+namespace amr {
+void graph_release(amr_ctx* c) {
+    GraphState* g = c->gs;
+    if (!g) return;
+    if (g->step_exec) cudaGraphExecDestroy(g->step_exec);
+    if (g->solve_exec) cudaGraphExecDestroy(g->solve_exec);
+    for (cudaStream_t s : g->streams) cudaStreamDestroy(s);
+    if (g->d_ctl) cudaFree(g->d_ctl);
+    if (g->h_ctl) cudaFreeHost(g->h_ctl);
+    if (g->h_steps) cudaFreeHost(g->h_steps);
+    if (g->d_nest) cudaFree(g->d_nest);
+    if (g->d_counter) cudaFree(g->d_counter);
+    delete g;
+    c->gs = nullptr;
+}
+}  // namespace amr
+
+extern "C" {
+
+// The Poisson solve as one graph launch (see amr_poisson_solve).
+int amr_graph_solve(amr_ctx* c, double tol, int max_cycles, double* l1_error, int* cycles) {
+    TRY(need(c));
+    GraphState* g = c->gs;
+    if (!g->solve_exec || g->solve_version != c->topo_version || g->solve_tol != tol) {
+        fill_lists(c);
+        TRY(capture(c, [&](cudaStream_t s) { return rec_solve(c, s, tol, 0); }, &g->solve_exec, &g->k_solve));
+        g->solve_version = c->topo_version;
+        g->solve_tol = tol;
+        g->nlevels_captured = max_level_present(c) + 1;
+    }
+    TRY(set_limits(c, max_cycles, -1));
+    CUDA_TRY(cudaGraphLaunch(g->solve_exec, c->stream));
+    TRY(read_ctl(c));
+    count_replay(c, g->k_solve);
+    if (l1_error) *l1_error = g->h_ctl->err;
+    if (cycles) *cycles = g->h_ctl->cycles;
+    if (g->h_ctl->status) {
+        c->err = g->h_ctl->status == 2 ? "Poisson solve exceeded max_cycles" : "relaxation loop exceeded its cap";
+        return AMR_ERR_NOCONVERGE;
+    }
+    return AMR_OK;
+}
+
+// amr_grav_step with the whole RK3 step replayed from a captured graph and
+// the CFL step (GridNode::max_dt + MAXDTINC clamp against the previous
+// graph step) formed on the device.  step_index 0 starts the clamp afresh.
+int amr_graph_grav_step(amr_ctx* c, double tol, double dynamic_range, int step_index, double* dt_out) {
+    TRY(need(c));
+    GraphState* g = c->gs;
+    const int max_cycles = 10000;
+    if (step_index <= 0) {
+        TRY(amr_graph_solve(c, tol, max_cycles, nullptr, nullptr));
+        TRY(amr_store_phi(c));
+    }
+    if (!g->step_exec || g->step_version != c->topo_version || g->step_tol != tol) {
+        fill_lists(c);
+        TRY(capture(c, [&](cudaStream_t s) { return rec_step(c, s, tol); }, &g->step_exec, &g->k_step));
+        g->step_version = c->topo_version;
+        g->step_tol = tol;
+        g->nlevels_captured = max_level_present(c) + 1;
+    }
+    TRY(set_limits(c, max_cycles, step_index <= 0 ? 0 : -1));
+    CUDA_TRY(cudaGraphLaunch(g->step_exec, c->stream));
+    TRY(read_ctl(c));
+    count_replay(c, g->k_step);
+    if (g->h_ctl->status) {
+        c->err = "solve inside the captured step did not converge";
+        return AMR_ERR_NOCONVERGE;
+    }
+    const double dt = g->h_ctl->dt;
+    for (Node* n : c->order) n->age += 3;  // three add_difs calls
+    if (step_index % 8 == 0) {
+        double smax;
+        TRY(amr_state_max(c, 0, &smax));
+        int changed = 0;
+        TRY(amr_check_for_refine(c, smax / dynamic_range, 1, &changed));
+        if (changed) {
+            TRY(amr_graph_solve(c, tol / 10.0, max_cycles, nullptr, nullptr));
+            TRY(amr_store_phi(c));
+        }
+    }
+    TRY(amr_set_time(c, c->time + dt));
+    if (dt_out) *dt_out = dt;
+    return AMR_OK;
+}
+
+}  // extern "C"

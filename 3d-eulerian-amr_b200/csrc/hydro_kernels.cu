@@ -222,10 +222,11 @@ __global__ void k_reflux(Geom g, DevState st, const RefluxItem* __restrict__ ite
 // Block = one brick, thread per interior cell.
 // ---------------------------------------------------------------------------
 __global__ void k_add_difs(Geom g, DevState st, const int* __restrict__ slots, const double* __restrict__ hs,
-                           double dt, double beta, int gravity) {
+                           double dt_arg, const double* __restrict__ dtp, double beta, int gravity) {
     const int b = slots[blockIdx.x];
     const int nx = g.nx, gnx = g.gnx, bw = g.bw, pnx = g.pnx;
     const int npen = nx * nx, fstride = npen * (nx + 1);
+    const double dt = dtp ? *dtp : dt_arg;  // device-computed step in captured graphs
     const double h = hs[b];
     const double hinv = 1.0 / h;
     for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
@@ -288,8 +289,10 @@ __global__ void k_add_difs(Geom g, DevState st, const int* __restrict__ slots, c
 // Root flow-off: Grid::sum_{x,y,z}_flow_off (grid.cpp:346-404) in the
 // sequential order of a one-thread OpenMP run, then FO update of
 // Grid::add_difs (grid.cpp:419).  fo = [FO(nf), FO0(nf)].  One thread/field.
-__global__ void k_flow_off(Geom g, DevState st, int root, double h, double dt, double beta, double* fo) {
+__global__ void k_flow_off(Geom g, DevState st, int root, double h, double dt_arg, const double* __restrict__ dtp,
+                           double beta, double* fo) {
     const int l = threadIdx.x;
+    const double dt = dtp ? *dtp : dt_arg;
     if (l >= g.nf) return;
     const int nx = g.nx, npen = nx * nx, fstride = npen * (nx + 1);
     const double* Fx = st.Fx + (size_t)root * g.nf * fstride + l * fstride;
@@ -535,13 +538,13 @@ void launch_reflux(const Geom& g, const DevState& st, const RefluxItem* items, i
     k_reflux<<<n, ((g.nf * half * half + 31) / 32) * 32, 0, s>>>(g, st, items);
 }
 void launch_add_difs(const Geom& g, const DevState& st, const int* slots, int n, const double* hs, double dt,
-                     double beta, int gravity, cudaStream_t s) {
+                     double beta, int gravity, cudaStream_t s, const double* dtp) {
     if (n <= 0) return;
-    k_add_difs<<<n, 256, 0, s>>>(g, st, slots, hs, dt, beta, gravity);
+    k_add_difs<<<n, 256, 0, s>>>(g, st, slots, hs, dt, dtp, beta, gravity);
 }
 void launch_flow_off(const Geom& g, const DevState& st, int root, double h, double dt, double beta, double* fo,
-                     cudaStream_t s) {
-    k_flow_off<<<1, 32, 0, s>>>(g, st, root, h, dt, beta, fo);
+                     cudaStream_t s, const double* dtp) {
+    k_flow_off<<<1, 32, 0, s>>>(g, st, root, h, dt, dtp, beta, fo);
 }
 void launch_inject(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                    cudaStream_t s) {

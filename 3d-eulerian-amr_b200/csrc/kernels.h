@@ -12,10 +12,11 @@ void launch_ghost_fill(const Geom& g, const BrickTable& bt, const DevState& st, 
                        cudaStream_t s);
 void launch_flux(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);
 void launch_reflux(const Geom& g, const DevState& st, const RefluxItem* items, int n, cudaStream_t s);
+// dtp: when non-null the step is read from device memory (captured graphs)
 void launch_add_difs(const Geom& g, const DevState& st, const int* slots, int n, const double* hs, double dt,
-                     double beta, int gravity, cudaStream_t s);
+                     double beta, int gravity, cudaStream_t s, const double* dtp = nullptr);
 void launch_flow_off(const Geom& g, const DevState& st, int root, double h, double dt, double beta, double* fo,
-                     cudaStream_t s);
+                     cudaStream_t s, const double* dtp = nullptr);
 void launch_inject(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                    cudaStream_t s);
 void launch_prolong(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,

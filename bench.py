@@ -120,25 +120,29 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
-def run_reference_sample(levels, threads, nvc=1):
+def run_reference_steps(levels, threads, warm, steps, timeout=3000):
     """The reference's own CPU code (oracle/_ref, built from the reference
-    sources): one RK3 hydro step with gravity sources and nvc V-cycles on the
-    same tree, timed separately."""
+    sources, g++ -O2 -fopenmp) on the same workload: `warm` untimed RK3 steps
+    (the first includes the initial solve from phi = 0), then `steps` timed
+    steps.  Returns per-step seconds, leaf cells and bricks."""
     exe = os.path.join(ROOT, "oracle", "_ref", "g05_harness")
     if not os.path.exists(exe):
         return None
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-    r = subprocess.run([exe, "sample_grav", "polytrope", str(levels), str(nvc)], env=env, capture_output=True,
-                       text=True, timeout=1800)
+    try:
+        r = subprocess.run([exe, "time_grav", "polytrope", str(levels), str(warm + steps), str(TOL), "-"],
+                           env=env, capture_output=True, text=True, timeout=timeout)
+    except subprocess.TimeoutExpired:
+        return None
     if r.returncode != 0:
         return None
-    return json.loads(r.stdout.strip().splitlines()[-1])
-
-
-# V-cycles per RK3 step of this workload in the reference itself: measured by
-# running the reference (oracle/_ref, time_grav polytrope 4 ... 1e-6) for
-# full steps; used to turn the bounded per-component CPU sample into a step.
-REF_VCYCLES_PER_STEP = None
+    rows = [json.loads(x) for x in r.stdout.strip().splitlines() if x.startswith("{")]
+    per = [x for x in rows if "step" in x]
+    summ = [x for x in rows if x.get("mode") == "grav"][-1]
+    timed = per[warm:]
+    return {"seconds": [x["seconds"] for x in timed], "vcycles": [x["vcycles"] for x in timed],
+            "leaf_cells": [x.get("leaf_cells", summ["leaf_cells"]) for x in timed],
+            "bricks": summ["bricks"], "threads": summ["threads"]}
 
 
 def reference_arm(args):
@@ -146,21 +150,21 @@ def reference_arm(args):
     if rank != 0:
         return 0
     threads = os.cpu_count() or 1
-    s = run_reference_sample(LEVELS, threads)
-    if s is None:
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/g05_harness missing or failed"}))
+    warm = max(1, args.warmup)
+    s = run_reference_steps(LEVELS, threads, warm, args.steps)
+    if s is None or not s["seconds"]:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/g05_harness missing, failed or timed out"}))
         return 0
-    nvc = REF_VCYCLES_PER_STEP or args.ref_vcycles
-    t_step = s["hydro_rk3_seconds"] + nvc * s["vcycle_seconds"]
-    value = s["leaf_cells"] / t_step
-    sample = ("one RK3 hydro step with gravity sources plus one V-cycle of the reference (oracle/_ref, "
-              "g++ -O2 -fopenmp) on the full %d-brick tree; step time = t_hydro + %.2f V-cycles x t_vcycle "
-              "(V-cycles per step of this workload)" % (s["bricks"], nvc))
+    t = sum(s["seconds"])
+    value = sum(s["leaf_cells"]) / t
+    sample = ("reference CPU code (oracle/_ref, g++ -O2 -fopenmp, %d threads): %d full RK3 steps after %d "
+              "untimed (the first solves from phi = 0), %d bricks, %.1f V-cycles/step" %
+              (s["threads"], len(s["seconds"]), warm, s["bricks"], sum(s["vcycles"]) / len(s["vcycles"])))
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_step, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "levels": LEVELS, "bricks": s["bricks"], "leaf_cells": s["leaf_cells"]},
+        "steps": len(s["seconds"]), "warmup": warm, "ms_per_step": 1000.0 * t / len(s["seconds"]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "levels": LEVELS, "bricks": s["bricks"]},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": s["threads"], "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -169,67 +173,46 @@ def reference_arm(args):
     return 0
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--ref-vcycles", type=float, default=15.0)
-    ap.add_argument("--json-out", default=None)
-    args = ap.parse_args()
-    if args.impl == "reference":
-        return reference_arm(args)
+def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile=False):
+    """Build the workload and time K steps of one form of our path.
 
-    import numpy as np
-    import torch
-    import torch.distributed as dist
-
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=torch.device("cuda", local))
-
-    amr, ini = load_amr()
+    form: "fp64"  plain FP64, host-orchestrated (reference operation order)
+          "graph" FP64, whole RK3 step replayed from a captured CUDA graph with
+                  every loop decided on the device (bitwise equal to fp64)
+    """
     a = amr.AMR(physics=amr.PHYSICS_EULER_GRAVITY, max_refine_level=LEVELS, grid_dim=0.5, z_reflect=0,
-                max_bricks=8192, precision=amr.PREC_MIXED if args.form == "mixed" else amr.PREC_FP64)
+                max_bricks=8192, precision=amr.PREC_FP64)
     ini.build_tree(a, "polytrope", 1.0e-6, 0.5, 0, LEVELS, device=True)
     stream = torch.cuda.ExternalStream(a.stream_handle())
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    state = {"step": 0, "last_dt": 0.0}
+
+    def one_step():
+        st = state["step"]
+        if form == "fp64":
+            dt = a.max_dt()
+            if st > 0:
+                dt = min(1.25 * state["last_dt"], dt)
+            state["last_dt"] = dt
+            a.grav_step(dt, TOL, DYNAMIC_RANGE, st)
+        else:
+            a.graph_grav_step(TOL, DYNAMIC_RANGE, st)
+        state["step"] = st + 1
 
     def barrier():
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
 
-    step = 0
-    last_dt = 0.0
-
-    def one_step():
-        nonlocal step, last_dt
-        dt = a.max_dt()
-        if step > 0:
-            dt = min(1.25 * last_dt, dt)
-        last_dt = dt
-        a.grav_step(dt, TOL, DYNAMIC_RANGE, step)
-        step += 1
-
     for _ in range(args.warmup):
         one_step()
+    res = {"form": form}
     st0 = a.stats()
     k0 = a.launch_count()
     sampler = ClockSampler(local)
     barrier()
     sampler.start()
-    times = []
-    cells = 0
+    times, cells = [], 0
     for _ in range(args.steps):
         with torch.cuda.stream(stream):
             flush.zero_()  # L2 flush between timed steps, outside the timed interval
@@ -243,112 +226,150 @@ def main():
         times.append(ev0.elapsed_time(ev1))
         cells += n_cells
     barrier()
-    clocks = sampler.stop()
+    res["clocks"] = sampler.stop()
     st1 = a.stats()
-    gpu_launches = a.launch_count() - k0
-    total_ms = sum(times)
-    t = torch.tensor([total_ms, float(cells)], dtype=torch.float64, device="cuda")
+    res["gpu_launches"] = a.launch_count() - k0
+    t = torch.tensor([sum(times), float(cells)], dtype=torch.float64, device="cuda")
     if world > 1:
-        tmax = t.clone()
-        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(tmax[1:2], op=dist.ReduceOp.SUM)
-        t = tmax
-    total_ms, all_cells = float(t[0]), float(t[1])
-    value = all_cells / (total_ms / 1000.0)
+        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
+    res["ms_total"], res["cells"] = float(t[0]), float(t[1])
+    res["value"] = res["cells"] / (res["ms_total"] / 1000.0)
+    res["ms_per_step"] = res["ms_total"] / args.steps
+    res["bricks"] = a.nbricks
+    res["relax_calls_per_step"] = (st1["relax_calls"] - st0["relax_calls"]) / args.steps
 
-    # end to end through the public API: host state in pinned memory is
-    # uploaded, stepped, and read back every step
-    e2e = None
-    if not args.no_e2e:
+    if e2e:
+        # end to end through the public API: the state lives in pinned host
+        # memory, is uploaded, stepped and read back every step
         cap = 8192 * a.nf * a.gnx ** 3
         hbuf = torch.empty(cap, dtype=torch.float64, pin_memory=True)
         U = a.download_state()
-        nb = U.size
-        hbuf[:nb].copy_(torch.from_numpy(U.reshape(-1)))
+        hbuf[:U.size].copy_(torch.from_numpy(U.reshape(-1)))
+        ptr = ctypes.cast(hbuf.data_ptr(), ctypes.POINTER(ctypes.c_double))
         barrier()
         e_times, e_cells, h2d, d2h = [], 0, 0, 0
         for _ in range(args.steps):
             ev0 = torch.cuda.Event(enable_timing=True)
             ev1 = torch.cuda.Event(enable_timing=True)
-            n = a.nbricks * a.nf * a.gnx ** 3
-            ptr = ctypes.cast(hbuf.data_ptr(), ctypes.POINTER(ctypes.c_double))
+            n_in = a.nbricks * a.nf * a.gnx ** 3
             e_cells += a.get_zone_cnt()
             ev0.record(stream)
             a._check(a.lib.amr_upload_state(a.ctx, ptr))
             one_step()
-            n2 = a.nbricks * a.nf * a.gnx ** 3
+            n_out = a.nbricks * a.nf * a.gnx ** 3
             a._check(a.lib.amr_download_state(a.ctx, ptr))
             ev1.record(stream)
             ev1.synchronize()
             e_times.append(ev0.elapsed_time(ev1))
-            h2d += 8 * n
-            d2h += 8 * n2
+            h2d += 8 * n_in
+            d2h += 8 * n_out
         barrier()
         et = torch.tensor([sum(e_times), float(e_cells)], dtype=torch.float64, device="cuda")
         if world > 1:
             dist.all_reduce(et[0:1], op=dist.ReduceOp.MAX)
             dist.all_reduce(et[1:2], op=dist.ReduceOp.SUM)
-        e2e = {"value": float(et[1]) / (float(et[0]) / 1000.0), "unit": UNIT,
-               "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
+        res["e2e"] = {"value": float(et[1]) / (float(et[0]) / 1000.0), "unit": UNIT,
+                      "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
 
-    # per-kernel-class device time over two profiled steps (separate pass)
-    a.profile(True)
-    a.profile_reset()
-    for _ in range(2):
-        one_step()
-    a.synchronize()
-    prof = a.profile_get()
-    a.profile(False)
+    if profile:
+        # per-kernel-class device time over two profiled steps of the plain
+        # launch sequence (event brackets need host-issued launches)
+        a.profile(True)
+        a.profile_reset()
+        for _ in range(2):
+            dt = a.max_dt()
+            a.grav_step(min(dt, 1.25 * state["last_dt"]) if state["last_dt"] > 0 else dt, TOL, DYNAMIC_RANGE,
+                        state["step"])
+            state["step"] += 1
+        a.synchronize()
+        res["profile"] = a.profile_get()
+        a.profile(False)
+    a.close()
+    return res
+
+
+def roofline_of(prof):
     known = {k: v for k, v in prof.items() if k in BYTES_PER_BRICK and v["launches"] > 0}
     dom = max(prof.items(), key=lambda kv: kv[1]["ms"])[0]
     peak, peak_kind = peaks()
-    roof_name = dom if dom in known else max(known.items(), key=lambda kv: kv[1]["ms"])[0]
-    pr = prof[roof_name]
-    bytes_per_launch = BYTES_PER_BRICK[roof_name] * pr["units"] / pr["launches"]
+    name = dom if dom in known else max(known.items(), key=lambda kv: kv[1]["ms"])[0]
+    pr = prof[name]
+    bytes_per_launch = BYTES_PER_BRICK[name] * pr["units"] / pr["launches"]
     ms_per_launch = pr["ms"] / pr["launches"]
     achieved = bytes_per_launch / (ms_per_launch * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            traffic = json.load(f).get(args.form, {}).get(roof_name)
-    roofline = {"bound": "hbm", "kernel": roof_name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
-                "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": ms_per_launch,
-                "dominant_class": dom,
-                "class_share": {k: round(v["ms"] / max(1e-9, sum(x["ms"] for x in prof.values())), 4)
-                                for k, v in prof.items() if v["ms"] > 0}}
+            traffic = json.load(f).get(name)
+    total = sum(x["ms"] for x in prof.values())
+    return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+            "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": ms_per_launch,
+            "dominant_class": dom,
+            "class_share": {k: round(v["ms"] / max(total, 1e-9), 4) for k, v in prof.items() if v["ms"] > 0}}
 
-    vcycles_per_step = None
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--form", default="graph", choices=["fp64", "graph"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--json-out", default=None)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    amr, ini = load_amr()
+    head = run_form(amr, ini, args.form, args, world, local, torch, dist, e2e=True, profile=True)
+    plain = None
+    if not args.no_compare and args.form != "fp64":
+        plain = run_form(amr, ini, "fp64", args, world, local, torch, dist)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        s = run_reference_sample(LEVELS, threads)
-        if s is not None:
-            nvc = REF_VCYCLES_PER_STEP or args.ref_vcycles
-            t_step = s["hydro_rk3_seconds"] + nvc * s["vcycle_seconds"]
-            cpu = {"value": s["leaf_cells"] / t_step, "unit": UNIT, "cores": s["threads"], "kind": "reference",
-                   "sample": "reference CPU code (oracle/_ref): one RK3 hydro step + one V-cycle on the full "
-                             "%d-brick tree, step = t_hydro + %.2f x t_vcycle" % (s["bricks"], nvc)}
+        s = run_reference_steps(LEVELS, threads, 1, 1, timeout=1200)
+        if s is not None and s["seconds"]:
+            cpu = {"value": sum(s["leaf_cells"]) / sum(s["seconds"]), "unit": UNIT, "cores": s["threads"],
+                   "kind": "reference",
+                   "sample": "reference CPU code (oracle/_ref): one full RK3 step of this workload after one "
+                             "untimed step (which solves from phi = 0), %d bricks, %d V-cycles" %
+                             (s["bricks"], s["vcycles"][0])}
     if rank == 0:
         out = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.form == "fp64" else "f32+f64",
-            "data": "synthetic",
-            "config": {"workload": WORKLOAD, "form": args.form, "levels": LEVELS, "bricks": a.nbricks,
-                       "leaf_cells_per_step": all_cells / args.steps / world, "tol_l1": TOL,
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "form": args.form, "levels": LEVELS, "bricks": head["bricks"],
+                       "leaf_cells_per_step": head["cells"] / args.steps / world, "tol_l1": TOL,
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
-            "relax_calls_per_step": (st1["relax_calls"] - st0["relax_calls"]) / args.steps,
-            "gpu_launches": gpu_launches,
+            "roofline": roofline_of(head["profile"]), "cpu_baseline": cpu, "e2e": head.get("e2e"),
+            "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
+            "relax_calls_per_step": head["relax_calls_per_step"],
+            "fp64_plain": None if plain is None else {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
+                                                       "gpu_launches": plain["gpu_launches"]},
         }
         line = json.dumps(out)
         print(line)
         if args.json_out:
             with open(args.json_out, "w") as f:
                 f.write(line + "\n")
-    a.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

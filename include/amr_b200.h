@@ -155,6 +155,17 @@ int amr_restore_half_phi(amr_ctx* ctx);                    /* poisson.cpp:200-22
  * regrid every 8 steps at state_max/dynamic_range. */
 int amr_grav_step(amr_ctx* ctx, double dt, double tol, double dynamic_range, int step_index);
 
+/* ---- graph-captured forms --------------------------------------------------
+ * The same step and solve with every loop decided on the device: the V-cycle
+ * loop and the relaxation loops are CUDA-graph WHILE nodes, the CFL step is
+ * reduced on the device, and the captured graph is replayed each step and
+ * re-instantiated only when a regrid changes the tree.  Results are those of
+ * amr_poisson_solve / amr_grav_step to the last bit. */
+int amr_graph_solve(amr_ctx* ctx, double tol, int max_cycles, double* l1_error, int* cycles);
+/* dt = GridNode::max_dt clamped to MAXDTINC x the previous step's (no clamp
+ * when step_index == 0); *dt_out receives it. */
+int amr_graph_grav_step(amr_ctx* ctx, double tol, double dynamic_range, int step_index, double* dt_out);
+
 /* ---- instrumentation ------------------------------------------------------
  * The reference times steps with omp_get_wtime (binary_driver.cpp:115,303);
  * here device time per kernel class comes from CUDA events on the context

@@ -528,6 +528,7 @@ int main(int argc, char* argv[]) {
             dts.push_back(dt);
             const double ts = omp_get_wtime();
             const size_t nv0 = drv.vcycle_errors.size();
+            const long leaf_before = (long)root->get_zone_cnt();
             drv.step(dt, tol);
             step_secs.push_back(omp_get_wtime() - ts);
             int cyc = 0;
@@ -535,8 +536,8 @@ int main(int argc, char* argv[]) {
                 if (drv.vcycle_errors[q] >= 0.0) cyc++;
             step_cycles.push_back(cyc);
             if (mode == "time_grav") {
-                printf("{\"step\": %d, \"seconds\": %.6f, \"vcycles\": %d, \"bricks\": %d}\n", s, step_secs.back(),
-                       cyc, root->get_node_cnt());
+                printf("{\"step\": %d, \"seconds\": %.6f, \"vcycles\": %d, \"bricks\": %d, \"leaf_cells\": %ld}\n", s,
+                       step_secs.back(), cyc, root->get_node_cnt(), leaf_before);
                 fflush(stdout);
             }
         }

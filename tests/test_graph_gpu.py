@@ -1,0 +1,81 @@
+"""The graph-captured forms reproduce the plain forms bit for bit.
+
+amr_graph_solve / amr_graph_grav_step run the same kernels as
+amr_poisson_solve / amr_grav_step, with the loop decisions (relaxation
+ratios, the L1 error test, the CFL step) taken on the device from the same
+nested sums; every array must come out identical.
+"""
+
+import numpy as np
+import pytest
+
+from cases import VARIANTS, load_golden, same_tree
+
+
+def make(gpu, maxlevel):
+    return gpu.AMR(max_refine_level=maxlevel, max_bricks=2048, physics=gpu.PHYSICS_EULER_GRAVITY,
+                   **VARIANTS["g05"])
+
+
+def load_state(a, g):
+    a.load_tree(g["init_level"], g["init_loc"], g["init_age"])
+    U = np.zeros((a.nbricks, a.nf, a.gnx, a.gnx, a.gnx))
+    U[:, :, 2:-2, 2:-2, 2:-2] = g["init_U"]
+    a.upload_state(U)
+    a.enforce_boundaries()
+
+
+@pytest.mark.gpu
+def test_graph_solve_is_bitwise_plain(gpu):
+    g = load_golden("poisson_poly_L2")
+    a, b = make(gpu, 2), make(gpu, 2)
+    load_state(a, g)
+    load_state(b, g)
+    ea, na = a.poisson_solve(1.0e-7)
+    eb, nb = b.graph_solve(1.0e-7)
+    assert na == nb and ea == eb
+    assert np.array_equal(a.download_poisson(), b.download_poisson())
+    assert np.array_equal(a.download_state(), b.download_state())
+    # a second solve on the same graph (replay) from the converged state
+    ea, na = a.poisson_solve(1.0e-9)
+    eb, nb = b.graph_solve(1.0e-9)
+    assert na == nb and ea == eb
+    assert np.array_equal(a.download_poisson()[0], b.download_poisson()[0])
+
+
+@pytest.mark.gpu
+def test_graph_grav_steps_are_bitwise_plain(gpu):
+    g = load_golden("grav_poly_L2")
+    a, b = make(gpu, 2), make(gpu, 2)
+    load_state(a, g)
+    load_state(b, g)
+    last = 0.0
+    for s in range(int(g["args"][2]) + 6):  # through a regrid at step 8
+        dt = a.max_dt()
+        if s > 0:
+            dt = min(1.25 * last, dt)
+        last = dt
+        a.grav_step(dt, 1.0e-6, 1.0e6, s)
+        dtb = b.graph_grav_step(1.0e-6, 1.0e6, s)
+        assert dtb == dt, (s, dt, dtb)
+        ta, tb = a.get_tree(), b.get_tree()
+        assert np.array_equal(ta["loc"], tb["loc"]) and np.array_equal(ta["age"], tb["age"])
+    assert np.array_equal(a.download_state(), b.download_state())
+    assert np.array_equal(a.download_poisson()[0], b.download_poisson()[0])
+    np.testing.assert_array_equal(a.flow_off(), b.flow_off())
+
+
+@pytest.mark.gpu
+def test_graph_steps_match_reference(gpu):
+    """The reference's 3-step coupled run, replayed through the graph form."""
+    g = load_golden("grav_poly_L2")
+    a = make(gpu, 2)
+    load_state(a, g)
+    dts = [a.graph_grav_step(1.0e-6, 1.0e6, s) for s in range(3)]
+    n = int(g["extra"][0])
+    np.testing.assert_allclose(dts, g["extra"][1:1 + n], rtol=1e-13)
+    assert same_tree(a.get_tree(), g, "final_")
+    U = a.download_state()[:, :, 2:-2, 2:-2, 2:-2]
+    s = U.reshape(U.shape[0], U.shape[1], -1).sum(axis=2)
+    rel = np.abs(s - g["final_Usum"]) / np.maximum(g["final_Uabs"], 1e-300)
+    assert rel.max() <= 1e-11
