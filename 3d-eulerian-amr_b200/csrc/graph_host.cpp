@@ -58,6 +58,11 @@ struct GraphState {
     long long k_step = 0, k_solve = 0, k_vbody = 0;
     int nlevels_captured = 0;
     long long last_cycles = 0, last_relax = 0;  // device counters at the last read
+    struct PendingCount {
+        cudaGraph_t body;
+        long long* out;
+    };
+    std::vector<PendingCount> pending_counts;
 };
 
 namespace {
@@ -144,7 +149,8 @@ int add_while(amr_ctx* c, cudaStream_t s, int depth, const std::function<int(cud
         c->err = std::string("body capture failed: ") + cudaGetErrorString(e);
         return AMR_ERR_CUDA;
     }
-    if (body_kernels) *body_kernels = kernel_nodes(bodyg);
+    // body graphs may only be inspected once the enclosing capture has ended
+    if (body_kernels) c->gs->pending_counts.push_back({bodyg, body_kernels});
     return AMR_OK;
 }
 
@@ -161,10 +167,10 @@ long long kernel_nodes(cudaGraph_t g) {
     return k;
 }
 
-int launched(amr_ctx* c) {
+int launched(amr_ctx* c, int line) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
-        c->err = std::string("CUDA launch error: ") + cudaGetErrorString(e);
+        c->err = std::string("CUDA launch error at graph_host.cpp:") + std::to_string(line) + ": " + cudaGetErrorString(e);
         return AMR_ERR_CUDA;
     }
     return AMR_OK;
@@ -183,13 +189,13 @@ int rec_relax_until(amr_ctx* c, cudaStream_t s, int l, double ratio, int depth) 
         [&](cudaStream_t q, cudaGraphConditionalHandle h) {
             launch_relax_dev(c->geom, c->bt, c->st, g->L, l, 0, ratio, h, g->d_ctl, c->d_pres, g->d_nest,
                              g->d_counter, q);
-            return launched(c);
+            return launched(c, __LINE__);
         },
         [&](cudaStream_t q, cudaGraphConditionalHandle h) {
             launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), q);
             launch_relax_dev(c->geom, c->bt, c->st, g->L, l, 1, ratio, h, g->d_ctl, c->d_pres, g->d_nest,
                              g->d_counter, q);
-            return launched(c);
+            return launched(c, __LINE__);
         });
 }
 
@@ -199,7 +205,7 @@ int rec_forces(amr_ctx* c, cudaStream_t s) {
         const int n = c->off_reflux[l + 1] - c->off_reflux[l];
         launch_adjust_force(c->geom, c->st, c->d_reflux + c->off_reflux[l], n, s);
     }
-    return launched(c);
+    return launched(c, __LINE__);
 }
 
 // Poisson::vcycle (poisson.cpp:1069-1074) ending in the loop decision.
@@ -213,7 +219,7 @@ int rec_vcycle(amr_ctx* c, cudaStream_t s, int depth, cudaGraphConditionalHandle
     for (int l = 0; l <= maxlevel; l++)
         launch_phi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
     launch_init_vcycle(c->geom, c->st, all(c), nall(c), s);
-    TRY(launched(c));
+    TRY(launched(c, __LINE__));
     for (int l = maxlevel; l >= 0; l--) {
         launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
         launch_vdown_a(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
@@ -222,13 +228,13 @@ int rec_vcycle(amr_ctx* c, cudaStream_t s, int depth, cudaGraphConditionalHandle
             launch_adjust_dphi(c->geom, c->bt, c->st, c->d_reflux + a, b - a, s);
         }
         launch_vdown_c(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
-        TRY(launched(c));
+        TRY(launched(c, __LINE__));
         TRY(rec_relax_until(c, s, l, 1.0, depth));
     }
     for (int l = 0; l <= maxlevel; l++) {
         launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
         if (l > 0) launch_coarse_correction(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
-        TRY(launched(c));
+        TRY(launched(c, __LINE__));
         TRY(rec_relax_until(c, s, l, 0.05, depth));
         launch_retire(c->geom, c->st, lvl(c, l), nlvl(c, l), s);
         launch_phi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
@@ -236,7 +242,7 @@ int rec_vcycle(amr_ctx* c, cudaStream_t s, int depth, cudaGraphConditionalHandle
     TRY(rec_forces(c, s));
     launch_error_dev(c->geom, c->bt, c->st, g->L, maxlevel + 1, tol, hsolve, g->d_ctl, c->d_pres, g->d_nest,
                      g->d_counter, s);
-    return launched(c);
+    return launched(c, __LINE__);
 }
 
 // solve(): boundaries, forces, V-cycles while the L1 error > tol, restriction.
@@ -251,19 +257,19 @@ int rec_solve(amr_ctx* c, cudaStream_t s, double tol, int depth) {
         c, s, depth,
         [&](cudaStream_t q, cudaGraphConditionalHandle h) {
             launch_open_loop(h, g->d_ctl, 1, q);
-            return launched(c);
+            return launched(c, __LINE__);
         },
         [&](cudaStream_t q, cudaGraphConditionalHandle h) { return rec_vcycle(c, q, depth + 1, h, tol); },
         &g->k_vbody));
     for (int l = c->tree.prm.max_level; l >= 0; l--)
         launch_inject(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l], (int)c->parent_slots[l].size(), s);
-    return launched(c);
+    return launched(c, __LINE__);
 }
 
 int rec_enforce_boundaries(amr_ctx* c, cudaStream_t s) {
     for (int l = 0; l <= c->tree.prm.max_level; l++)
         launch_ghost_fill(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
-    return launched(c);
+    return launched(c, __LINE__);
 }
 
 int maxslot(amr_ctx* c) {
@@ -293,7 +299,7 @@ int rec_step(amr_ctx* c, cudaStream_t s, double tol) {
         launch_flow_off(c->geom, c->st, c->tree.root()->slot, c->tree.root()->h, 0.0, betas[rk], c->d_fo, s, dtp);
         launch_add_difs(c->geom, c->st, all(c), nall(c), c->bt.h, 0.0, betas[rk], 1, s, dtp);
         launch_phi_time(c->geom, c->st, all(c), nall(c), rk == 0 ? 0 : (rk == 1 ? 2 : 1), s);
-        TRY(launched(c));
+        TRY(launched(c, __LINE__));
         TRY(rec_solve(c, s, tol, 0));
     }
     return rec_enforce_boundaries(c, s);
@@ -305,11 +311,19 @@ int capture(amr_ctx* c, const std::function<int(cudaStream_t)>& rec, cudaGraphEx
         *exec = nullptr;
     }
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    {
+        const cudaError_t pre = cudaGetLastError();
+        if (pre != cudaSuccess) {
+            c->err = std::string("error pending before capture: ") + cudaGetErrorString(pre);
+            return AMR_ERR_CUDA;
+        }
+    }
     CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
     const int rc = rec(c->stream);
     cudaGraph_t graph;
     const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     if (rc) {
+        c->gs->pending_counts.clear();
         if (e == cudaSuccess) cudaGraphDestroy(graph);
         return rc;
     }
@@ -318,6 +332,8 @@ int capture(amr_ctx* c, const std::function<int(cudaStream_t)>& rec, cudaGraphEx
         return AMR_ERR_CUDA;
     }
     *kernels = kernel_nodes(graph);
+    for (auto& pc : c->gs->pending_counts) *pc.out = kernel_nodes(pc.body);
+    c->gs->pending_counts.clear();
     const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
     cudaGraphDestroy(graph);
     if (ei != cudaSuccess) {
