@@ -236,6 +236,15 @@ int rebuild_topology(amr_ctx* c) {
                 CUDA_TRY(cudaMalloc(&c->d_msrc, sizeof(double) * 32 * c->msrc_cap));
                 CUDA_TRY(cudaMalloc(&c->d_allref, sizeof(int) * c->msrc_cap));
             }
+            // (point, brick) scratch of the domain-face potential: all points
+            // at once up to 32 Mi doubles, batched beyond
+            const size_t need = (size_t)c->n_bfaces * c->geom.pnx * c->geom.pnx * (size_t)n;
+            const size_t want = std::min<size_t>(std::max<size_t>(need, (size_t)n), (size_t)32 << 20);
+            if (want > c->own_cap) {
+                if (c->d_own) cudaFree(c->d_own);
+                c->own_cap = want;
+                CUDA_TRY(cudaMalloc(&c->d_own, sizeof(double) * c->own_cap));
+            }
         }
     }
     if ((int)items.size() > c->d_reflux_cap) {

@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cstddef>
+#include <cstdio>
 #include <functional>
 #include <string>
 #include <vector>
@@ -78,6 +79,12 @@ int ensure_state(amr_ctx* c) {
     CUDA_TRY(cudaMalloc(&g->d_nest, sizeof(double) * c->cap));
     CUDA_TRY(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CUDA_TRY(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned int) * 4, c->stream));
+    // side streams for capturing nested loop bodies, created outside any capture
+    for (int d = 0; d < 4; d++) {
+        cudaStream_t s;
+        CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        g->streams.push_back(s);
+    }
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     return AMR_OK;
 }
@@ -154,15 +161,29 @@ int add_while(amr_ctx* c, cudaStream_t s, int depth, const std::function<int(cud
     return AMR_OK;
 }
 
+// Kernel nodes directly in graph g (not in nested bodies).  Any failure of
+// the queries is cleared from the runtime's last-error state and reported
+// as -1, so it cannot surface later as a launch error.
 long long kernel_nodes(cudaGraph_t g) {
     size_t n = 0;
-    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+    cudaError_t e = cudaGraphGetNodes(g, nullptr, &n);
+    if (e != cudaSuccess) {
+        fprintf(stderr, "[amr] cudaGraphGetNodes: %s\n", cudaGetErrorString(e));
+        cudaGetLastError();
+        return -1;
+    }
     std::vector<cudaGraphNode_t> nodes(n);
-    cudaGraphGetNodes(g, nodes.data(), &n);
+    if (n) e = cudaGraphGetNodes(g, nodes.data(), &n);
     long long k = 0;
-    for (auto nd : nodes) {
+    for (size_t q = 0; q < n && e == cudaSuccess; q++) {
         cudaGraphNodeType t;
-        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+        e = cudaGraphNodeGetType(nodes[q], &t);
+        if (e == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    if (e != cudaSuccess) {
+        fprintf(stderr, "[amr] graph node query: %s\n", cudaGetErrorString(e));
+        cudaGetLastError();
+        return -1;
     }
     return k;
 }
@@ -251,7 +272,7 @@ int rec_solve(amr_ctx* c, cudaStream_t s, double tol, int depth) {
     launch_set_source(c->geom, c->st, all(c), nall(c), s);
     launch_source_sums(c->geom, c->bt, c->st, all(c), nall(c), c->d_msrc, c->d_allref, s);
     launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, all(c), nall(c), c->d_msrc, c->d_allref, c->d_bphi,
-                      s);
+                      c->d_own, c->own_cap, s);
     TRY(rec_forces(c, s));
     TRY(add_while(
         c, s, depth,

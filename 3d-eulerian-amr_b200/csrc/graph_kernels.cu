@@ -8,6 +8,7 @@
 
 #include "euler_state.cuh"
 #include "graph.h"
+#include "relax_brick.cuh"
 
 namespace amr {
 
@@ -45,45 +46,16 @@ template <int NX>
 __global__ void __launch_bounds__(NX* NX* NX)
     k_relax_dev(Geom g, BrickTable bt, DevState st, LevelLists L, int level, int mode, double ratio,
                 cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest, unsigned int* counter) {
-    constexpr int P = NX + 2, P3 = P * P * P, NT = NX * NX * NX, NW = NT / 32;
-    __shared__ double d[P3];
-    __shared__ double red[NW];
-    __shared__ double total;
+    constexpr int P = NX + 2, P3 = P * P * P;
+    __shared__ RelaxSmem<NX> sm;
     __shared__ bool last;
     const int b = L.slots[L.off[level] + blockIdx.x];
     const size_t base = (size_t)b * P3;
-    for (int t = threadIdx.x; t < P3; t += NT) d[t] = st.dphi[base + t];
     const int t = threadIdx.x;
-    const int i = t % NX + 1, j = (t / NX) % NX + 1, k = t / (NX * NX) + 1;
-    const int c = (k * P + j) * P + i;
-    const double d1 = st.dphi1[base + c];
-    __syncthreads();
-    double resid0 = 0.0, resid = 0.0;
-    int iters = 0;
-    bool first = true;
-    do {
-        const double div = (d[c + 1] + d[c - 1] + d[c + P] + d[c - P] + d[c + P * P] + d[c - P * P]) - (d[c] * 6.0);
-        const double tmp0 = d1 + div * (1.0 / 6.0);
-        __syncthreads();
-        d[c] += tmp0;
-        double sq = tmp0 * tmp0;
-        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-        if ((t & 31) == 0) red[t >> 5] = sq;
-        __syncthreads();
-        if (t == 0) {
-            double s = 0.0;
-            for (int w = 0; w < NW; w++) s += red[w];
-            total = s;
-        }
-        __syncthreads();
-        resid = total;
-        if (first) {
-            resid0 = resid;
-            first = false;
-        }
-        iters++;
-    } while (resid / resid0 > 0.5 && iters < 16);
-    st.dphi[base + c] = d[c];
+    const int c = ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
+    double v;
+    const double resid = relax_brick<NX>(sm, st.dphi + base, st.dphi1 + base, &v);
+    st.dphi[base + c] = v;
     if (t == 0) pres[b] = resid;
     // last block: reduce and decide
     __threadfence();

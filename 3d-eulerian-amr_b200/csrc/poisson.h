@@ -15,8 +15,10 @@ void launch_poisson_new_bricks(const Geom& g, const BrickTable& bt, const DevSta
 void launch_set_source(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);
 void launch_source_sums(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                         double* msrc, int* allref, cudaStream_t s);
+// scratch: (point, brick) own sums, scratch_cap doubles; points are batched
 void launch_phys_bound(const Geom& g, const BrickTable& bt, const int* bfaces, int nbf, const int* order, int n,
-                       const double* msrc, const int* allref, double* bphi, cudaStream_t s);
+                       const double* msrc, const int* allref, double* bphi, double* scratch, size_t scratch_cap,
+                       cudaStream_t s);
 void launch_phi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,
                            const int* slots, int n, cudaStream_t s);
 void launch_dphi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,

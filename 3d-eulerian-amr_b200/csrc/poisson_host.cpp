@@ -250,7 +250,7 @@ int check_device_error(amr_ctx* c) {
 
 void amr_poisson_release(amr_ctx* c) {
     if (!c) return;
-    void* ptrs[] = {c->d_bphi, c->d_msrc, c->d_allref, c->d_pres, c->d_bfaces, c->d_perr};
+    void* ptrs[] = {c->d_bphi, c->d_msrc, c->d_allref, c->d_pres, c->d_bfaces, c->d_perr, c->d_own};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -315,7 +315,7 @@ int amr_poisson_boundaries(amr_ctx* c) {
     {
         ProfScope ps_(c->prof, KC_PHYS_BOUND, c->stream);
         launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, all(c), nall(c), c->d_msrc, c->d_allref, c->d_bphi,
-                          c->stream);
+                          c->d_own, c->own_cap, c->stream);
     }
     return check_launch(c);
 }

@@ -6,6 +6,7 @@
 #include "context.h"
 #include "euler_state.cuh"
 #include "poisson.h"
+#include "relax_brick.cuh"
 
 namespace amr {
 
@@ -118,15 +119,14 @@ __global__ void k_source_sums(Geom g, BrickTable bt, DevState st, const int* __r
 // (poisson_phys_bound.cpp:70-81) evaluating Single::compute_phi
 // (single/single.cpp:219-243): the recursive sum over all bricks of
 // -alpha m / r over their octant monopoles, with each brick's own sum formed
-// first and the children's sums added after it in child order.  One block per
-// boundary point: threads form the per-brick own sums of a chunk in parallel,
-// thread 0 accumulates them with the nesting of the recursion.
-__global__ void k_phys_bound(Geom g, BrickTable bt, const int* __restrict__ bfaces, const int* __restrict__ order,
-                             int n, const double* __restrict__ msrc, const int* __restrict__ allref,
-                             double* __restrict__ bphi) {
+// first and the children's sums added after it in child order.  Two kernels:
+// every (point, brick) own sum in parallel into a scratch matrix [brick][point],
+// then one thread per point accumulates them with the nesting of the
+// recursion (a stack of partial sums indexed by level).
+__device__ __forceinline__ void bound_point(const Geom& g, const BrickTable& bt, const int* bfaces, int p, double* xyz,
+                                            int* where) {
     const int pnx = g.pnx;
-    const int fe = blockIdx.x / (pnx * pnx);
-    const int pt = blockIdx.x % (pnx * pnx);
+    const int fe = p / (pnx * pnx), pt = p % (pnx * pnx);
     const int b = bfaces[2 * fe], face = bfaces[2 * fe + 1];
     const int a = pt / pnx, cc = pt % pnx;  // table[a][cc]: lower, higher transverse
     const int ax = face >> 1;
@@ -135,53 +135,55 @@ __global__ void k_phys_bound(Geom g, BrickTable bt, const int* __restrict__ bfac
     pi[ax == 0 ? 1 : 0] = a;
     pi[ax == 2 ? 1 : 2] = cc;
     const double h = bt.h[b];
-    const double x = cell_centre(g, 0, bt.off[3 * b + 0], h, pi[0] + g.bw - 1);
-    const double y = cell_centre(g, 1, bt.off[3 * b + 1], h, pi[1] + g.bw - 1);
-    const double z = cell_centre(g, 2, bt.off[3 * b + 2], h, pi[2] + g.bw - 1);
+    for (int d = 0; d < 3; d++) xyz[d] = cell_centre(g, d, bt.off[3 * b + d], h, pi[d] + g.bw - 1);
+    if (where) *where = ((b * 6 + face) * pnx * pnx) + a * pnx + cc;
+}
+
+__global__ void k_phys_own(Geom g, BrickTable bt, const int* __restrict__ bfaces, int p0, int np, int n,
+                           const double* __restrict__ msrc, const int* __restrict__ allref, double* __restrict__ own) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;  // point within the batch
+    const int e = blockIdx.y;                              // brick (DFS entry)
+    if (p >= np) return;
+    double xyz[3];
+    bound_point(g, bt, bfaces, p0 + p, xyz, nullptr);
     const double alpha = g.z_reflect ? 2.0 : 1.0;
-    __shared__ double own[128];
-    __shared__ int lev[128];
+    const double* m = msrc + (size_t)e * 32;
+    const bool ar = allref[e] != 0;
+    double sum = 0.0;
+    for (int q = 0; q < 8; q++) {
+        const double dx = xyz[0] - m[4 * q + 1], dy = xyz[1] - m[4 * q + 2], dz = xyz[2] - m[4 * q + 3];
+        if (!ar) {
+            sum -= alpha * m[4 * q + 0] / sqrt(dx * dx + dy * dy + dz * dz);
+        } else {
+            sum = 0.0;
+        }
+    }
+    own[(size_t)e * np + p] = sum;
+}
+
+__global__ void k_phys_accum(Geom g, BrickTable bt, const int* __restrict__ bfaces, const int* __restrict__ order,
+                             int p0, int np, int n, const double* __restrict__ own, double* __restrict__ bphi) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
     double acc[16];
     int depth = -1;
-    for (int base = 0; base < n; base += 128) {
-        const int e = base + threadIdx.x;
-        if (e < n) {
-            const double* m = msrc + (size_t)e * 32;
-            double sum = 0.0;
-            const bool ar = allref[e] != 0;
-            for (int q = 0; q < 8; q++) {
-                const double dx = x - m[4 * q + 1], dy = y - m[4 * q + 2], dz = z - m[4 * q + 3];
-                if (!ar) {
-                    sum -= alpha * m[4 * q + 0] / sqrt(dx * dx + dy * dy + dz * dz);
-                } else {
-                    sum = 0.0;
-                }
-            }
-            own[threadIdx.x] = sum;
-            lev[threadIdx.x] = bt.level[order[e]];
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const int m = min(128, n - base);
-            for (int q = 0; q < m; q++) {
-                const int L = lev[q];
-                while (depth >= L) {
-                    acc[depth - 1] += acc[depth];
-                    depth--;
-                }
-                acc[L] = own[q];
-                depth = L;
-            }
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        while (depth > 0) {
+    for (int e = 0; e < n; e++) {
+        const int L = bt.level[order[e]];
+        while (depth >= L) {
             acc[depth - 1] += acc[depth];
             depth--;
         }
-        bphi[((size_t)b * 6 + face) * pnx * pnx + a * pnx + cc] = acc[0];
+        acc[L] = own[(size_t)e * np + p];
+        depth = L;
     }
+    while (depth > 0) {
+        acc[depth - 1] += acc[depth];
+        depth--;
+    }
+    double xyz[3];
+    int where;
+    bound_point(g, bt, bfaces, p0 + p, xyz, &where);
+    bphi[where] = acc[0];
 }
 
 // ---------------------------------------------------------------------------
@@ -526,48 +528,17 @@ __global__ void k_vdown_c(Geom g, BrickTable bt, DevState st, const int* __restr
 template <int NX>
 __global__ void __launch_bounds__(NX* NX* NX) k_relax(Geom g, DevState st, const int* __restrict__ slots,
                                                       double* __restrict__ out, int* __restrict__ sweeps_out) {
-    constexpr int P = NX + 2, P3 = P * P * P, NT = NX * NX * NX, NW = NT / 32;
-    __shared__ double d[P3];
-    __shared__ double red[NW];
-    __shared__ double total;
+    constexpr int P = NX + 2, P3 = P * P * P;
+    __shared__ RelaxSmem<NX> sm;
     const int b = slots[blockIdx.x];
     const size_t base = (size_t)b * P3;
-    for (int t = threadIdx.x; t < P3; t += NT) d[t] = st.dphi[base + t];
     const int t = threadIdx.x;
-    const int i = t % NX + 1, j = (t / NX) % NX + 1, k = t / (NX * NX) + 1;
-    const int c = (k * P + j) * P + i;
-    const double d1 = st.dphi1[base + c];
-    __syncthreads();
-    double resid0 = 0.0, resid = 0.0;
-    int iters = 0;
-    bool first = true;
-    do {
-        const double div = (d[c + 1] + d[c - 1] + d[c + P] + d[c - P] + d[c + P * P] + d[c - P * P]) - (d[c] * 6.0);
-        const double tmp0 = d1 + div * (1.0 / 6.0);
-        __syncthreads();
-        d[c] += tmp0;
-        double sq = tmp0 * tmp0;
-        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-        if ((t & 31) == 0) red[t >> 5] = sq;
-        __syncthreads();
-        if (t == 0) {
-            double s = 0.0;
-            for (int w = 0; w < NW; w++) s += red[w];
-            total = s;
-        }
-        __syncthreads();
-        resid = total;
-        if (first) {
-            resid0 = resid;
-            first = false;
-        }
-        iters++;
-    } while (resid / resid0 > 0.5 && iters < 16);
-    st.dphi[base + c] = d[c];
-    if (t == 0) {
-        out[b] = resid;
-        if (sweeps_out) atomicAdd(sweeps_out, iters);
-    }
+    const int c = ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
+    double v;
+    const double resid = relax_brick<NX>(sm, st.dphi + base, st.dphi1 + base, &v);
+    st.dphi[base + c] = v;
+    if (t == 0) out[b] = resid;
+    (void)sweeps_out;
 }
 
 // Poisson::vcycle_coarse_correction (poisson.cpp:17-51): child dphi +=
@@ -754,8 +725,16 @@ void launch_source_sums(const Geom& g, const BrickTable& bt, const DevState& st,
     if (n > 0) k_source_sums<<<n, 32, 0, s>>>(g, bt, st, slots, msrc, allref);
 }
 void launch_phys_bound(const Geom& g, const BrickTable& bt, const int* bfaces, int nbf, const int* order, int n,
-                       const double* msrc, const int* allref, double* bphi, cudaStream_t s) {
-    if (nbf > 0) k_phys_bound<<<nbf * g.pnx * g.pnx, 128, 0, s>>>(g, bt, bfaces, order, n, msrc, allref, bphi);
+                       const double* msrc, const int* allref, double* bphi, double* scratch, size_t scratch_cap,
+                       cudaStream_t s) {
+    if (nbf <= 0 || n <= 0) return;
+    const int npts = nbf * g.pnx * g.pnx;
+    const int batch = (int)std::min<size_t>((size_t)npts, scratch_cap / (size_t)n);
+    for (int p0 = 0; p0 < npts; p0 += batch) {
+        const int np = std::min(batch, npts - p0);
+        k_phys_own<<<dim3((np + 127) / 128, n), 128, 0, s>>>(g, bt, bfaces, p0, np, n, msrc, allref, scratch);
+        k_phys_accum<<<(np + 127) / 128, 128, 0, s>>>(g, bt, bfaces, order, p0, np, n, scratch, bphi);
+    }
 }
 void launch_phi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,
                            const int* slots, int n, cudaStream_t s) {

@@ -1,0 +1,67 @@
+// Jacobi sweeps of Poisson::vcycle_relax (poisson.cpp:88-130) on one brick
+// staged in shared memory, one thread per interior cell.
+//
+// Each sweep computes tmp0 = dphi1 + lap(dphi)/6 for every cell from the
+// previous sweep's values and adds it; the sweep's sum of tmp0^2 decides the
+// loop (ratio to the first sweep's > 0.5, at most 16 sweeps).  The two shared
+// buffers alternate so one block barrier per sweep suffices; every thread
+// adds the per-warp partial sums itself along the same fixed pairwise tree,
+// so all threads take the same loop decision.  (The reference adds the
+// squares sequentially; the sums differ in the last bits only.)
+#pragma once
+
+namespace amr {
+
+template <int NX>
+struct RelaxSmem {
+    static constexpr int P = NX + 2, P3 = P * P * P, NT = NX * NX * NX, NW = NT / 32;
+    double buf[2][P3];
+    double red[2][NW];
+};
+
+// Stages the brick (slot base) into both buffers; returns the last sweep's
+// sum and leaves the relaxed interior value of this thread's cell in *out.
+template <int NX>
+__device__ __forceinline__ double relax_brick(RelaxSmem<NX>& sm, const double* __restrict__ dphi,
+                                              const double* __restrict__ dphi1, double* out) {
+    constexpr int P = RelaxSmem<NX>::P, P3 = RelaxSmem<NX>::P3, NT = RelaxSmem<NX>::NT, NW = RelaxSmem<NX>::NW;
+    const int t = threadIdx.x;
+    for (int q = t; q < P3; q += NT) {
+        const double v = dphi[q];
+        sm.buf[0][q] = v;
+        sm.buf[1][q] = v;
+    }
+    const int i = t % NX + 1, j = (t / NX) % NX + 1, k = t / (NX * NX) + 1;
+    const int c = (k * P + j) * P + i;
+    const double d1 = dphi1[c];
+    __syncthreads();
+    double resid0 = 0.0, resid = 0.0;
+    int iters = 0, cur = 0;
+    do {
+        const double* d = sm.buf[cur];
+        const double div = (d[c + 1] + d[c - 1] + d[c + P] + d[c - P] + d[c + P * P] + d[c - P * P]) - (d[c] * 6.0);
+        const double tmp0 = d1 + div * (1.0 / 6.0);
+        sm.buf[cur ^ 1][c] = d[c] + tmp0;
+        double sq = tmp0 * tmp0;
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
+        if ((t & 31) == 0) sm.red[cur][t >> 5] = sq;
+        __syncthreads();
+        // pairwise sum of the warp partials (fixed tree, identical in every
+        // thread): log2(NW) dependent additions instead of NW
+        double r[NW];
+#pragma unroll
+        for (int w = 0; w < NW; w++) r[w] = sm.red[cur][w];
+#pragma unroll
+        for (int span = 1; span < NW; span <<= 1)
+#pragma unroll
+            for (int w = 0; w + span < NW; w += 2 * span) r[w] = r[w] + r[w + span];
+        resid = r[0];
+        if (iters == 0) resid0 = resid;
+        iters++;
+        cur ^= 1;
+    } while (resid / resid0 > 0.5 && iters < 16);
+    *out = sm.buf[cur][c];
+    return resid;
+}
+
+}  // namespace amr
