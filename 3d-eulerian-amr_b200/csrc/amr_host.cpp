@@ -16,6 +16,8 @@
 
 using namespace amr;
 
+thread_local long long amr::g_launch_tally = 0;
+
 #define CUDA_TRY(call)                                                                                  \
     do {                                                                                                \
         cudaError_t e__ = (call);                                                                       \
@@ -236,10 +238,29 @@ int rebuild_topology(amr_ctx* c) {
                 CUDA_TRY(cudaMalloc(&c->d_msrc, sizeof(double) * 32 * c->msrc_cap));
                 CUDA_TRY(cudaMalloc(&c->d_allref, sizeof(int) * c->msrc_cap));
             }
-            // (point, brick) scratch of the domain-face potential: all points
-            // at once up to 32 Mi doubles, batched beyond
-            const size_t need = (size_t)c->n_bfaces * c->geom.pnx * c->geom.pnx * (size_t)n;
-            const size_t want = std::min<size_t>(std::max<size_t>(need, (size_t)n), (size_t)32 << 20);
+            // walk program of the domain-face potential: subtrees of at most
+            // ~sqrt(n) bricks summed in parallel, then the walk above them
+            std::vector<int> lv(n), segs, top;
+            for (int i = 0; i < n; i++) lv[i] = c->order[i]->level;
+            const int limit = std::max(4, (int)std::ceil(std::sqrt((double)n)));
+            build_phys_walk(lv.data(), n, limit, segs, top);
+            c->n_pseg = (int)segs.size() / 2;
+            c->n_ptop = (int)top.size();
+            std::vector<int> walk(segs);
+            walk.insert(walk.end(), top.begin(), top.end());
+            if ((int)walk.size() > c->pwalk_cap) {
+                if (c->d_pwalk) cudaFree(c->d_pwalk);
+                c->pwalk_cap = (int)walk.size() * 2 + 64;
+                CUDA_TRY(cudaMalloc(&c->d_pwalk, sizeof(int) * c->pwalk_cap));
+            }
+            if (!walk.empty())
+                CUDA_TRY(cudaMemcpyAsync(c->d_pwalk, walk.data(), sizeof(int) * walk.size(), cudaMemcpyHostToDevice,
+                                         c->stream));
+            // (subtree, point) scratch: all points at once up to 32 Mi
+            // doubles, batched beyond
+            const size_t per = (size_t)std::max(c->n_pseg, 1);
+            const size_t need = (size_t)c->n_bfaces * c->geom.pnx * c->geom.pnx * per;
+            const size_t want = std::min<size_t>(std::max<size_t>(need, per), (size_t)32 << 20);
             if (want > c->own_cap) {
                 if (c->d_own) cudaFree(c->d_own);
                 c->own_cap = want;
@@ -407,6 +428,7 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
     g.pnx3 = g.pnx * g.pnx * g.pnx;
     g.ucount = g.nf * g.gnx3;
     g.z_reflect = cfg->z_reflect;
+    g.precision = cfg->precision;
     g.grid_dim = cfg->grid_dim;
     g.h0 = tp.h0;
     for (int d = 0; d < 3; d++) g.origin[d] = cfg->origin[d];

@@ -22,6 +22,7 @@ struct Geom {
     int bw, nx, gnx, nf, pnx;
     int gnx3, pnx3, ucount;  // gnx^3, pnx^3, nf*gnx^3
     int z_reflect;
+    int precision;  // AMR_PREC_FP64 / AMR_PREC_MIXED
     double grid_dim, h0;
     double origin[3];
     double theta, cfl, gamma, rho_floor, ei_floor, grav_g;
@@ -62,5 +63,8 @@ struct DevState {
 struct RefluxItem {
     int coarse, child, dir, i0, ic, cj, ck, pad;
 };
+
+// Kernels launched (or recorded into a graph) by the calling host thread.
+extern thread_local long long g_launch_tally;
 
 }  // namespace amr

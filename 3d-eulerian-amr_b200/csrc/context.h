@@ -57,8 +57,10 @@ struct amr_ctx {
     int* d_bfaces = nullptr;    // [nbf][2] (slot, face) of physical (non-mirror) faces
     int* d_perr = nullptr;      // device error word (bad mirror index)
     int n_bfaces = 0, msrc_cap = 0, bfaces_cap = 0;
-    double* d_own = nullptr;    // (point, brick) own sums of the domain-face potential
+    double* d_own = nullptr;    // (point, subtree) partial sums of the domain-face potential
     size_t own_cap = 0;
+    int* d_pwalk = nullptr;     // subtree ranges [nseg][2] | top-level walk [ntop]
+    int pwalk_cap = 0, n_pseg = 0, n_ptop = 0;
     std::vector<int> off_reflux_dir;  // [(maxl+1)*3+1] items sorted by (level, dir)
     int vcycle_max_outer = 1000;
     long long relax_calls = 0, relax_sweeps_total = 0;

@@ -14,6 +14,7 @@ struct LevelLists {
     const int* slots;  // packed lists
     const int* all;    // all bricks, DFS order
     int nall;
+    int cap;           // brick pool capacity (slot range)
     int off[MAX_LEVELS];
     int cnt[MAX_LEVELS];
 };
@@ -32,11 +33,13 @@ struct Control {
     long long cycles_total;  // V-cycles since the context started
     int steps;
     int pad;
+    int snap_par[MAX_LEVELS];  // which face-snapshot buffer the next pass reads
 };
 
+// snap: [2][cap][6][nx][nx] first-interior layers published by every pass
 void launch_relax_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int level,
                       int mode, double ratio, cudaGraphConditionalHandle cond, Control* ctl, double* pres,
-                      double* nest, unsigned int* counter, cudaStream_t s);
+                      double* nest, unsigned int* counter, double* snap, size_t snap_stride, cudaStream_t s);
 void launch_error_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int nlevels,
                       double tol, cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest,
                       unsigned int* counter, cudaStream_t s);

@@ -38,10 +38,14 @@ using namespace amr;
         if (rc__) return rc__; \
     } while (0)
 
+// doubles per brick in one face-snapshot buffer: 6 faces of nx*nx (nx = 8)
+constexpr size_t SNAP_STRIDE = 6 * 8 * 8;
+
 struct GraphState {
     Control* d_ctl = nullptr;
     Control* h_ctl = nullptr;  // pinned mirror
     double* d_nest = nullptr;
+    double* d_snap = nullptr;  // [2][cap][6][8][8] first-interior dphi layers
     unsigned int* d_counter = nullptr;
     int* h_steps = nullptr;     // pinned scalar staging
     cudaGraphExec_t step_exec = nullptr;
@@ -53,17 +57,15 @@ struct GraphState {
     int solve_max = -1;
     std::vector<cudaStream_t> streams;  // capture streams of nested bodies
     LevelLists L{};
-    // kernel nodes of the captured graphs: top level of the step / solve
-    // graph, one V-cycle body (outside its relaxation loops); a relaxation
-    // loop body holds 2 (ghost fill + relax)
-    long long k_step = 0, k_solve = 0, k_vbody = 0;
+    // kernels recorded into the captured graphs (counted by the launch
+    // tally while recording): top level of the step / solve graph, one
+    // V-cycle body outside its relaxation loops, one relaxation loop body
+    long long k_step = 0, k_solve = 0, k_vbody = 0, k_rbody = 0;
+    long long rec_in_bodies = 0;  // kernels recorded inside outermost WHILE bodies
+    long long rec_nested = 0;     // kernels recorded inside the bodies of the body being recorded
+    int while_depth = 0;
     int nlevels_captured = 0;
     long long last_cycles = 0, last_relax = 0;  // device counters at the last read
-    struct PendingCount {
-        cudaGraph_t body;
-        long long* out;
-    };
-    std::vector<PendingCount> pending_counts;
 };
 
 namespace {
@@ -77,6 +79,7 @@ int ensure_state(amr_ctx* c) {
     CUDA_TRY(cudaMallocHost(&g->h_ctl, sizeof(Control)));
     CUDA_TRY(cudaMallocHost(&g->h_steps, sizeof(int) * 4));
     CUDA_TRY(cudaMalloc(&g->d_nest, sizeof(double) * c->cap));
+    CUDA_TRY(cudaMalloc(&g->d_snap, sizeof(double) * 2 * SNAP_STRIDE * (size_t)c->cap));
     CUDA_TRY(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CUDA_TRY(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned int) * 4, c->stream));
     // side streams for capturing nested loop bodies, created outside any capture
@@ -100,6 +103,7 @@ void fill_lists(amr_ctx* c) {
     L.slots = c->d_slots;
     L.all = c->d_slots + c->off_all[0];
     L.nall = (int)c->all_slots.size();
+    L.cap = c->cap;
     for (int m = 0; m < MAX_LEVELS; m++) {
         const bool ok = m < (int)c->level_slots.size();
         L.off[m] = ok ? c->off_level[m] : 0;
@@ -117,13 +121,10 @@ cudaStream_t body_stream(amr_ctx* c, int depth) {
     return g->streams[depth];
 }
 
-long long kernel_nodes(cudaGraph_t g);
-
 // At the current capture point of s: run pre(s, h), then add a WHILE node on
 // handle h whose body is captured from body(s2, h) on a side stream.
 int add_while(amr_ctx* c, cudaStream_t s, int depth, const std::function<int(cudaStream_t, cudaGraphConditionalHandle)>& pre,
-              const std::function<int(cudaStream_t, cudaGraphConditionalHandle)>& body,
-              long long* body_kernels = nullptr) {
+              const std::function<int(cudaStream_t, cudaGraphConditionalHandle)>& body) {
     cudaStreamCaptureStatus status;
     cudaGraph_t graph;
     const cudaGraphNode_t* deps = nullptr;
@@ -148,7 +149,16 @@ int add_while(amr_ctx* c, cudaStream_t s, int depth, const std::function<int(cud
     CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
     cudaStream_t s2 = body_stream(c, depth);
     CUDA_TRY(cudaStreamBeginCaptureToGraph(s2, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+    GraphState* gs = c->gs;
+    const long long t0 = g_launch_tally, n0 = gs->rec_nested;
+    gs->rec_nested = 0;
+    gs->while_depth++;
     const int rc = body(s2, h);
+    gs->while_depth--;
+    const long long all_k = g_launch_tally - t0, own = all_k - gs->rec_nested;
+    gs->rec_nested = n0 + all_k;
+    if (gs->while_depth == 0) gs->rec_in_bodies += all_k;
+    (depth == 0 ? gs->k_vbody : gs->k_rbody) = own;
     cudaGraph_t out;
     const cudaError_t e = cudaStreamEndCapture(s2, &out);
     if (rc) return rc;
@@ -156,36 +166,7 @@ int add_while(amr_ctx* c, cudaStream_t s, int depth, const std::function<int(cud
         c->err = std::string("body capture failed: ") + cudaGetErrorString(e);
         return AMR_ERR_CUDA;
     }
-    // body graphs may only be inspected once the enclosing capture has ended
-    if (body_kernels) c->gs->pending_counts.push_back({bodyg, body_kernels});
     return AMR_OK;
-}
-
-// Kernel nodes directly in graph g (not in nested bodies).  Any failure of
-// the queries is cleared from the runtime's last-error state and reported
-// as -1, so it cannot surface later as a launch error.
-long long kernel_nodes(cudaGraph_t g) {
-    size_t n = 0;
-    cudaError_t e = cudaGraphGetNodes(g, nullptr, &n);
-    if (e != cudaSuccess) {
-        fprintf(stderr, "[amr] cudaGraphGetNodes: %s\n", cudaGetErrorString(e));
-        cudaGetLastError();
-        return -1;
-    }
-    std::vector<cudaGraphNode_t> nodes(n);
-    if (n) e = cudaGraphGetNodes(g, nodes.data(), &n);
-    long long k = 0;
-    for (size_t q = 0; q < n && e == cudaSuccess; q++) {
-        cudaGraphNodeType t;
-        e = cudaGraphNodeGetType(nodes[q], &t);
-        if (e == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
-    }
-    if (e != cudaSuccess) {
-        fprintf(stderr, "[amr] graph node query: %s\n", cudaGetErrorString(e));
-        cudaGetLastError();
-        return -1;
-    }
-    return k;
 }
 
 int launched(amr_ctx* c, int line) {
@@ -209,13 +190,13 @@ int rec_relax_until(amr_ctx* c, cudaStream_t s, int l, double ratio, int depth) 
         c, s, depth,
         [&](cudaStream_t q, cudaGraphConditionalHandle h) {
             launch_relax_dev(c->geom, c->bt, c->st, g->L, l, 0, ratio, h, g->d_ctl, c->d_pres, g->d_nest,
-                             g->d_counter, q);
+                             g->d_counter, g->d_snap, SNAP_STRIDE, q);
             return launched(c, __LINE__);
         },
         [&](cudaStream_t q, cudaGraphConditionalHandle h) {
-            launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), q);
+            // ghost fill folded into the pass (face snapshot of the previous pass)
             launch_relax_dev(c->geom, c->bt, c->st, g->L, l, 1, ratio, h, g->d_ctl, c->d_pres, g->d_nest,
-                             g->d_counter, q);
+                             g->d_counter, g->d_snap, SNAP_STRIDE, q);
             return launched(c, __LINE__);
         });
 }
@@ -271,8 +252,11 @@ int rec_solve(amr_ctx* c, cudaStream_t s, double tol, int depth) {
     GraphState* g = c->gs;
     launch_set_source(c->geom, c->st, all(c), nall(c), s);
     launch_source_sums(c->geom, c->bt, c->st, all(c), nall(c), c->d_msrc, c->d_allref, s);
-    launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, all(c), nall(c), c->d_msrc, c->d_allref, c->d_bphi,
-                      c->d_own, c->own_cap, s);
+    if (launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, all(c), phys_walk(c), c->d_msrc, c->d_allref,
+                          c->d_bphi, c->d_own, c->own_cap, s)) {
+        c->err = "domain-face potential scratch too small";
+        return AMR_ERR_STATE;
+    }
     TRY(rec_forces(c, s));
     TRY(add_while(
         c, s, depth,
@@ -280,8 +264,7 @@ int rec_solve(amr_ctx* c, cudaStream_t s, double tol, int depth) {
             launch_open_loop(h, g->d_ctl, 1, q);
             return launched(c, __LINE__);
         },
-        [&](cudaStream_t q, cudaGraphConditionalHandle h) { return rec_vcycle(c, q, depth + 1, h, tol); },
-        &g->k_vbody));
+        [&](cudaStream_t q, cudaGraphConditionalHandle h) { return rec_vcycle(c, q, depth + 1, h, tol); }));
     for (int l = c->tree.prm.max_level; l >= 0; l--)
         launch_inject(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l], (int)c->parent_slots[l].size(), s);
     return launched(c, __LINE__);
@@ -340,11 +323,16 @@ int capture(amr_ctx* c, const std::function<int(cudaStream_t)>& rec, cudaGraphEx
         }
     }
     CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    GraphState* gs = c->gs;
+    gs->rec_in_bodies = 0;
+    gs->rec_nested = 0;
+    gs->while_depth = 0;
+    const long long t0 = g_launch_tally;
     const int rc = rec(c->stream);
+    *kernels = g_launch_tally - t0 - gs->rec_in_bodies;
     cudaGraph_t graph;
     const cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
     if (rc) {
-        c->gs->pending_counts.clear();
         if (e == cudaSuccess) cudaGraphDestroy(graph);
         return rc;
     }
@@ -352,9 +340,6 @@ int capture(amr_ctx* c, const std::function<int(cudaStream_t)>& rec, cudaGraphEx
         c->err = std::string("capture failed: ") + cudaGetErrorString(e);
         return AMR_ERR_CUDA;
     }
-    *kernels = kernel_nodes(graph);
-    for (auto& pc : c->gs->pending_counts) *pc.out = kernel_nodes(pc.body);
-    c->gs->pending_counts.clear();
     const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
     cudaGraphDestroy(graph);
     if (ei != cudaSuccess) {
@@ -387,15 +372,15 @@ int read_ctl(amr_ctx* c) {
     return AMR_OK;
 }
 
-// Kernels executed by the replay just read back: the graph's top-level kernel
-// nodes, one V-cycle body per V-cycle, two kernels per relaxation pass beyond
-// the first of each loop (the first is part of the V-cycle body).
+// Kernels executed by the replay just read back: the graph's top-level
+// kernels, one V-cycle body per V-cycle, one relaxation loop body per pass
+// beyond the first of each loop (the first is part of the V-cycle body).
 void count_replay(amr_ctx* c, long long top_kernels) {
     GraphState* g = c->gs;
     const long long dc = g->h_ctl->cycles_total - g->last_cycles;
     const long long dr = g->h_ctl->relax_calls - g->last_relax;
     const long long loops = dr - dc * 2LL * g->nlevels_captured;
-    c->prof.kernels += top_kernels + dc * g->k_vbody + 2LL * loops;
+    c->prof.kernels += top_kernels + dc * g->k_vbody + loops * g->k_rbody;
     c->relax_calls += dr;
     g->last_cycles = g->h_ctl->cycles_total;
     g->last_relax = g->h_ctl->relax_calls;
@@ -430,6 +415,7 @@ void graph_release(amr_ctx* c) {
     if (g->h_ctl) cudaFreeHost(g->h_ctl);
     if (g->h_steps) cudaFreeHost(g->h_steps);
     if (g->d_nest) cudaFree(g->d_nest);
+    if (g->d_snap) cudaFree(g->d_snap);
     if (g->d_counter) cudaFree(g->d_counter);
     delete g;
     c->gs = nullptr;

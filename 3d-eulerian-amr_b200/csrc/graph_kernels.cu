@@ -9,6 +9,7 @@
 #include "euler_state.cuh"
 #include "graph.h"
 #include "relax_brick.cuh"
+#include "launch.cuh"
 
 namespace amr {
 
@@ -42,20 +43,82 @@ __device__ double nested_sum_block(const LevelLists& L, const int* __restrict__ 
 // decides the relaxation loop of vcycle0 (poisson.cpp:66-70, 74-78):
 // mode 0 records resid0 and opens the loop, mode 1 continues it while
 // resid / resid0 > ratio.
+//
+// Ghost zones: in mode 0 they come from the brick's own dphi array (filled
+// just before by the face ghost kernel).  In mode 1 the block fills them
+// itself -- what Poisson::enforce_dphi_boundaries (poisson.cpp:890-929) would
+// copy: a same-level neighbour's first interior layer from the snapshot the
+// previous pass published, the parent's value across a coarse-fine face
+// (PoissonAMRBound::get_dphi), 0 on a domain face, the mirror on z = 0 -- and
+// also stores them into its global ghost cells, so the arrays end the loop
+// exactly as the reference leaves them.  Every pass publishes its new first
+// interior layers for the next pass.
+template <int NX>
+__device__ __forceinline__ double ghost_dphi(const Geom& g, const BrickTable& bt, const DevState& st,
+                                             const double* snap_rd, size_t stride, int b, int face, int t1, int t2) {
+    constexpr int P = NX + 2;
+    const int kind = bt.ftype[6 * b + face];
+    const int nbr = bt.fnbr[6 * b + face];
+    if (kind == FACE_SIB) return __ldcg(snap_rd + (size_t)nbr * stride + ((face ^ 1) * NX + (t1 - 1)) * NX + (t2 - 1));
+    if (kind == FACE_OUTFLOW) return 0.0;
+    const int ax = face >> 1;
+    int q[3];
+    q[ax] = (face & 1) ? 1 : P - 2;
+    q[ax == 0 ? 1 : 0] = t1;
+    q[ax == 2 ? 1 : 2] = t2;
+    if (kind == FACE_REFLECT) {  // own value mirrored through z = 0, before this pass
+        const int kk = q[2] == 1 ? P - 2 : 1;
+        return st.dphi[(size_t)b * P * P * P + (kk * P + q[1]) * P + q[0]];
+    }
+    const int v = (face & 1) ? 1 : -1;
+    int r[3];
+    for (int d = 0; d < 3; d++) {
+        const int rel = bt.off[3 * b + d] + (d == ax ? v * (P - 2) : 0) - 2 * bt.off[3 * nbr + d] - (g.bw - 1);
+        r[d] = (rel + q[d]) / 2;
+    }
+    return st.dphi[(size_t)nbr * P * P * P + (r[2] * P + r[1]) * P + r[0]];
+}
+
 template <int NX>
 __global__ void __launch_bounds__(NX* NX* NX)
     k_relax_dev(Geom g, BrickTable bt, DevState st, LevelLists L, int level, int mode, double ratio,
-                cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest, unsigned int* counter) {
-    constexpr int P = NX + 2, P3 = P * P * P;
+                cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest, unsigned int* counter,
+                double* snap, size_t stride, size_t snap_half) {
+    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX;
     __shared__ RelaxSmem<NX> sm;
     __shared__ bool last;
     const int b = L.slots[L.off[level] + blockIdx.x];
     const size_t base = (size_t)b * P3;
     const int t = threadIdx.x;
+    // snapshot buffers: the previous pass wrote buffer `par`, this one writes par^1
+    const int par = mode == 0 ? 0 : ctl->snap_par[level];
+    const double* snap_rd = snap + (size_t)par * snap_half;
+    double* snap_wr = snap + (size_t)(mode == 0 ? 0 : par ^ 1) * snap_half;
+    if (mode == 1 && t < 6 * F) {
+        const int face = t / F, qq = t % F;
+        const int t1 = qq % NX + 1, t2 = qq / NX + 1;
+        const double gv = ghost_dphi<NX>(g, bt, st, snap_rd, stride, b, face, t1, t2);
+        const int ax = face >> 1;
+        int d[3];
+        d[ax] = (face & 1) ? P - 1 : 0;
+        d[ax == 0 ? 1 : 0] = t1;
+        d[ax == 2 ? 1 : 2] = t2;
+        st.dphi[base + (d[2] * P + d[1]) * P + d[0]] = gv;
+    }
+    if (mode == 1) __syncthreads();
     const int c = ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
+    const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
     double v;
     const double resid = relax_brick<NX>(sm, st.dphi + base, st.dphi1 + base, &v);
     st.dphi[base + c] = v;
+    // publish first interior layers: layer of face f holds the cells adjacent to it
+    double* sw = snap_wr + (size_t)b * stride;
+    if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = v;
+    if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = v;
+    if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = v;
+    if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = v;
+    if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = v;
+    if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v;
     if (t == 0) pres[b] = resid;
     // last block: reduce and decide
     __threadfence();
@@ -68,6 +131,7 @@ __global__ void __launch_bounds__(NX* NX* NX)
     if (t == 0) {
         *counter = 0u;
         ctl->relax_calls++;
+        ctl->snap_par[level] = mode == 0 ? 0 : par ^ 1;  // the buffer just written
         if (mode == 0) {
             ctl->r0[level] = r;
             ctl->outer[level] = 0;
@@ -189,25 +253,27 @@ __global__ void k_dt_reduce(BrickTable bt, LevelLists L, int nlevels, const doub
 // ---------------------------------------------------------------------------
 void launch_relax_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int level,
                       int mode, double ratio, cudaGraphConditionalHandle cond, Control* ctl, double* pres,
-                      double* nest, unsigned int* counter, cudaStream_t s) {
+                      double* nest, unsigned int* counter, double* snap, size_t snap_stride, cudaStream_t s) {
     const int n = L.cnt[level];
     if (n <= 0) return;
-    k_relax_dev<8><<<n, 512, 0, s>>>(g, bt, st, L, level, mode, ratio, cond, ctl, pres, nest, counter);
+    // two buffers, each one stride per brick slot of the pool
+    launch_k(k_relax_dev<8>, n, 512, 0, s, g, bt, st, L, level, mode, ratio, cond, ctl, pres, nest, counter, snap,
+                                     snap_stride, snap_stride * (size_t)L.cap);
 }
 
 void launch_error_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int nlevels,
                       double tol, cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest,
                       unsigned int* counter, cudaStream_t s) {
-    k_error_dev<<<L.nall, 256, 0, s>>>(g, bt, st, L, nlevels, tol, cond, ctl, pres, nest, counter);
+    launch_k(k_error_dev, L.nall, 256, 0, s, g, bt, st, L, nlevels, tol, cond, ctl, pres, nest, counter);
 }
 
 void launch_open_loop(cudaGraphConditionalHandle cond, Control* ctl, int reset_cycles, cudaStream_t s) {
-    k_open_loop<<<1, 1, 0, s>>>(cond, ctl, reset_cycles);
+    launch_k(k_open_loop, 1, 1, 0, s, cond, ctl, reset_cycles);
 }
 
 void launch_dt_reduce(const BrickTable& bt, const LevelLists& L, int nlevels, const double* per, double* nest,
                       Control* ctl, double maxdtinc, cudaStream_t s) {
-    k_dt_reduce<<<1, 1024, 0, s>>>(bt, L, nlevels, per, nest, ctl, maxdtinc);
+    launch_k(k_dt_reduce, 1, 1024, 0, s, bt, L, nlevels, per, nest, ctl, maxdtinc);
 }
 
 }  // namespace amr

@@ -8,19 +8,11 @@
 //   Fy [slot][f][k'][j'][i'] faces j'=0..nx
 //   Fz [slot][f][k'][j'][i'] faces k'=0..nx
 #include "euler_state.cuh"
+#include "flux_kernel.cuh"
 #include "kernels.h"
+#include "launch.cuh"
 
 namespace amr {
-
-// index of flux array element for direction d: face index fi (0..nx) along d,
-// transverse interior indices t1 (lower axis) and t2 (higher axis).
-__device__ __forceinline__ int flux_index(int d, int nx, int fi, int t1, int t2) {
-    if (d == 0) return (t2 * nx + t1) * (nx + 1) + fi;
-    if (d == 1) return (t2 * (nx + 1) + fi) * nx + t1;
-    return (fi * nx + t2) * nx + t1;
-}
-
-__device__ __forceinline__ int cell_index(int gnx, int i, int j, int k) { return (k * gnx + j) * gnx + i; }
 
 // ---------------------------------------------------------------------------
 // ghost zones: GridNode::enforce_boundaries (grid_node.cpp:59-112) with the
@@ -110,77 +102,7 @@ __global__ void k_ghost_fill(Geom g, BrickTable bt, DevState st, const int* __re
 // cells keeping a four-cell window of primitives.
 // ---------------------------------------------------------------------------
 __global__ void k_flux_minmod(Geom g, DevState st, const int* __restrict__ slots) {
-    const int b = slots[blockIdx.x];
-    const int nx = g.nx, gnx = g.gnx, bw = g.bw;
-    const int npen = nx * nx;
-    const int d = threadIdx.x / npen;
-    if (d >= 3) return;
-    const int p = threadIdx.x % npen;
-    const int t1 = p % nx, t2 = p / nx;  // interior transverse indices
-    const double* U = st.U + (size_t)b * g.ucount;
-    int stride, base;
-    if (d == 0) {
-        stride = 1;
-        base = cell_index(gnx, 0, t1 + bw, t2 + bw);
-    } else if (d == 1) {
-        stride = gnx;
-        base = cell_index(gnx, t1 + bw, 0, t2 + bw);
-    } else {
-        stride = gnx * gnx;
-        base = cell_index(gnx, t1 + bw, t2 + bw, 0);
-    }
-    double* F = (d == 0 ? st.Fx : (d == 1 ? st.Fy : st.Fz)) + (size_t)b * g.nf * npen * (nx + 1);
-    const int fstride = npen * (nx + 1);
-    const double th = g.theta, gam = g.gamma;
-
-    double w[4][NF_EULER];  // primitives of cells f-2 .. f+1
-    for (int n = 0; n < 3; n++) {
-#pragma unroll
-        for (int l = 0; l < NF_EULER; l++) w[n + 1][l] = U[l * g.gnx3 + base + n * stride];
-        st_to_prim(w[n + 1]);
-    }
-    double sR[NF_EULER];
-    // slope at cell 1 (becomes s[f-1] for the first face f = bw = 2 when
-    // bw == 2); general bw: advance the window up to face bw.
-    for (int n = 3; n < bw + 1; n++) {
-#pragma unroll
-        for (int m = 0; m < 3; m++)
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) w[m][l] = w[m + 1][l];
-#pragma unroll
-        for (int l = 0; l < NF_EULER; l++) w[3][l] = U[l * g.gnx3 + base + n * stride];
-        st_to_prim(w[3]);
-    }
-    // now w[1..3] hold cells bw-2 .. bw (for bw == 2: cells 0,1,2)
-#pragma unroll
-    for (int l = 0; l < NF_EULER; l++) sR[l] = minmod_theta(w[3][l] - w[2][l], w[2][l] - w[1][l], th);
-    for (int f = bw; f <= gnx - bw; f++) {
-        // shift window: w[0..3] = cells f-2, f-1, f, f+1
-#pragma unroll
-        for (int m = 0; m < 3; m++)
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) w[m][l] = w[m + 1][l];
-#pragma unroll
-        for (int l = 0; l < NF_EULER; l++) w[3][l] = U[l * g.gnx3 + base + (f + 1) * stride];
-        st_to_prim(w[3]);
-        double ql[NF_EULER], qr[NF_EULER], sL[NF_EULER];
-#pragma unroll
-        for (int l = 0; l < NF_EULER; l++) {
-            sL[l] = sR[l];  // s[f-1]
-            sR[l] = minmod_theta(w[3][l] - w[2][l], w[2][l] - w[1][l], th);  // s[f]
-            ql[l] = w[1][l] + sL[l] / 2.0;
-            qr[l] = w[2][l] - sR[l] / 2.0;
-        }
-        st_to_con(ql);
-        st_to_con(qr);
-        double fl[NF_EULER], fr[NF_EULER];
-        const double al = st_flux(ql, d, gam, fl);
-        const double ar = st_flux(qr, d, gam, fr);
-        const double a = r_max(al, ar);
-        const int fi = flux_index(d, nx, f - bw, t1, t2);
-#pragma unroll
-        for (int l = 0; l < NF_EULER; l++) F[l * fstride + fi] = ((fl[l] + fr[l]) - (qr[l] - ql[l]) * a) * 0.5;
-    }
+    flux_pencils<double>(g, st, slots[blockIdx.x]);
 }
 
 // ---------------------------------------------------------------------------
@@ -526,52 +448,56 @@ __global__ void k_state_max(Geom g, BrickTable bt, DevState st, const int* __res
 void launch_ghost_fill(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                        cudaStream_t s) {
     if (n <= 0) return;
-    k_ghost_fill<<<dim3(n, 6), 128, 0, s>>>(g, bt, st, slots);
+    launch_k(k_ghost_fill, dim3(n, 6), 128, 0, s, g, bt, st, slots);
 }
 void launch_flux(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
     if (n <= 0) return;
-    k_flux_minmod<<<n, 3 * g.nx * g.nx, 0, s>>>(g, st, slots);
+    if (g.precision == AMR_PREC_MIXED) {
+        launch_flux_f32(g, st, slots, n, s);
+        return;
+    }
+    launch_k(k_flux_minmod, n, 3 * g.nx * g.nx, 0, s, g, st, slots);
 }
 void launch_reflux(const Geom& g, const DevState& st, const RefluxItem* items, int n, cudaStream_t s) {
     if (n <= 0) return;
     const int half = g.nx / 2;
-    k_reflux<<<n, ((g.nf * half * half + 31) / 32) * 32, 0, s>>>(g, st, items);
+    launch_k(k_reflux, n, ((g.nf * half * half + 31) / 32) * 32, 0, s, g, st, items);
 }
 void launch_add_difs(const Geom& g, const DevState& st, const int* slots, int n, const double* hs, double dt,
                      double beta, int gravity, cudaStream_t s, const double* dtp) {
     if (n <= 0) return;
-    k_add_difs<<<n, 256, 0, s>>>(g, st, slots, hs, dt, dtp, beta, gravity);
+    launch_k(k_add_difs, n, 256, 0, s, g, st, slots, hs, dt, dtp, beta, gravity);
 }
 void launch_flow_off(const Geom& g, const DevState& st, int root, double h, double dt, double beta, double* fo,
                      cudaStream_t s, const double* dtp) {
-    k_flow_off<<<1, 32, 0, s>>>(g, st, root, h, dt, dtp, beta, fo);
+    launch_k(k_flow_off, 1, 32, 0, s, g, st, root, h, dt, dtp, beta, fo);
 }
 void launch_inject(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                    cudaStream_t s) {
     if (n <= 0) return;
     const int half = g.nx / 2;
-    k_inject<<<dim3(n, 8), ((half * half * half + 31) / 32) * 32, 0, s>>>(g, bt, st, slots);
+    launch_k(k_inject, dim3(n, 8), ((half * half * half + 31) / 32) * 32, 0, s, g, bt, st, slots);
 }
 void launch_prolong(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                     cudaStream_t s) {
     if (n <= 0) return;
     const int half = g.nx / 2;
-    k_prolong<<<n, ((half * half * half + 31) / 32) * 32, 0, s>>>(g, bt, st, slots);
+    launch_k(k_prolong, n, ((half * half * half + 31) / 32) * 32, 0, s, g, bt, st, slots);
 }
 void launch_max_dt(const Geom& g, const DevState& st, const int* slots, int n, const double* hs, double* dt_out,
                    cudaStream_t s) {
     if (n <= 0) return;
-    k_max_dt<<<n, 192, 0, s>>>(g, st, slots, hs, dt_out);
+    launch_k(k_max_dt, n, 192, 0, s, g, st, slots, hs, dt_out);
 }
 void launch_refine_flags(const Geom& g, const DevState& st, const int* slots, int n, double thr,
                          unsigned char* flags, cudaStream_t s) {
     if (n <= 0) return;
-    k_refine_flags<<<n, 256, 0, s>>>(g, st, slots, thr, flags);
+    launch_k(k_refine_flags, n, 256, 0, s, g, st, slots, thr, flags);
 }
 void launch_state_max(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n, int field,
                       double* out, cudaStream_t s) {
     if (n <= 0) return;
-    k_state_max<<<n, 256, 0, s>>>(g, bt, st, slots, field, out);
+    launch_k(k_state_max, n, 256, 0, s, g, bt, st, slots, field, out);
 }
 
 }  // namespace amr
@@ -595,10 +521,10 @@ __global__ void k_scatter(const double* __restrict__ src, const int* __restrict_
 }
 void launch_gather(const double* src, const int* slots, int n, int count, double* dst, cudaStream_t s) {
     if (n <= 0) return;
-    k_gather<<<dim3((count + 255) / 256, n), 256, 0, s>>>(src, slots, count, dst);
+    launch_k(k_gather, dim3((count + 255) / 256, n), 256, 0, s, src, slots, count, dst);
 }
 void launch_scatter(const double* src, const int* slots, int n, int count, double* dst, cudaStream_t s) {
     if (n <= 0) return;
-    k_scatter<<<dim3((count + 255) / 256, n), 256, 0, s>>>(src, slots, count, dst);
+    launch_k(k_scatter, dim3((count + 255) / 256, n), 256, 0, s, src, slots, count, dst);
 }
 }  // namespace amr

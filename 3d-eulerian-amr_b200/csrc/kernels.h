@@ -11,6 +11,8 @@ namespace amr {
 void launch_ghost_fill(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                        cudaStream_t s);
 void launch_flux(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);
+// hydro_mixed.cu: FP32 reconstruction + flux (used by launch_flux when g.precision is mixed)
+void launch_flux_f32(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);
 void launch_reflux(const Geom& g, const DevState& st, const RefluxItem* items, int n, cudaStream_t s);
 // dtp: when non-null the step is read from device memory (captured graphs)
 void launch_add_difs(const Geom& g, const DevState& st, const int* slots, int n, const double* hs, double dt,

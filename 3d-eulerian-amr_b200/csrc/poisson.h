@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "amr_internal.h"
 
 struct amr_ctx;
@@ -15,10 +17,25 @@ void launch_poisson_new_bricks(const Geom& g, const BrickTable& bt, const DevSta
 void launch_set_source(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);
 void launch_source_sums(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                         double* msrc, int* allref, cudaStream_t s);
-// scratch: (point, brick) own sums, scratch_cap doubles; points are batched
-void launch_phys_bound(const Geom& g, const BrickTable& bt, const int* bfaces, int nbf, const int* order, int n,
-                       const double* msrc, const int* allref, double* bphi, double* scratch, size_t scratch_cap,
-                       cudaStream_t s);
+// Walk program of the domain-face potential sum over the DFS-ordered bricks:
+// segs[2s], segs[2s+1] = DFS entry range of subtree s; top = the walk above
+// the subtrees (entry e >= 0, or subtree s as -s-1).  Device pointers.
+struct PhysWalk {
+    const int* segs;
+    int nseg;
+    const int* top;
+    int ntop;
+};
+// Split the DFS-ordered brick levels into subtrees of at most `limit` bricks
+// and the walk above them (host).
+void build_phys_walk(const int* levels, int n, int limit, std::vector<int>& segs, std::vector<int>& top);
+// The context's walk program (device pointers into its walk buffer).
+PhysWalk phys_walk(const amr_ctx* c);
+// scratch: (subtree, point) partial sums, scratch_cap doubles; points are
+// batched so that one batch fits.  Returns -1 when not even one point fits.
+int launch_phys_bound(const Geom& g, const BrickTable& bt, const int* bfaces, int nbf, const int* order,
+                      const PhysWalk& w, const double* msrc, const int* allref, double* bphi, double* scratch,
+                      size_t scratch_cap, cudaStream_t s);
 void launch_phi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,
                            const int* slots, int n, cudaStream_t s);
 void launch_dphi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,

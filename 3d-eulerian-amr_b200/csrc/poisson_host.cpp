@@ -248,9 +248,40 @@ int check_device_error(amr_ctx* c) {
 
 }  // namespace
 
+namespace amr {
+PhysWalk phys_walk(const amr_ctx* c) {
+    return PhysWalk{c->d_pwalk, c->n_pseg, c->d_pwalk + 2 * c->n_pseg, c->n_ptop};
+}
+
+void build_phys_walk(const int* levels, int n, int limit, std::vector<int>& segs, std::vector<int>& top) {
+    segs.clear();
+    top.clear();
+    // end[e]: one past the last DFS entry of e's subtree
+    std::vector<int> end(n, n), open;
+    for (int e = 0; e < n; e++) {
+        while (!open.empty() && levels[open.back()] >= levels[e]) {
+            end[open.back()] = e;
+            open.pop_back();
+        }
+        open.push_back(e);
+    }
+    for (int e = 0; e < n;) {
+        if (end[e] - e <= limit) {
+            top.push_back(-(int)(segs.size() / 2) - 1);
+            segs.push_back(e);
+            segs.push_back(end[e]);
+            e = end[e];
+        } else {
+            top.push_back(e);
+            e++;
+        }
+    }
+}
+}  // namespace amr
+
 void amr_poisson_release(amr_ctx* c) {
     if (!c) return;
-    void* ptrs[] = {c->d_bphi, c->d_msrc, c->d_allref, c->d_pres, c->d_bfaces, c->d_perr, c->d_own};
+    void* ptrs[] = {c->d_bphi, c->d_msrc, c->d_allref, c->d_pres, c->d_bfaces, c->d_perr, c->d_own, c->d_pwalk};
     for (void* p : ptrs)
         if (p) cudaFree(p);
 }
@@ -314,8 +345,11 @@ int amr_poisson_boundaries(amr_ctx* c) {
     }
     {
         ProfScope ps_(c->prof, KC_PHYS_BOUND, c->stream);
-        launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, all(c), nall(c), c->d_msrc, c->d_allref, c->d_bphi,
-                          c->d_own, c->own_cap, c->stream);
+        if (launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, all(c), phys_walk(c), c->d_msrc, c->d_allref,
+                              c->d_bphi, c->d_own, c->own_cap, c->stream)) {
+            c->err = "domain-face potential scratch too small";
+            return AMR_ERR_STATE;
+        }
     }
     return check_launch(c);
 }

@@ -7,8 +7,11 @@
 #include "euler_state.cuh"
 #include "poisson.h"
 #include "relax_brick.cuh"
+#include "launch.cuh"
 
 namespace amr {
+
+constexpr int MAX_NEST = 16;  // refinement levels 0..12 (amr_create rejects deeper trees)
 
 __device__ __forceinline__ int pidx(int pnx, int i, int j, int k) { return (k * pnx + j) * pnx + i; }
 
@@ -139,16 +142,11 @@ __device__ __forceinline__ void bound_point(const Geom& g, const BrickTable& bt,
     if (where) *where = ((b * 6 + face) * pnx * pnx) + a * pnx + cc;
 }
 
-__global__ void k_phys_own(Geom g, BrickTable bt, const int* __restrict__ bfaces, int p0, int np, int n,
-                           const double* __restrict__ msrc, const int* __restrict__ allref, double* __restrict__ own) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;  // point within the batch
-    const int e = blockIdx.y;                              // brick (DFS entry)
-    if (p >= np) return;
-    double xyz[3];
-    bound_point(g, bt, bfaces, p0 + p, xyz, nullptr);
-    const double alpha = g.z_reflect ? 2.0 : 1.0;
-    const double* m = msrc + (size_t)e * 32;
-    const bool ar = allref[e] != 0;
+// Potential at point xyz of one brick's eight octant monopoles
+// (PoissonPhysBound::compute_boundaries, poisson_phys_bound.cpp:70-81: a
+// fully refined brick contributes 0).
+__device__ __forceinline__ double own_term(const double* xyz, const double* __restrict__ m, bool ar,
+                                           double alpha) {
     double sum = 0.0;
     for (int q = 0; q < 8; q++) {
         const double dx = xyz[0] - m[4 * q + 1], dy = xyz[1] - m[4 * q + 2], dz = xyz[2] - m[4 * q + 3];
@@ -158,32 +156,77 @@ __global__ void k_phys_own(Geom g, BrickTable bt, const int* __restrict__ bfaces
             sum = 0.0;
         }
     }
-    own[(size_t)e * np + p] = sum;
+    return sum;
 }
 
-__global__ void k_phys_accum(Geom g, BrickTable bt, const int* __restrict__ bfaces, const int* __restrict__ order,
-                             int p0, int np, int n, const double* __restrict__ own, double* __restrict__ bphi) {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= np) return;
-    double acc[16];
+// Nested sum of the reference's recursion: a brick's value is its own term
+// plus its children's subtree values, added child by child in DFS order.
+// acc[l] holds the running value of the open brick at level l.
+struct NestStack {
+    double acc[MAX_NEST];
     int depth = -1;
-    for (int e = 0; e < n; e++) {
-        const int L = bt.level[order[e]];
+    __device__ __forceinline__ void push(int L, double v) {
         while (depth >= L) {
             acc[depth - 1] += acc[depth];
             depth--;
         }
-        acc[L] = own[(size_t)e * np + p];
+        acc[L] = v;
         depth = L;
     }
-    while (depth > 0) {
-        acc[depth - 1] += acc[depth];
-        depth--;
+    __device__ __forceinline__ double close(int L0) {
+        while (depth > L0) {
+            acc[depth - 1] += acc[depth];
+            depth--;
+        }
+        return acc[L0];
     }
+};
+
+// Pass 1: thread (point p, subtree s) forms the nested sum of subtree s
+// (DFS entries segs[2s] .. segs[2s+1]-1, a brick and all its descendants)
+// and leaves it in part[s][p].
+__global__ void k_phys_seg(Geom g, BrickTable bt, const int* __restrict__ bfaces, const int* __restrict__ order,
+                           const int* __restrict__ segs, int p0, int np, const double* __restrict__ msrc,
+                           const int* __restrict__ allref, double* __restrict__ part) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    const int sg = blockIdx.y;
+    if (p >= np) return;
+    double xyz[3];
+    bound_point(g, bt, bfaces, p0 + p, xyz, nullptr);
+    const double alpha = g.z_reflect ? 2.0 : 1.0;
+    const int e0 = segs[2 * sg], e1 = segs[2 * sg + 1];
+    const int L0 = bt.level[order[e0]];
+    NestStack st;
+    for (int e = e0; e < e1; e++)
+        st.push(bt.level[order[e]], own_term(xyz, msrc + (size_t)e * 32, allref[e] != 0, alpha));
+    part[(size_t)sg * np + p] = st.close(L0);
+}
+
+// Pass 2: thread p walks the bricks above the subtrees (own terms formed
+// here) and the subtrees themselves (their sums from pass 1) in DFS order,
+// giving the same additions in the same order as one walk over all bricks.
+// top[t] >= 0: a DFS entry; top[t] < 0: subtree -top[t]-1.
+__global__ void k_phys_top(Geom g, BrickTable bt, const int* __restrict__ bfaces, const int* __restrict__ order,
+                           const int* __restrict__ segs, const int* __restrict__ top, int ntop, int p0, int np,
+                           const double* __restrict__ msrc, const int* __restrict__ allref,
+                           const double* __restrict__ part, double* __restrict__ bphi) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
     double xyz[3];
     int where;
     bound_point(g, bt, bfaces, p0 + p, xyz, &where);
-    bphi[where] = acc[0];
+    const double alpha = g.z_reflect ? 2.0 : 1.0;
+    NestStack st;
+    for (int t = 0; t < ntop; t++) {
+        const int code = top[t];
+        if (code >= 0) {
+            st.push(bt.level[order[code]], own_term(xyz, msrc + (size_t)code * 32, allref[code] != 0, alpha));
+        } else {
+            const int sg = -code - 1;
+            st.push(bt.level[order[segs[2 * sg]]], part[(size_t)sg * np + p]);
+        }
+    }
+    bphi[where] = st.close(0);
 }
 
 // ---------------------------------------------------------------------------
@@ -710,7 +753,7 @@ __global__ void k_poisson_new(Geom g, BrickTable bt, DevState st, const int* __r
 void launch_poisson_new_bricks(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                                cudaStream_t s) {
     if (n <= 0) return;
-    k_poisson_new<<<n, 256, 0, s>>>(g, bt, st, slots);
+    launch_k(k_poisson_new, n, 256, 0, s, g, bt, st, slots);
 }
 
 }  // namespace amr
@@ -718,86 +761,92 @@ void launch_poisson_new_bricks(const Geom& g, const BrickTable& bt, const DevSta
 namespace amr {
 
 void launch_set_source(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
-    if (n > 0) k_set_source<<<n, 256, 0, s>>>(g, st, slots);
+    if (n > 0) launch_k(k_set_source, n, 256, 0, s, g, st, slots);
 }
 void launch_source_sums(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                         double* msrc, int* allref, cudaStream_t s) {
-    if (n > 0) k_source_sums<<<n, 32, 0, s>>>(g, bt, st, slots, msrc, allref);
+    if (n > 0) launch_k(k_source_sums, n, 32, 0, s, g, bt, st, slots, msrc, allref);
 }
-void launch_phys_bound(const Geom& g, const BrickTable& bt, const int* bfaces, int nbf, const int* order, int n,
-                       const double* msrc, const int* allref, double* bphi, double* scratch, size_t scratch_cap,
-                       cudaStream_t s) {
-    if (nbf <= 0 || n <= 0) return;
+int launch_phys_bound(const Geom& g, const BrickTable& bt, const int* bfaces, int nbf, const int* order,
+                      const PhysWalk& w, const double* msrc, const int* allref, double* bphi, double* scratch,
+                      size_t scratch_cap, cudaStream_t s) {
+    if (nbf <= 0 || w.ntop <= 0) return 0;
     const int npts = nbf * g.pnx * g.pnx;
-    const int batch = (int)std::min<size_t>((size_t)npts, scratch_cap / (size_t)n);
+    const size_t per = (size_t)std::max(w.nseg, 1);
+    if (scratch_cap < per) return -1;
+    const int batch = (int)std::min<size_t>((size_t)npts, scratch_cap / per);
     for (int p0 = 0; p0 < npts; p0 += batch) {
         const int np = std::min(batch, npts - p0);
-        k_phys_own<<<dim3((np + 127) / 128, n), 128, 0, s>>>(g, bt, bfaces, p0, np, n, msrc, allref, scratch);
-        k_phys_accum<<<(np + 127) / 128, 128, 0, s>>>(g, bt, bfaces, order, p0, np, n, scratch, bphi);
+        if (w.nseg > 0)
+            launch_k(k_phys_seg, dim3((np + 127) / 128, w.nseg), 128, 0, s, g, bt, bfaces, order, w.segs, p0, np, msrc,
+                                                                      allref, scratch);
+        launch_k(k_phys_top, (np + 63) / 64, 64, 0, s, g, bt, bfaces, order, w.segs, w.top, w.ntop, p0, np, msrc, allref,
+                                                 scratch, bphi);
     }
+    return 0;
 }
 void launch_phi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,
                            const int* slots, int n, cudaStream_t s) {
     if (n <= 0) return;
     PoissonAux aux{bphi, err};
-    k_phi_faces<<<dim3(n, 6), 64, 0, s>>>(g, bt, st, aux, slots, 0);
-    k_phi_edges<<<n, g.pnx - 2, 0, s>>>(g, bt, st, aux, slots);
-    k_phi_vertices<<<n, 32, 0, s>>>(g, bt, st, aux, slots);
+    launch_k(k_phi_faces, dim3(n, 6), 64, 0, s, g, bt, st, aux, slots, 0);
+    launch_k(k_phi_edges, n, g.pnx - 2, 0, s, g, bt, st, aux, slots);
+    launch_k(k_phi_vertices, n, 32, 0, s, g, bt, st, aux, slots);
 }
 void launch_dphi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,
                             const int* slots, int n, cudaStream_t s) {
     if (n <= 0) return;
     PoissonAux aux{bphi, err};
-    k_phi_faces<<<dim3(n, 6), 64, 0, s>>>(g, bt, st, aux, slots, 1);
+    launch_k(k_phi_faces, dim3(n, 6), 64, 0, s, g, bt, st, aux, slots, 1);
 }
 void launch_phi_from_children(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                               cudaStream_t s) {
     const int half = (g.pnx - 2) / 2;
-    if (n > 0) k_phi_from_children<<<dim3(n, 8), ((half * half * half + 31) / 32) * 32, 0, s>>>(g, bt, st, slots);
+    if (n > 0) launch_k(k_phi_from_children, dim3(n, 8), ((half * half * half + 31) / 32) * 32, 0, s, g, bt, st, slots);
 }
 void launch_init_vcycle(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
-    if (n > 0) k_init_vcycle<<<n, 256, 0, s>>>(g, st, slots);
+    if (n > 0) launch_k(k_init_vcycle, n, 256, 0, s, g, st, slots);
 }
 void launch_vdown_a(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                     cudaStream_t s) {
-    if (n > 0) k_vdown_a<<<n, 256, 0, s>>>(g, bt, st, slots);
+    if (n > 0) launch_k(k_vdown_a, n, 256, 0, s, g, bt, st, slots);
 }
 void launch_adjust_dphi(const Geom& g, const BrickTable& bt, const DevState& st, const RefluxItem* items, int n,
                         cudaStream_t s) {
-    if (n > 0) k_adjust_dphi<<<n, 32, 0, s>>>(g, bt, st, items);
+    if (n > 0) launch_k(k_adjust_dphi, n, 32, 0, s, g, bt, st, items);
 }
 void launch_vdown_c(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                     cudaStream_t s) {
-    if (n > 0) k_vdown_c<<<n, 256, 0, s>>>(g, bt, st, slots);
+    if (n > 0) launch_k(k_vdown_c, n, 256, 0, s, g, bt, st, slots);
 }
 int launch_relax(const Geom& g, const DevState& st, const int* slots, int n, double* out, int* sweeps,
                  cudaStream_t s) {
     if (n <= 0) return 0;
     if (g.nx != 8) return -1;
-    k_relax<8><<<n, 512, 0, s>>>(g, st, slots, out, sweeps);
+    launch_k(k_relax<8>, n, 512, 0, s, g, st, slots, out, sweeps);
     return 0;
 }
 void launch_coarse_correction(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                               cudaStream_t s) {
     const int half = (g.pnx - 2) / 2;
-    if (n > 0) k_coarse_correction<<<n, ((half * half * half + 31) / 32) * 32, 0, s>>>(g, bt, st, slots);
+    if (n > 0) launch_k(k_coarse_correction, n, ((half * half * half + 31) / 32) * 32, 0, s, g, bt, st, slots);
 }
 void launch_retire(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
-    if (n > 0) k_retire<<<n, 256, 0, s>>>(g, st, slots);
+    if (n > 0) launch_k(k_retire, n, 256, 0, s, g, st, slots);
 }
 void launch_forces(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                    cudaStream_t s) {
-    if (n > 0) k_forces<<<n, 256, 0, s>>>(g, bt, st, slots);
+    if (n > 0) launch_k(k_forces, n, 256, 0, s, g, bt, st, slots);
 }
 void launch_adjust_force(const Geom& g, const DevState& st, const RefluxItem* items, int n, cudaStream_t s) {
-    if (n > 0) k_adjust_force<<<n, 32, 0, s>>>(g, st, items);
+    if (n > 0) launch_k(k_adjust_force, n, 32, 0, s, g, st, items);
 }
 void launch_solution_error(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                            double* out, cudaStream_t s) {
-    if (n > 0) k_solution_error<<<n, 256, 0, s>>>(g, bt, st, slots, out);
+    if (n > 0) launch_k(k_solution_error, n, 256, 0, s, g, bt, st, slots, out);
 }
 void launch_phi_time(const Geom& g, const DevState& st, const int* slots, int n, int mode, cudaStream_t s) {
-    if (n > 0) k_phi_time<<<n, 256, 0, s>>>(g, st, slots, mode);
+    if (n > 0) launch_k(k_phi_time, n, 256, 0, s, g, st, slots, mode);
 }
 
 }  // namespace amr

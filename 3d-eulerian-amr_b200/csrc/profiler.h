@@ -7,6 +7,8 @@
 
 #include <vector>
 
+#include "amr_internal.h"
+
 namespace amr {
 
 enum KernelClass {
@@ -88,13 +90,15 @@ struct ProfScope {
     cudaStream_t s;
     cudaEvent_t a;
     long long n;
-    ProfScope(Profiler& p_, int cls_, cudaStream_t s_, long long n_ = 0) : p(p_), cls(cls_), s(s_), n(n_) {
-        // kernels issued by the bracketed wrapper (the phi ghost fill issues
-        // faces, edges and vertices as three kernels)
-        p.kernels += (cls == KC_PHI_BOUND) ? 3 : 1;
+    long long tally0;  // launch tally when the bracket opened
+    ProfScope(Profiler& p_, int cls_, cudaStream_t s_, long long n_ = 0)
+        : p(p_), cls(cls_), s(s_), n(n_), tally0(g_launch_tally) {
         p.begin(cls, s, &a);
     }
-    ~ProfScope() { p.end(cls, s, a, n); }
+    ~ProfScope() {
+        p.kernels += g_launch_tally - tally0;
+        p.end(cls, s, a, n);
+    }
 };
 
 }  // namespace amr
