@@ -150,6 +150,18 @@ int amr_poisson_solve(amr_ctx* ctx, double tol, int max_cycles, double* l1_error
 int amr_store_phi(amr_ctx* ctx);                           /* poisson.cpp:166-181 */
 int amr_restore_phi(amr_ctx* ctx);                         /* poisson.cpp:183-198 */
 int amr_restore_half_phi(amr_ctx* ctx);                    /* poisson.cpp:200-221 */
+/* amr_poisson_boundaries without any device allocation.  No counterpart in
+ * the reference: it is for host codes that may not call cudaMalloc once they
+ * run (all free device memory handed to their own pool allocator, or a
+ * section where an allocation's implicit device synchronisation is not
+ * allowed).  Its scratch is a 16 MiB static device array inside this library
+ * (held on every GPU that loads the library until exit, shared by all calls:
+ * calls that overlap on the GPU race).  It needs the context's Poisson
+ * buffers to exist (one earlier ordinary Poisson call, else AMR_ERR_STATE)
+ * and rejects trees whose per-point subtree sums exceed the scratch
+ * (AMR_ERR_RANGE).  The first call on a device looks up the scratch address;
+ * make it before any stream capture.  The context's device must be current. */
+int amr_poisson_boundaries_noalloc(amr_ctx* ctx);
 /* Self-gravitating RK3 step (binary/binary_driver.cpp:346-459 sequence on the
  * Euler state): per substep hydro + gravity sources, phi time level, solve;
  * regrid every 8 steps at state_max/dynamic_range. */
