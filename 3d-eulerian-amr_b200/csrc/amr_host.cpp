@@ -268,6 +268,43 @@ int rebuild_topology(amr_ctx* c) {
             }
         }
     }
+    // per coarse brick, in level-list order: its x, then y, then z items
+    {
+        std::vector<RefluxItem> vitems;
+        std::vector<int> vr;
+        c->off_vrange.assign(maxl + 1, 0);
+        std::vector<int> pos(c->cap > 0 ? c->cap : 1, -1);
+        for (int l = 0; l <= maxl; l++) {
+            c->off_vrange[l] = (int)vr.size() / 4;
+            const std::vector<int>& ls = c->level_slots[l];
+            for (int q = 0; q < (int)ls.size(); q++) pos[ls[q]] = q;
+            std::vector<std::vector<RefluxItem>> by(ls.size() * 3);
+            for (const RefluxItem& it : c->reflux[l]) by[3 * pos[it.coarse] + it.dir].push_back(it);
+            for (int q = 0; q < (int)ls.size(); q++) {
+                for (int d = 0; d < 3; d++) {
+                    vr.push_back((int)vitems.size());
+                    vitems.insert(vitems.end(), by[3 * q + d].begin(), by[3 * q + d].end());
+                }
+                vr.push_back((int)vitems.size());
+            }
+        }
+        if ((int)vitems.size() > c->vitems_cap) {
+            if (c->d_vitems) cudaFree(c->d_vitems);
+            c->vitems_cap = (int)vitems.size() * 2 + 64;
+            CUDA_TRY(cudaMalloc(&c->d_vitems, sizeof(RefluxItem) * c->vitems_cap));
+        }
+        if ((int)vr.size() > c->vranges_cap) {
+            if (c->d_vranges) cudaFree(c->d_vranges);
+            c->vranges_cap = (int)vr.size() * 2 + 64;
+            CUDA_TRY(cudaMalloc(&c->d_vranges, sizeof(int) * c->vranges_cap));
+        }
+        if (!vitems.empty())
+            CUDA_TRY(cudaMemcpyAsync(c->d_vitems, vitems.data(), sizeof(RefluxItem) * vitems.size(),
+                                     cudaMemcpyHostToDevice, c->stream));
+        if (!vr.empty())
+            CUDA_TRY(cudaMemcpyAsync(c->d_vranges, vr.data(), sizeof(int) * vr.size(), cudaMemcpyHostToDevice,
+                                     c->stream));
+    }
     if ((int)items.size() > c->d_reflux_cap) {
         if (c->d_reflux) cudaFree(c->d_reflux);
         c->d_reflux_cap = (int)items.size() * 2 + 64;
@@ -463,6 +500,10 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
             double** parr[8] = {&c->st.phi, &c->st.phi0, &c->st.dphi, &c->st.dphi1,
                                 &c->st.S,   &c->st.fx,   &c->st.fy,   &c->st.fz};
             for (auto p : parr) rc |= dev_alloc(c, p, (size_t)cap * g.pnx3);
+            if (cfg->precision == AMR_PREC_MIXED) {
+                rc |= dev_alloc(c, &c->st.fdphi, (size_t)cap * g.pnx3);
+                rc |= dev_alloc(c, &c->st.fdphi1, (size_t)cap * g.pnx3);
+            }
         }
         rc |= dev_alloc(c, &c->bt.level, cap);
         rc |= dev_alloc(c, &c->bt.off, 3 * (size_t)cap);
@@ -512,7 +553,8 @@ int amr_destroy(amr_ctx* c) {
                         c->st.phi0, c->st.dphi, c->st.dphi1,  c->st.S,      c->st.fx,      c->st.fy,
                         c->st.fz,   c->bt.level, c->bt.off,   c->bt.h,      c->bt.ftype,   c->bt.fnbr,
                         c->bt.parent, c->bt.cidx, c->bt.child, c->d_fo,     c->d_dt,       c->d_red,
-                        c->d_flags, c->d_stage, c->d_slots,  c->d_reflux};
+                        c->d_flags, c->d_stage, c->d_slots,  c->d_reflux, c->d_vitems, c->d_vranges,
+                        c->st.fdphi, c->st.fdphi1};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         amr_poisson_release(c);

@@ -55,6 +55,10 @@ struct DevState {
     double* fx;
     double* fy;
     double* fz;
+    // mixed-precision form: the V-cycle correction (dphi, dphi1) in FP32;
+    // null in the FP64 form
+    float* fdphi;
+    float* fdphi1;
 };
 
 // One coarse-fine flux (or force) correction task: coarse brick's face

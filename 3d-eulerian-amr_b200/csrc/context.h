@@ -62,6 +62,13 @@ struct amr_ctx {
     int* d_pwalk = nullptr;     // subtree ranges [nseg][2] | top-level walk [ntop]
     int pwalk_cap = 0, n_pseg = 0, n_ptop = 0;
     std::vector<int> off_reflux_dir;  // [(maxl+1)*3+1] items sorted by (level, dir)
+    // the same items grouped by coarse brick for the fused V-cycle down
+    // sweep: d_vitems in level-list order, x then y then z per brick;
+    // d_vranges[4 (off_vrange[l] + q) + 0..3] = first x, y, z item, end
+    amr::RefluxItem* d_vitems = nullptr;
+    int* d_vranges = nullptr;
+    int vitems_cap = 0, vranges_cap = 0;
+    std::vector<int> off_vrange;
     int vcycle_max_outer = 1000;
     long long relax_calls = 0, relax_sweeps_total = 0;
     bool topo_dirty = true;

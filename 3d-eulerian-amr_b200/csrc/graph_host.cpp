@@ -223,18 +223,12 @@ int rec_vcycle(amr_ctx* c, cudaStream_t s, int depth, cudaGraphConditionalHandle
     launch_init_vcycle(c->geom, c->st, all(c), nall(c), s);
     TRY(launched(c, __LINE__));
     for (int l = maxlevel; l >= 0; l--) {
-        launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
-        launch_vdown_a(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
-        for (int dir = 0; dir < 3; dir++) {
-            const int a = c->off_reflux_dir[3 * l + dir], b = c->off_reflux_dir[3 * l + dir + 1];
-            launch_adjust_dphi(c->geom, c->bt, c->st, c->d_reflux + a, b - a, s);
-        }
-        launch_vdown_c(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
+        launch_vdown(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->d_vitems, c->d_vranges + 4 * c->off_vrange[l],
+                     s);
         TRY(launched(c, __LINE__));
         TRY(rec_relax_until(c, s, l, 1.0, depth));
     }
     for (int l = 0; l <= maxlevel; l++) {
-        launch_dphi_boundaries(c->geom, c->bt, c->st, c->d_bphi, c->d_perr, lvl(c, l), nlvl(c, l), s);
         if (l > 0) launch_coarse_correction(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), s);
         TRY(launched(c, __LINE__));
         TRY(rec_relax_until(c, s, l, 0.05, depth));

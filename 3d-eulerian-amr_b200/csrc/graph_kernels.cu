@@ -6,6 +6,7 @@
 // V-cycles or relaxation passes.  FP64, compiled with --fmad=false.
 #include <cuda_runtime.h>
 
+#include "corr.cuh"
 #include "euler_state.cuh"
 #include "graph.h"
 #include "relax_brick.cuh"
@@ -53,14 +54,15 @@ __device__ double nested_sum_block(const LevelLists& L, const int* __restrict__ 
 // also stores them into its global ghost cells, so the arrays end the loop
 // exactly as the reference leaves them.  Every pass publishes its new first
 // interior layers for the next pass.
-template <int NX>
-__device__ __forceinline__ double ghost_dphi(const Geom& g, const BrickTable& bt, const DevState& st,
-                                             const double* snap_rd, size_t stride, int b, int face, int t1, int t2) {
+template <int NX, typename CT>
+__device__ __forceinline__ CT ghost_dphi(const Geom& g, const BrickTable& bt, const DevState& st, const CT* snap_rd,
+                                         size_t stride, int b, int face, int t1, int t2) {
     constexpr int P = NX + 2;
     const int kind = bt.ftype[6 * b + face];
     const int nbr = bt.fnbr[6 * b + face];
+    const CT* D = Corr<CT>::dphi(st);
     if (kind == FACE_SIB) return __ldcg(snap_rd + (size_t)nbr * stride + ((face ^ 1) * NX + (t1 - 1)) * NX + (t2 - 1));
-    if (kind == FACE_OUTFLOW) return 0.0;
+    if (kind == FACE_OUTFLOW) return CT(0);
     const int ax = face >> 1;
     int q[3];
     q[ax] = (face & 1) ? 1 : P - 2;
@@ -68,7 +70,7 @@ __device__ __forceinline__ double ghost_dphi(const Geom& g, const BrickTable& bt
     q[ax == 2 ? 1 : 2] = t2;
     if (kind == FACE_REFLECT) {  // own value mirrored through z = 0, before this pass
         const int kk = q[2] == 1 ? P - 2 : 1;
-        return st.dphi[(size_t)b * P * P * P + (kk * P + q[1]) * P + q[0]];
+        return D[(size_t)b * P * P * P + (kk * P + q[1]) * P + q[0]];
     }
     const int v = (face & 1) ? 1 : -1;
     int r[3];
@@ -76,43 +78,44 @@ __device__ __forceinline__ double ghost_dphi(const Geom& g, const BrickTable& bt
         const int rel = bt.off[3 * b + d] + (d == ax ? v * (P - 2) : 0) - 2 * bt.off[3 * nbr + d] - (g.bw - 1);
         r[d] = (rel + q[d]) / 2;
     }
-    return st.dphi[(size_t)nbr * P * P * P + (r[2] * P + r[1]) * P + r[0]];
+    return D[(size_t)nbr * P * P * P + (r[2] * P + r[1]) * P + r[0]];
 }
 
-template <int NX>
+template <int NX, typename CT>
 __global__ void __launch_bounds__(NX* NX* NX)
     k_relax_dev(Geom g, BrickTable bt, DevState st, LevelLists L, int level, int mode, double ratio,
                 cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest, unsigned int* counter,
-                double* snap, size_t stride, size_t snap_half) {
+                CT* snap, size_t stride, size_t snap_half) {
     constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX;
-    __shared__ RelaxSmem<NX> sm;
+    __shared__ RelaxSmem<NX, CT> sm;
+    CT* D = Corr<CT>::dphi(st);
     __shared__ bool last;
     const int b = L.slots[L.off[level] + blockIdx.x];
     const size_t base = (size_t)b * P3;
     const int t = threadIdx.x;
     // snapshot buffers: the previous pass wrote buffer `par`, this one writes par^1
     const int par = mode == 0 ? 0 : ctl->snap_par[level];
-    const double* snap_rd = snap + (size_t)par * snap_half;
-    double* snap_wr = snap + (size_t)(mode == 0 ? 0 : par ^ 1) * snap_half;
+    const CT* snap_rd = snap + (size_t)par * snap_half;
+    CT* snap_wr = snap + (size_t)(mode == 0 ? 0 : par ^ 1) * snap_half;
     if (mode == 1 && t < 6 * F) {
         const int face = t / F, qq = t % F;
         const int t1 = qq % NX + 1, t2 = qq / NX + 1;
-        const double gv = ghost_dphi<NX>(g, bt, st, snap_rd, stride, b, face, t1, t2);
+        const CT gv = ghost_dphi<NX, CT>(g, bt, st, snap_rd, stride, b, face, t1, t2);
         const int ax = face >> 1;
         int d[3];
         d[ax] = (face & 1) ? P - 1 : 0;
         d[ax == 0 ? 1 : 0] = t1;
         d[ax == 2 ? 1 : 2] = t2;
-        st.dphi[base + (d[2] * P + d[1]) * P + d[0]] = gv;
+        D[base + (d[2] * P + d[1]) * P + d[0]] = gv;
     }
     if (mode == 1) __syncthreads();
     const int c = ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
     const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
-    double v;
-    const double resid = relax_brick<NX>(sm, st.dphi + base, st.dphi1 + base, &v);
-    st.dphi[base + c] = v;
+    CT v;
+    const double resid = relax_brick<NX, CT>(sm, D + base, Corr<CT>::dphi1(st) + base, &v);
+    D[base + c] = v;
     // publish first interior layers: layer of face f holds the cells adjacent to it
-    double* sw = snap_wr + (size_t)b * stride;
+    CT* sw = snap_wr + (size_t)b * stride;
     if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = v;
     if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = v;
     if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = v;
@@ -150,9 +153,11 @@ __global__ void __launch_bounds__(NX* NX* NX)
 
 // Poisson::solution_error (poisson.cpp:637-669) + the solve loop condition
 // (error > tol, bounded by max_cycles).
+template <typename CT>
 __global__ void k_error_dev(Geom g, BrickTable bt, DevState st, LevelLists L, int nlevels, double tol,
                             cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest,
                             unsigned int* counter) {
+    CT* D = Corr<CT>::dphi(st);
     const int b = L.all[blockIdx.x];
     const int pnx = g.pnx, nx = pnx - 2, half = nx / 2;
     const double h = bt.h[b];
@@ -170,10 +175,10 @@ __global__ void k_error_dev(Geom g, BrickTable bt, DevState st, LevelLists L, in
             df -= (st.fy[base + c + pnx] - st.fy[base + c]) * hinv;
             df -= (st.fz[base + c + pnx * pnx] - st.fz[base + c]) * hinv;
             const double r = df - st.S[base + c];
-            st.dphi[base + c] = r;
+            D[base + c] = CT(r);
             sum += fabs(r) * h3;
         } else {
-            st.dphi[base + c] = 0.0;
+            D[base + c] = CT(0);
         }
     }
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -256,15 +261,23 @@ void launch_relax_dev(const Geom& g, const BrickTable& bt, const DevState& st, c
                       double* nest, unsigned int* counter, double* snap, size_t snap_stride, cudaStream_t s) {
     const int n = L.cnt[level];
     if (n <= 0) return;
-    // two buffers, each one stride per brick slot of the pool
-    launch_k(k_relax_dev<8>, n, 512, 0, s, g, bt, st, L, level, mode, ratio, cond, ctl, pres, nest, counter, snap,
-                                     snap_stride, snap_stride * (size_t)L.cap);
+    // two buffers, each one stride per brick slot of the pool (FP32 entries
+    // in the mixed form, in the same allocation)
+    if (g.precision == AMR_PREC_MIXED)
+        launch_k(k_relax_dev<8, float>, n, 512, 0, s, g, bt, st, L, level, mode, ratio, cond, ctl, pres, nest, counter,
+                 reinterpret_cast<float*>(snap), snap_stride, snap_stride * (size_t)L.cap);
+    else
+        launch_k(k_relax_dev<8, double>, n, 512, 0, s, g, bt, st, L, level, mode, ratio, cond, ctl, pres, nest,
+                 counter, snap, snap_stride, snap_stride * (size_t)L.cap);
 }
 
 void launch_error_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int nlevels,
                       double tol, cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest,
                       unsigned int* counter, cudaStream_t s) {
-    launch_k(k_error_dev, L.nall, 256, 0, s, g, bt, st, L, nlevels, tol, cond, ctl, pres, nest, counter);
+    if (g.precision == AMR_PREC_MIXED)
+        launch_k(k_error_dev<float>, L.nall, 256, 0, s, g, bt, st, L, nlevels, tol, cond, ctl, pres, nest, counter);
+    else
+        launch_k(k_error_dev<double>, L.nall, 256, 0, s, g, bt, st, L, nlevels, tol, cond, ctl, pres, nest, counter);
 }
 
 void launch_open_loop(cudaGraphConditionalHandle cond, Control* ctl, int reset_cycles, cudaStream_t s) {

@@ -43,14 +43,12 @@ void launch_dphi_boundaries(const Geom& g, const BrickTable& bt, const DevState&
 void launch_phi_from_children(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                               cudaStream_t s);
 void launch_init_vcycle(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);
-void launch_vdown_a(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
-                    cudaStream_t s);
-void launch_adjust_dphi(const Geom& g, const BrickTable& bt, const DevState& st, const RefluxItem* items, int n,
-                        cudaStream_t s);
-void launch_vdown_c(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
-                    cudaStream_t s);
-int launch_relax(const Geom& g, const DevState& st, const int* slots, int n, double* out, int* sweeps,
-                 cudaStream_t s);
+// vcycle_down of one level (residual / child averages, adjust_{x,y,z}_dphi,
+// dphi1 = dphi) in one launch; ranges[4 q + 0..3] = first x, y, z item of
+// the brick at list position q in `items` and the end of its items.
+void launch_vdown(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                  const RefluxItem* items, const int* ranges, cudaStream_t s);
+int launch_relax(const Geom& g, const DevState& st, const int* slots, int n, double* out, cudaStream_t s);
 void launch_coarse_correction(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                               cudaStream_t s);
 void launch_retire(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s);

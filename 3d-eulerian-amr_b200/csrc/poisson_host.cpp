@@ -117,7 +117,7 @@ int relax(amr_ctx* c, int l, double* resid) {
     int bad;
     {
         ProfScope ps_(c->prof, KC_RELAX, c->stream, nlvl(c, l));
-        bad = launch_relax(c->geom, c->st, lvl(c, l), nlvl(c, l), c->d_pres, nullptr, c->stream);
+        bad = launch_relax(c->geom, c->st, lvl(c, l), nlvl(c, l), c->d_pres, c->stream);
     }
     if (bad) {
         c->err = "relaxation kernel built for nx == 8 only";
@@ -170,28 +170,19 @@ int vcycle0(amr_ctx* c) {
         ProfScope ps_(c->prof, KC_VDOWN, c->stream);
         launch_init_vcycle(c->geom, c->st, all(c), nall(c), c->stream);
     }
+    // The reference fills the dphi ghosts before vcycle_down and before the
+    // coarse correction as well; neither reads them and relax_until fills
+    // them again first, so those two fills are left out (same results).
     for (int l = maxlevel; l >= 0; l--) {
-        TRY(dphi_boundaries(c, l));
         {
-            ProfScope ps_(c->prof, KC_VDOWN, c->stream);
-            launch_vdown_a(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->stream);
-        }
-        for (int dir = 0; dir < 3; dir++) {
-            const int a = c->off_reflux_dir[3 * l + dir], b = c->off_reflux_dir[3 * l + dir + 1];
-            {
-                ProfScope ps_(c->prof, KC_VDOWN, c->stream);
-                launch_adjust_dphi(c->geom, c->bt, c->st, c->d_reflux + a, b - a, c->stream);
-            }
-        }
-        {
-            ProfScope ps_(c->prof, KC_VDOWN, c->stream);
-            launch_vdown_c(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->stream);
+            ProfScope ps_(c->prof, KC_VDOWN, c->stream, nlvl(c, l));
+            launch_vdown(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->d_vitems,
+                         c->d_vranges + 4 * c->off_vrange[l], c->stream);
         }
         TRY(check_launch(c));
         TRY(relax_until(c, l, 1.0));
     }
     for (int l = 0; l <= maxlevel; l++) {
-        TRY(dphi_boundaries(c, l));
         if (l > 0) {
             ProfScope ps_(c->prof, KC_CORRECT, c->stream);
             launch_coarse_correction(c->geom, c->bt, c->st, lvl(c, l), nlvl(c, l), c->stream);

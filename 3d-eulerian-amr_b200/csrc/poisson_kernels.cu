@@ -4,6 +4,7 @@
 // Poisson arrays live on the PNX^3 frame of every brick (PNX = nx + 2: the
 // interior plus one ghost layer); Poisson index p <-> grid index p + BW - 1.
 #include "context.h"
+#include "corr.cuh"
 #include "euler_state.cuh"
 #include "poisson.h"
 #include "relax_brick.cuh"
@@ -47,12 +48,13 @@ __device__ __forceinline__ double divergence(const double* a, int pnx, int i, in
 }
 
 // Array3d::oct_avg (array3d.h:151-161)
-__device__ __forceinline__ double oct_avg(const double* a, int pnx, int i, int j, int k) {
+template <typename T>
+__device__ __forceinline__ T oct_avg(const T* a, int pnx, int i, int j, int k) {
     const int c = pidx(pnx, i, j, k);
     const int s = pnx * pnx;
     return (a[c] + a[c + 1] + a[c + pnx] + a[c + pnx + 1] + a[c + s] + a[c + s + 1] + a[c + s + pnx] +
             a[c + s + pnx + 1]) *
-           0.125;
+           T(0.125);
 }
 
 // ---------------------------------------------------------------------------
@@ -304,19 +306,21 @@ __device__ double get_phi_from(const Geom& g, const BrickTable& bt, const DevSta
 
 // get_dphi: neighbour copy; PoissonAMRBound::get_dphi (poisson_amr_bound.cpp
 // :111-116) parent value without interpolation; 0 on a domain face; mirror.
-__device__ double get_dphi_from(const Geom& g, const BrickTable& bt, const DevState& st, const PoissonAux& aux, int b,
-                                int face, int i, int j, int k) {
+template <typename CT>
+__device__ CT get_dphi_from(const Geom& g, const BrickTable& bt, const DevState& st, const PoissonAux& aux, int b,
+                            int face, int i, int j, int k) {
     const int pnx = g.pnx;
     const int kind = bt.ftype[6 * b + face];
     const int nbr = bt.fnbr[6 * b + face];
-    if (kind == FACE_SIB) return st.dphi[(size_t)nbr * g.pnx3 + pidx(pnx, i, j, k)];
-    if (kind == FACE_OUTFLOW) return 0.0;
+    const CT* D = Corr<CT>::dphi(st);
+    if (kind == FACE_SIB) return D[(size_t)nbr * g.pnx3 + pidx(pnx, i, j, k)];
+    if (kind == FACE_OUTFLOW) return CT(0);
     if (kind == FACE_REFLECT) {
-        const double* d = st.dphi + (size_t)b * g.pnx3;
+        const CT* d = D + (size_t)b * g.pnx3;
         if (k == 1) return d[pidx(pnx, i, j, pnx - 2)];
         if (k == pnx - 2) return d[pidx(pnx, i, j, 1)];
         atomicExch(aux.err, 1);
-        return 0.0;
+        return CT(0);
     }
     const int ax = face >> 1;
     const int v = (face & 1) ? 1 : -1;
@@ -326,7 +330,7 @@ __device__ double get_dphi_from(const Geom& g, const BrickTable& bt, const DevSt
         const int rel = bt.off[3 * b + d] + (d == ax ? v * (pnx - 2) : 0) - 2 * bt.off[3 * nbr + d] - (g.bw - 1);
         r[d] = (rel + q[d]) / 2;
     }
-    return st.dphi[(size_t)nbr * g.pnx3 + pidx(pnx, r[0], r[1], r[2])];
+    return D[(size_t)nbr * g.pnx3 + pidx(pnx, r[0], r[1], r[2])];
 }
 
 // ---------------------------------------------------------------------------
@@ -335,8 +339,7 @@ __device__ double get_dphi_from(const Geom& g, const BrickTable& bt, const DevSt
 // ---------------------------------------------------------------------------
 // faces: phi(0,j,k) = sib(XL).get_phi(PNX-2,j,k), phi(PNX-1,j,k) =
 // sib(XU).get_phi(1,j,k), ... over the transverse interior.
-__global__ void k_phi_faces(Geom g, BrickTable bt, DevState st, PoissonAux aux, const int* __restrict__ slots,
-                            int dphi_mode) {
+__global__ void k_phi_faces(Geom g, BrickTable bt, DevState st, PoissonAux aux, const int* __restrict__ slots) {
     const int b = slots[blockIdx.x];
     const int face = blockIdx.y;
     const int pnx = g.pnx, m = pnx - 2;
@@ -348,13 +351,28 @@ __global__ void k_phi_faces(Geom g, BrickTable bt, DevState st, PoissonAux aux, 
         src[ax] = (face & 1) ? 1 : pnx - 2;
         dst[ax == 0 ? 1 : 0] = src[ax == 0 ? 1 : 0] = t1;
         dst[ax == 2 ? 1 : 2] = src[ax == 2 ? 1 : 2] = t2;
-        if (dphi_mode) {
-            const double v = get_dphi_from(g, bt, st, aux, b, face, src[0], src[1], src[2]);
-            st.dphi[(size_t)b * g.pnx3 + pidx(pnx, dst[0], dst[1], dst[2])] = v;
-        } else {
-            const double v = get_phi_from(g, bt, st, aux, b, face, src[0], src[1], src[2]);
-            st.phi[(size_t)b * g.pnx3 + pidx(pnx, dst[0], dst[1], dst[2])] = v;
-        }
+        const double v = get_phi_from(g, bt, st, aux, b, face, src[0], src[1], src[2]);
+        st.phi[(size_t)b * g.pnx3 + pidx(pnx, dst[0], dst[1], dst[2])] = v;
+    }
+}
+
+// the same face fill for the correction (enforce_dphi_boundaries)
+template <typename CT>
+__global__ void k_dphi_faces(Geom g, BrickTable bt, DevState st, PoissonAux aux, const int* __restrict__ slots) {
+    const int b = slots[blockIdx.x];
+    const int face = blockIdx.y;
+    const int pnx = g.pnx, m = pnx - 2;
+    const int ax = face >> 1;
+    CT* D = Corr<CT>::dphi(st);
+    for (int t = threadIdx.x; t < m * m; t += blockDim.x) {
+        const int t1 = t % m + 1, t2 = t / m + 1;
+        int dst[3], src[3];
+        dst[ax] = (face & 1) ? pnx - 1 : 0;
+        src[ax] = (face & 1) ? 1 : pnx - 2;
+        dst[ax == 0 ? 1 : 0] = src[ax == 0 ? 1 : 0] = t1;
+        dst[ax == 2 ? 1 : 2] = src[ax == 2 ? 1 : 2] = t2;
+        const CT v = get_dphi_from<CT>(g, bt, st, aux, b, face, src[0], src[1], src[2]);
+        D[(size_t)b * g.pnx3 + pidx(pnx, dst[0], dst[1], dst[2])] = v;
     }
 }
 
@@ -478,89 +496,96 @@ __global__ void k_phi_from_children(Geom g, BrickTable bt, DevState st, const in
 }
 
 // Poisson::init_vcycle (poisson.cpp:931-948)
+template <typename CT>
 __global__ void k_init_vcycle(Geom g, DevState st, const int* __restrict__ slots) {
     const size_t base = (size_t)slots[blockIdx.x] * g.pnx3;
+    CT* D = Corr<CT>::dphi(st);
+    CT* D1 = Corr<CT>::dphi1(st);
     for (int t = threadIdx.x; t < g.pnx3; t += blockDim.x) {
-        st.dphi[base + t] = 0.0;
-        st.dphi1[base + t] = 0.0;
+        D[base + t] = CT(0);
+        D1[base + t] = CT(0);
     }
 }
 
-// Poisson::vcycle_down first part (poisson.cpp:989-1017): residual/6 on
-// uncovered cells, child averages of dphi and dphi1 on covered ones.
-__global__ void k_vdown_a(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
+// Poisson::vcycle_down (poisson.cpp:989-1046) for one brick per block:
+//  (a) residual/6 from phi and S on uncovered cells, child averages of dphi
+//      and dphi1 on covered ones (poisson.cpp:989-1017);
+//  (b) adjust_x_dphi, adjust_y_dphi, adjust_z_dphi (poisson.cpp:249-443):
+//      on uncovered cells next to a face refined on one side, the coarse
+//      minus the averaged fine potential difference /6 is added / subtracted;
+//      this brick's items, x then y then z (an item touches only cells of
+//      its coarse brick, so bricks are independent);
+//  (c) dphi1 = dphi on uncovered cells (poisson.cpp:1021-1040).
+// The residual and the corrections are formed in FP64 from phi; they are
+// stored in the correction type CT.  ranges[4 q .. 4 q + 3] = first x, y, z
+// item and end of the brick at list position q.
+template <typename CT>
+__global__ void k_vdown(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots,
+                        const RefluxItem* __restrict__ items, const int* __restrict__ ranges) {
     const int b = slots[blockIdx.x];
     const int pnx = g.pnx, nx = pnx - 2, half = nx / 2;
     const double h = bt.h[b];
     const double h2 = h * h;
     const size_t base = (size_t)b * g.pnx3;
+    CT* D = Corr<CT>::dphi(st);
+    CT* D1 = Corr<CT>::dphi1(st);
     for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
         const int i = t % nx + 1, j = (t / nx) % nx + 1, k = t / (nx * nx) + 1;
         const int oc = ((i - 1) / half) | (((j - 1) / half) << 1) | (((k - 1) / half) << 2);
         const int ch = bt.child[8 * b + oc];
         const int c = pidx(pnx, i, j, k);
         if (ch < 0) {
-            st.dphi[base + c] = (divergence(st.phi + base, pnx, i, j, k) - h2 * st.S[base + c]) * (1.0 / 6.0);
+            D[base + c] = CT((divergence(st.phi + base, pnx, i, j, k) - h2 * st.S[base + c]) * (1.0 / 6.0));
         } else {
             const int ci = 2 * (i - (oc & 1) * half) - 1;
             const int cj = 2 * (j - ((oc >> 1) & 1) * half) - 1;
             const int ck = 2 * (k - ((oc >> 2) & 1) * half) - 1;
             const size_t cb = (size_t)ch * g.pnx3;
-            st.dphi1[base + c] = oct_avg(st.dphi1 + cb, pnx, ci, cj, ck);
-            st.dphi[base + c] = oct_avg(st.dphi + cb, pnx, ci, cj, ck);
+            D1[base + c] = oct_avg(D1 + cb, pnx, ci, cj, ck);
+            D[base + c] = oct_avg(D + cb, pnx, ci, cj, ck);
         }
     }
-}
-
-// Poisson::adjust_{x,y,z}_dphi (poisson.cpp:249-443): coarse-fine
-// correction of dphi on uncovered cells next to a face refined on one side.
-// The items are the coarse-fine flux items of the hydro in the PNX frame.
-__global__ void k_adjust_dphi(Geom g, BrickTable bt, DevState st, const RefluxItem* __restrict__ items) {
-    const RefluxItem it = items[blockIdx.x];
-    const int pnx = g.pnx, half = (pnx - 2) / 2;
-    const int t = threadIdx.x;
-    if (t >= half * half) return;
-    const int a = t % half, cc = t / half;
-    const int j = 2 * a + 1, k = 2 * cc + 1;                          // child transverse (lower, higher)
-    const int j0 = a + 1 + it.cj * half, k0 = cc + 1 + it.ck * half;  // coarse transverse
-    const int i = it.ic - g.bw + 1, i0 = it.i0 - g.bw + 1;            // PNX frame
-    const int d = it.dir;
-    auto at = [&](int nrm, int t1, int t2) {
-        int q[3];
-        q[d] = nrm;
-        q[d == 0 ? 1 : 0] = t1;
-        q[d == 2 ? 1 : 2] = t2;
-        return pidx(pnx, q[0], q[1], q[2]);
-    };
-    const double* C = st.phi + (size_t)it.child * g.pnx3;
-    const size_t pb = (size_t)it.coarse * g.pnx3;
-    const double* P = st.phi + pb;
-    double v = +C[at(i, j, k)] - C[at(i - 1, j, k)];
-    v += C[at(i, j + 1, k)] - C[at(i - 1, j + 1, k)];
-    v += C[at(i, j, k + 1)] - C[at(i - 1, j, k + 1)];
-    v += C[at(i, j + 1, k + 1)] - C[at(i - 1, j + 1, k + 1)];
-    v *= 0.5;
-    const double dd = (P[at(i0, j0, k0)] - P[at(i0 - 1, j0, k0)] - v) * (1.0 / 6.0);
+    const int* rg = ranges + 4 * blockIdx.x;
+    const int hh = half * half;
     auto refined = [&](int cell) {
         const int ci = cell % pnx, cj = (cell / pnx) % pnx, ck = cell / (pnx * pnx);
         const int oc = (2 * ci / pnx) | ((2 * cj / pnx) << 1) | ((2 * ck / pnx) << 2);
-        return bt.child[8 * it.coarse + oc] >= 0;
+        return bt.child[8 * b + oc] >= 0;
     };
-    const int c1 = at(i0, j0, k0), c0 = at(i0 - 1, j0, k0);
-    if (!refined(c1)) st.dphi[pb + c1] += dd;
-    if (!refined(c0)) st.dphi[pb + c0] -= dd;
-}
-
-// Poisson::vcycle_down last part (poisson.cpp:1021-1040): dphi1 = dphi on
-// uncovered cells.
-__global__ void k_vdown_c(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
-    const int b = slots[blockIdx.x];
-    const int pnx = g.pnx, nx = pnx - 2, half = nx / 2;
-    const size_t base = (size_t)b * g.pnx3;
+    for (int d = 0; d < 3; d++) {
+        __syncthreads();
+        const int i_beg = rg[d], i_end = rg[d + 1];
+        for (int q = threadIdx.x; q < (i_end - i_beg) * hh; q += blockDim.x) {
+            const RefluxItem it = items[i_beg + q / hh];
+            const int a = (q % hh) % half, cc = (q % hh) / half;
+            const int j = 2 * a + 1, k = 2 * cc + 1;                          // child transverse
+            const int j0 = a + 1 + it.cj * half, k0 = cc + 1 + it.ck * half;  // coarse transverse
+            const int i = it.ic - g.bw + 1, i0 = it.i0 - g.bw + 1;            // PNX frame
+            auto at = [&](int nrm, int t1, int t2) {
+                int qq[3];
+                qq[d] = nrm;
+                qq[d == 0 ? 1 : 0] = t1;
+                qq[d == 2 ? 1 : 2] = t2;
+                return pidx(pnx, qq[0], qq[1], qq[2]);
+            };
+            const double* C = st.phi + (size_t)it.child * g.pnx3;
+            const double* P = st.phi + base;
+            double v = +C[at(i, j, k)] - C[at(i - 1, j, k)];
+            v += C[at(i, j + 1, k)] - C[at(i - 1, j + 1, k)];
+            v += C[at(i, j, k + 1)] - C[at(i - 1, j, k + 1)];
+            v += C[at(i, j + 1, k + 1)] - C[at(i - 1, j + 1, k + 1)];
+            v *= 0.5;
+            const double dd = (P[at(i0, j0, k0)] - P[at(i0 - 1, j0, k0)] - v) * (1.0 / 6.0);
+            const int c1 = at(i0, j0, k0), c0 = at(i0 - 1, j0, k0);
+            if (!refined(c1)) D[base + c1] = CT(double(D[base + c1]) + dd);
+            if (!refined(c0)) D[base + c0] = CT(double(D[base + c0]) - dd);
+        }
+    }
+    __syncthreads();
     for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
         const int i = t % nx + 1, j = (t / nx) % nx + 1, k = t / (nx * nx) + 1;
         const int oc = ((i - 1) / half) | (((j - 1) / half) << 1) | (((k - 1) / half) << 2);
-        if (bt.child[8 * b + oc] < 0) st.dphi1[base + pidx(pnx, i, j, k)] = st.dphi[base + pidx(pnx, i, j, k)];
+        if (bt.child[8 * b + oc] < 0) D1[base + pidx(pnx, i, j, k)] = D[base + pidx(pnx, i, j, k)];
     }
 }
 
@@ -568,24 +593,25 @@ __global__ void k_vdown_c(Geom g, BrickTable bt, DevState st, const int* __restr
 // with its ghost dphi frozen, until the sweep's sum of squared updates drops
 // below half the first sweep's or 16 sweeps.  Block = one brick, thread per
 // interior cell, dphi staged in shared memory.  out[e] = last sweep's sum.
-template <int NX>
+template <int NX, typename CT>
 __global__ void __launch_bounds__(NX* NX* NX) k_relax(Geom g, DevState st, const int* __restrict__ slots,
-                                                      double* __restrict__ out, int* __restrict__ sweeps_out) {
+                                                      double* __restrict__ out) {
     constexpr int P = NX + 2, P3 = P * P * P;
-    __shared__ RelaxSmem<NX> sm;
+    __shared__ RelaxSmem<NX, CT> sm;
     const int b = slots[blockIdx.x];
     const size_t base = (size_t)b * P3;
     const int t = threadIdx.x;
     const int c = ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
-    double v;
-    const double resid = relax_brick<NX>(sm, st.dphi + base, st.dphi1 + base, &v);
-    st.dphi[base + c] = v;
+    CT* D = Corr<CT>::dphi(st);
+    CT v;
+    const double resid = relax_brick<NX, CT>(sm, D + base, Corr<CT>::dphi1(st) + base, &v);
+    D[base + c] = v;
     if (t == 0) out[b] = resid;
-    (void)sweeps_out;
 }
 
 // Poisson::vcycle_coarse_correction (poisson.cpp:17-51): child dphi +=
 // parent dphi - mean of the child's 2x2x2 group.
+template <typename CT>
 __global__ void k_coarse_correction(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
     const int b = slots[blockIdx.x];
     const int p = bt.parent[b];
@@ -597,19 +623,21 @@ __global__ void k_coarse_correction(Geom g, BrickTable bt, DevState st, const in
     const int a = t % half, bb = (t / half) % half, cc = t / (half * half);
     const int i = 2 * a + 1, j = 2 * bb + 1, k = 2 * cc + 1;
     const int i0 = a + 1 + (c & 1) * half, j0 = bb + 1 + ((c >> 1) & 1) * half, k0 = cc + 1 + ((c >> 2) & 1) * half;
-    double* D = st.dphi + (size_t)b * g.pnx3;
-    const double av = st.dphi[(size_t)p * g.pnx3 + pidx(pnx, i0, j0, k0)] - oct_avg(D, pnx, i, j, k);
+    CT* D = Corr<CT>::dphi(st) + (size_t)b * g.pnx3;
+    const CT av = Corr<CT>::dphi(st)[(size_t)p * g.pnx3 + pidx(pnx, i0, j0, k0)] - oct_avg(D, pnx, i, j, k);
     for (int o = 0; o < 8; o++) D[pidx(pnx, i + (o & 1), j + ((o >> 1) & 1), k + ((o >> 2) & 1))] += av;
 }
 
-// Poisson::vcycle_retire_dphi (poisson.cpp:1048-1067): phi += dphi.
+// Poisson::vcycle_retire_dphi (poisson.cpp:1048-1067): phi += dphi, in FP64.
+template <typename CT>
 __global__ void k_retire(Geom g, DevState st, const int* __restrict__ slots) {
     const int b = slots[blockIdx.x];
     const int pnx = g.pnx, nx = pnx - 2;
     const size_t base = (size_t)b * g.pnx3;
+    const CT* D = Corr<CT>::dphi(st);
     for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
         const int c = pidx(pnx, t % nx + 1, (t / nx) % nx + 1, t / (nx * nx) + 1);
-        st.phi[base + c] += st.dphi[base + c];
+        st.phi[base + c] += double(D[base + c]);
     }
 }
 
@@ -660,8 +688,10 @@ __global__ void k_adjust_force(Geom g, DevState st, const RefluxItem* __restrict
 
 // Poisson::solution_error (poisson.cpp:637-669): dphi := div f - S on
 // uncovered cells (0 on covered), per-brick sum of |dphi| h^3.
+template <typename CT>
 __global__ void k_solution_error(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots,
                                  double* __restrict__ out) {
+    CT* D = Corr<CT>::dphi(st);
     const int b = slots[blockIdx.x];
     const int pnx = g.pnx, nx = pnx - 2, half = nx / 2;
     const double h = bt.h[b];
@@ -678,10 +708,10 @@ __global__ void k_solution_error(Geom g, BrickTable bt, DevState st, const int* 
             df -= (st.fy[base + c + pnx] - st.fy[base + c]) * hinv;
             df -= (st.fz[base + c + pnx * pnx] - st.fz[base + c]) * hinv;
             const double r = df - st.S[base + c];
-            st.dphi[base + c] = r;
+            D[base + c] = CT(r);
             sum += fabs(r) * h3;
         } else {
-            st.dphi[base + c] = 0.0;
+            D[base + c] = CT(0);
         }
     }
     for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
@@ -729,6 +759,10 @@ __global__ void k_poisson_new(Geom g, BrickTable bt, DevState st, const int* __r
         st.fx[base + t] = 0.0;
         st.fy[base + t] = 0.0;
         st.fz[base + t] = 0.0;
+        if (st.fdphi) {
+            st.fdphi[base + t] = 0.0f;
+            st.fdphi1[base + t] = 0.0f;
+        }
     }
     __syncthreads();
     const int p = bt.parent[b];
@@ -789,7 +823,7 @@ void launch_phi_boundaries(const Geom& g, const BrickTable& bt, const DevState& 
                            const int* slots, int n, cudaStream_t s) {
     if (n <= 0) return;
     PoissonAux aux{bphi, err};
-    launch_k(k_phi_faces, dim3(n, 6), 64, 0, s, g, bt, st, aux, slots, 0);
+    launch_k(k_phi_faces, dim3(n, 6), 64, 0, s, g, bt, st, aux, slots);
     launch_k(k_phi_edges, n, g.pnx - 2, 0, s, g, bt, st, aux, slots);
     launch_k(k_phi_vertices, n, 32, 0, s, g, bt, st, aux, slots);
 }
@@ -797,7 +831,10 @@ void launch_dphi_boundaries(const Geom& g, const BrickTable& bt, const DevState&
                             const int* slots, int n, cudaStream_t s) {
     if (n <= 0) return;
     PoissonAux aux{bphi, err};
-    launch_k(k_phi_faces, dim3(n, 6), 64, 0, s, g, bt, st, aux, slots, 1);
+    if (g.precision == AMR_PREC_MIXED)
+        launch_k(k_dphi_faces<float>, dim3(n, 6), 64, 0, s, g, bt, st, aux, slots);
+    else
+        launch_k(k_dphi_faces<double>, dim3(n, 6), 64, 0, s, g, bt, st, aux, slots);
 }
 void launch_phi_from_children(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                               cudaStream_t s) {
@@ -805,34 +842,45 @@ void launch_phi_from_children(const Geom& g, const BrickTable& bt, const DevStat
     if (n > 0) launch_k(k_phi_from_children, dim3(n, 8), ((half * half * half + 31) / 32) * 32, 0, s, g, bt, st, slots);
 }
 void launch_init_vcycle(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
-    if (n > 0) launch_k(k_init_vcycle, n, 256, 0, s, g, st, slots);
+    if (n <= 0) return;
+    if (g.precision == AMR_PREC_MIXED)
+        launch_k(k_init_vcycle<float>, n, 256, 0, s, g, st, slots);
+    else
+        launch_k(k_init_vcycle<double>, n, 256, 0, s, g, st, slots);
 }
-void launch_vdown_a(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
-                    cudaStream_t s) {
-    if (n > 0) launch_k(k_vdown_a, n, 256, 0, s, g, bt, st, slots);
+void launch_vdown(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
+                  const RefluxItem* items, const int* ranges, cudaStream_t s) {
+    if (n <= 0) return;
+    if (g.precision == AMR_PREC_MIXED)
+        launch_k(k_vdown<float>, n, 256, 0, s, g, bt, st, slots, items, ranges);
+    else
+        launch_k(k_vdown<double>, n, 256, 0, s, g, bt, st, slots, items, ranges);
 }
-void launch_adjust_dphi(const Geom& g, const BrickTable& bt, const DevState& st, const RefluxItem* items, int n,
-                        cudaStream_t s) {
-    if (n > 0) launch_k(k_adjust_dphi, n, 32, 0, s, g, bt, st, items);
-}
-void launch_vdown_c(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
-                    cudaStream_t s) {
-    if (n > 0) launch_k(k_vdown_c, n, 256, 0, s, g, bt, st, slots);
-}
-int launch_relax(const Geom& g, const DevState& st, const int* slots, int n, double* out, int* sweeps,
-                 cudaStream_t s) {
+int launch_relax(const Geom& g, const DevState& st, const int* slots, int n, double* out, cudaStream_t s) {
     if (n <= 0) return 0;
     if (g.nx != 8) return -1;
-    launch_k(k_relax<8>, n, 512, 0, s, g, st, slots, out, sweeps);
+    if (g.precision == AMR_PREC_MIXED)
+        launch_k(k_relax<8, float>, n, 512, 0, s, g, st, slots, out);
+    else
+        launch_k(k_relax<8, double>, n, 512, 0, s, g, st, slots, out);
     return 0;
 }
 void launch_coarse_correction(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                               cudaStream_t s) {
     const int half = (g.pnx - 2) / 2;
-    if (n > 0) launch_k(k_coarse_correction, n, ((half * half * half + 31) / 32) * 32, 0, s, g, bt, st, slots);
+    if (n <= 0) return;
+    const int nt = ((half * half * half + 31) / 32) * 32;
+    if (g.precision == AMR_PREC_MIXED)
+        launch_k(k_coarse_correction<float>, n, nt, 0, s, g, bt, st, slots);
+    else
+        launch_k(k_coarse_correction<double>, n, nt, 0, s, g, bt, st, slots);
 }
 void launch_retire(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
-    if (n > 0) launch_k(k_retire, n, 256, 0, s, g, st, slots);
+    if (n <= 0) return;
+    if (g.precision == AMR_PREC_MIXED)
+        launch_k(k_retire<float>, n, 256, 0, s, g, st, slots);
+    else
+        launch_k(k_retire<double>, n, 256, 0, s, g, st, slots);
 }
 void launch_forces(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                    cudaStream_t s) {
@@ -843,7 +891,11 @@ void launch_adjust_force(const Geom& g, const DevState& st, const RefluxItem* it
 }
 void launch_solution_error(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                            double* out, cudaStream_t s) {
-    if (n > 0) launch_k(k_solution_error, n, 256, 0, s, g, bt, st, slots, out);
+    if (n <= 0) return;
+    if (g.precision == AMR_PREC_MIXED)
+        launch_k(k_solution_error<float>, n, 256, 0, s, g, bt, st, slots, out);
+    else
+        launch_k(k_solution_error<double>, n, 256, 0, s, g, bt, st, slots, out);
 }
 void launch_phi_time(const Geom& g, const DevState& st, const int* slots, int n, int mode, cudaStream_t s) {
     if (n > 0) launch_k(k_phi_time, n, 256, 0, s, g, st, slots, mode);

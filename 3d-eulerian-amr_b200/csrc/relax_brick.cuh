@@ -12,37 +12,40 @@
 
 namespace amr {
 
-template <int NX>
+template <int NX, typename CT = double>
 struct RelaxSmem {
     static constexpr int P = NX + 2, P3 = P * P * P, NT = NX * NX * NX, NW = NT / 32;
-    double buf[2][P3];
+    CT buf[2][P3];
     double red[2][NW];
 };
 
 // Stages the brick (slot base) into both buffers; returns the last sweep's
 // sum and leaves the relaxed interior value of this thread's cell in *out.
-template <int NX>
-__device__ __forceinline__ double relax_brick(RelaxSmem<NX>& sm, const double* __restrict__ dphi,
-                                              const double* __restrict__ dphi1, double* out) {
-    constexpr int P = RelaxSmem<NX>::P, P3 = RelaxSmem<NX>::P3, NT = RelaxSmem<NX>::NT, NW = RelaxSmem<NX>::NW;
+// CT is the correction's storage and arithmetic type (FP64, or FP32 in the
+// mixed form); the sums of squares are formed in FP64 either way.
+template <int NX, typename CT = double>
+__device__ __forceinline__ double relax_brick(RelaxSmem<NX, CT>& sm, const CT* __restrict__ dphi,
+                                              const CT* __restrict__ dphi1, CT* out) {
+    constexpr int P = RelaxSmem<NX, CT>::P, P3 = RelaxSmem<NX, CT>::P3, NT = RelaxSmem<NX, CT>::NT,
+                  NW = RelaxSmem<NX, CT>::NW;
     const int t = threadIdx.x;
     for (int q = t; q < P3; q += NT) {
-        const double v = dphi[q];
+        const CT v = dphi[q];
         sm.buf[0][q] = v;
         sm.buf[1][q] = v;
     }
     const int i = t % NX + 1, j = (t / NX) % NX + 1, k = t / (NX * NX) + 1;
     const int c = (k * P + j) * P + i;
-    const double d1 = dphi1[c];
+    const CT d1 = dphi1[c];
     __syncthreads();
     double resid0 = 0.0, resid = 0.0;
     int iters = 0, cur = 0;
     do {
-        const double* d = sm.buf[cur];
-        const double div = (d[c + 1] + d[c - 1] + d[c + P] + d[c - P] + d[c + P * P] + d[c - P * P]) - (d[c] * 6.0);
-        const double tmp0 = d1 + div * (1.0 / 6.0);
+        const CT* d = sm.buf[cur];
+        const CT div = (d[c + 1] + d[c - 1] + d[c + P] + d[c - P] + d[c + P * P] + d[c - P * P]) - (d[c] * CT(6.0));
+        const CT tmp0 = d1 + div * (CT(1.0) / CT(6.0));
         sm.buf[cur ^ 1][c] = d[c] + tmp0;
-        double sq = tmp0 * tmp0;
+        double sq = double(tmp0) * double(tmp0);
         for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
         if ((t & 31) == 0) sm.red[cur][t >> 5] = sq;
         __syncthreads();

@@ -27,6 +27,8 @@ import tempfile
 import threading
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "3d-eulerian-amr_b200")
 
@@ -179,9 +181,13 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
     form: "fp64"  plain FP64, host-orchestrated (reference operation order)
           "graph" FP64, whole RK3 step replayed from a captured CUDA graph with
                   every loop decided on the device (bitwise equal to fp64)
+          "mixed" the graph form with the multigrid correction (smoothing,
+                  restriction, prolongation of dphi) and the KT flux in FP32;
+                  residual, potential and conserved update in FP64
     """
+    prec = amr.PREC_MIXED if form == "mixed" else amr.PREC_FP64
     a = amr.AMR(physics=amr.PHYSICS_EULER_GRAVITY, max_refine_level=LEVELS, grid_dim=0.5, z_reflect=0,
-                max_bricks=8192, precision=amr.PREC_FP64)
+                max_bricks=8192, precision=prec)
     ini.build_tree(a, "polytrope", 1.0e-6, 0.5, 0, LEVELS, device=True)
     stream = torch.cuda.ExternalStream(a.stream_handle())
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -231,6 +237,9 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
     res["clocks"] = sampler.stop()
     st1 = a.stats()
     res["gpu_launches"] = a.launch_count() - k0
+    # state after warm-up + timed steps, for the error of one form against another
+    res["final"] = {"U": a.download_state(), "phi": a.download_poisson()[0], "level": a.get_tree()["level"],
+                    "loc": a.get_tree()["loc"]}
     t = torch.tensor([sum(times), float(cells)], dtype=torch.float64, device="cuda")
     if world > 1:
         dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
@@ -291,6 +300,173 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
     return res
 
 
+EOS_POINTS = 1 << 24
+EOS_FLOPS_PER_POINT = 1000  # FP64 adds/muls of one helm_point call, counted in helm_kernels.cu
+EOS_IO_BYTES = 56  # rho, T, abar, zbar in; p, e, cs out (FP64)
+FP64_NOMINAL_TFLOPS = 37.0  # B200 FP64 (non-tensor), vendor figure: no measured FP64 peak exists here
+
+
+def _load_module(name, path):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def run_eos(torch, steps, warmup, cpu_sample):
+    """Helmholtz EOS throughput: 2^24 points, forward (rho,T)->(p,e,cs) and
+    inverse (rho,e)->T by Newton, each one launch over device arrays."""
+    helm_table = _load_module("helm_table", os.path.join(PKG, "helm_table.py"))
+    helm_mod = _load_module("helm_b200", os.path.join(PKG, "helm.py"))
+    tdir = tempfile.mkdtemp(prefix="helm_table_")
+    table = helm_table.ensure_table(tdir)
+    h = helm_mod.Helm(table)
+    n = EOS_POINTS
+    g = torch.Generator(device="cpu").manual_seed(20261203)
+    u = lambda lo, hi: lo + (hi - lo) * torch.rand(n, dtype=torch.float64, generator=g)
+    rho_h = torch.pow(10.0, u(-2.0, 9.0))
+    T_h = torch.pow(10.0, u(4.0, 9.0))
+    abar_h = u(12.0, 16.0)
+    guess_h = T_h * torch.pow(10.0, u(-0.5, 0.5))
+    dev = lambda t: t.cuda()
+    rho, T, abar, guess = dev(rho_h), dev(T_h), dev(abar_h), dev(guess_h)
+    zbar = abar / 2
+    p, e, cs = (torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(3))
+    status = torch.empty(n, dtype=torch.int32, device="cuda")
+    Tout = torch.empty_like(T)
+    iters = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def fwd():
+        h.eos_device(rho, T, abar, zbar, p, e, cs, status, stream=stream)
+
+    def inv():
+        Tout.copy_(guess)
+        h.invert_T_device(rho, e_target, abar, zbar, Tout, status_i, iters=iters, stream=stream)
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        ts = []
+        for _ in range(steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn()
+            b.record()
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    ms_f = timed(fwd)
+    bad_f = int((status != 0).sum())
+    e_target = e.clone()
+    status_i = torch.empty_like(status)
+    # the Newton launch starts from the guess each time (the copy is timed with it)
+    ms_i = timed(inv)
+    bad_i = int((status_i != 0).sum())
+    it = iters.double()
+    # accuracy against the oracle restatement on a sample
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import helm_oracle
+    tab = helm_oracle.Table(table)
+    idx = torch.arange(0, n, n // 4096)
+    w = helm_oracle.eos(tab, rho_h[idx].numpy(), T_h[idx].numpy(), abar_h[idx].numpy(), abar_h[idx].numpy() / 2)
+    err = {}
+    for k, t in (("p", p), ("e", e), ("cs", cs)):
+        got = t[idx.cuda()].cpu().numpy()
+        err[k] = float((abs(got - w[k]) / abs(w[k])).max())
+    Trel = float(((Tout - T).abs() / T).max())
+    flops = EOS_FLOPS_PER_POINT * n / (ms_f * 1e-3) / 1e12
+    res = {
+        "points": n, "forward_ms": ms_f, "forward_points_per_s": n / (ms_f * 1e-3),
+        "inverse_ms": ms_i, "inverse_points_per_s": n / (ms_i * 1e-3),
+        "newton_iters_mean": float(it.mean()), "newton_iters_max": int(it.max()),
+        "bad_status_forward": bad_f, "bad_status_inverse": bad_i,
+        "forward_max_rel_err_vs_oracle": err, "inverse_max_rel_err_T_vs_true": Trel,
+        "forward_fp64_tflops": flops, "fp64_peak_tflops": FP64_NOMINAL_TFLOPS, "fp64_peak_source": "nominal",
+        "forward_fp64_frac": flops / FP64_NOMINAL_TFLOPS,
+        "forward_io_gbs": EOS_IO_BYTES * n / (ms_f * 1e-3) / 1e9,
+        "table": "synthetic closed-form free energy in the reference's table format (the real table is not shipped)",
+    }
+    if cpu_sample:
+        exe = os.path.join(ROOT, "oracle", "_ref", "helm_harness")
+        if os.path.exists(exe):
+            import numpy as np
+            m = 1 << 18
+            with open(os.path.join(tdir, "in.bin"), "wb") as fh:
+                np.array([m], np.int64).tofile(fh)
+                np.stack([rho_h[:m].numpy(), T_h[:m].numpy(), abar_h[:m].numpy(), abar_h[:m].numpy() / 2],
+                         1).tofile(fh)
+            with open(os.path.join(tdir, "one.bin"), "wb") as fh:
+                np.array([1], np.int64).tofile(fh)
+                np.array([1e6, 1e6, 12.0, 6.0]).tofile(fh)
+            t0 = time.time()
+            subprocess.run([exe, "fwd", "in.bin", "out.bin"], cwd=tdir, check=True)
+            t1 = time.time()
+            subprocess.run([exe, "fwd", "one.bin", "out1.bin"], cwd=tdir, check=True)
+            t2 = time.time()
+            sec = max((t1 - t0) - (t2 - t1), 1e-9)  # minus process start + table read
+            res["cpu_baseline"] = {"value": m / sec, "unit": "EOS points/s", "cores": 1, "kind": "reference",
+                                   "sample": "reference helmholtz_eos (oracle/_ref/helm_harness, scalar) on the "
+                                             "first 2^18 points of the same workload"}
+    h.close()
+    import shutil
+    shutil.rmtree(tdir, ignore_errors=True)
+    return res
+
+
+def leaf_mask(t, nx):
+    """[bricks, nx, nx, nx] True where the interior cell is not covered by a child."""
+    n = t["level"].size
+    half = nx // 2
+    idx = np.arange(nx) // half
+    oc = idx[None, None, :] | (idx[None, :, None] << 1) | (idx[:, None, None] << 2)  # [k][j][i]
+    return ((t["child_mask"][:, None, None, None] >> oc[None]) & 1) == 0
+
+
+def state_errors(fin, ref, bw):
+    """Relative L2 of phi and relative L1 of density and energy over all bricks."""
+    if not (np.array_equal(fin["level"], ref["level"]) and np.array_equal(fin["loc"], ref["loc"])):
+        return {"comparable": False, "why": "the forms regridded to different trees"}
+    sl = (slice(None), slice(bw, -bw), slice(bw, -bw), slice(bw, -bw))
+    r0, r1 = fin["U"][:, 0][sl], ref["U"][:, 0][sl]
+    e0, e1 = fin["U"][:, 4][sl], ref["U"][:, 4][sl]
+    p0, p1 = fin["phi"][:, 1:-1, 1:-1, 1:-1], ref["phi"][:, 1:-1, 1:-1, 1:-1]
+    return {"comparable": True,
+            "phi_rel_l2": float(np.linalg.norm(p0 - p1) / np.linalg.norm(p1)),
+            "rho_rel_l1": float(np.abs(r0 - r1).sum() / np.abs(r1).sum()),
+            "energy_rel_l1": float(np.abs(e0 - e1).sum() / np.abs(e1).sum())}
+
+
+def poisson_precision_check(amr, ini, rel_tol=1e-10):
+    """Poisson solve of the initial star to L1 residual rel_tol x L1(4 pi G rho)
+    in the FP64 graph form and the mixed form; potential error of the mixed
+    form against FP64."""
+    out = {}
+    phis = {}
+    for name, prec in (("fp64", amr.PREC_FP64), ("mixed", amr.PREC_MIXED)):
+        a = amr.AMR(physics=amr.PHYSICS_EULER_GRAVITY, max_refine_level=LEVELS, grid_dim=0.5, z_reflect=0,
+                    max_bricks=8192, precision=prec)
+        t, U = ini.build_tree(a, "polytrope", 1.0e-6, 0.5, 0, LEVELS, device=True)
+        bw, nx = a.bw, a.nx
+        tt = a.get_tree()
+        rho = U[:, 0, bw:-bw, bw:-bw, bw:-bw]
+        l1_src = float((4.0 * np.pi * a.cfg.grav_g * np.abs(rho) * leaf_mask(tt, nx)).sum(axis=(1, 2, 3))
+                       @ (tt["h"] ** 3))
+        tol = rel_tol * l1_src
+        t0 = time.time()
+        err, cycles = a.graph_solve(tol, 100000)
+        a.synchronize()
+        out[name] = {"l1_residual": err, "tol": tol, "vcycles": cycles, "seconds": time.time() - t0}
+        phis[name] = a.download_poisson()[0][:, 1:-1, 1:-1, 1:-1]
+        a.close()
+    p64, p32 = phis["fp64"], phis["mixed"]
+    out["phi_rel_l2_mixed_vs_fp64"] = float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64))
+    out["relative_residual"] = rel_tol
+    return out
+
+
 def roofline_of(prof):
     known = {k: v for k, v in prof.items() if k in BYTES_PER_BRICK and v["launches"] > 0}
     dom = max(prof.items(), key=lambda kv: kv[1]["ms"])[0]
@@ -319,10 +495,11 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="graph", choices=["fp64", "graph"])
+    ap.add_argument("--form", default="mixed", choices=["fp64", "graph", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--json-out", default=None)
+    ap.add_argument("--no-eos", action="store_true", help="skip the Helmholtz EOS throughput section")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -340,9 +517,18 @@ def main():
                                 device_id=torch.device("cuda", local))
     amr, ini = load_amr()
     head = run_form(amr, ini, args.form, args, world, local, torch, dist, e2e=True, profile=True)
-    plain = None
+    plain = graph64 = None
+    errors = None
+    pcheck = None
     if not args.no_compare and args.form != "fp64":
         plain = run_form(amr, ini, "fp64", args, world, local, torch, dist)
+        if args.form == "mixed":
+            graph64 = run_form(amr, ini, "graph", args, world, local, torch, dist)
+            errors = state_errors(head["final"], plain["final"], 2)
+            errors["steps"] = args.warmup + args.steps
+            errors["against"] = "plain FP64 form (parity-tested against the reference CPU code)"
+            if rank == 0:
+                pcheck = poisson_precision_check(amr, ini)
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -353,11 +539,16 @@ def main():
                    "sample": "reference CPU code (oracle/_ref): one full RK3 step of this workload after one "
                              "untimed step (which solves from phi = 0), %d bricks, %d V-cycles" %
                              (s["bricks"], s["vcycles"][0])}
+    eos = None
+    if rank == 0 and not args.no_eos:
+        eos = run_eos(torch, max(args.steps, 3), max(args.warmup, 3), not args.no_cpu_baseline)
     if rank == 0:
         out = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.form != "mixed" else "f64+f32",
+            "data": "synthetic",
             "config": {"workload": WORKLOAD, "form": args.form, "levels": LEVELS, "bricks": head["bricks"],
                        "leaf_cells_per_step": head["cells"] / args.steps / world, "tol_l1": TOL,
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"},
@@ -366,6 +557,12 @@ def main():
             "relax_calls_per_step": head["relax_calls_per_step"],
             "fp64_plain": None if plain is None else {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
                                                        "gpu_launches": plain["gpu_launches"]},
+            "fp64_graph": None if graph64 is None else {"value": graph64["value"],
+                                                         "ms_per_step": graph64["ms_per_step"],
+                                                         "gpu_launches": graph64["gpu_launches"]},
+            "errors_vs_fp64": errors,
+            "poisson_precision": pcheck,
+            "helmholtz_eos": eos,
         }
         line = json.dumps(out)
         print(line)
