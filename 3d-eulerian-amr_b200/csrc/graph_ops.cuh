@@ -1,0 +1,115 @@
+// Device pieces shared by the graph-captured relaxation loop
+// (graph_kernels.cu) and the persistent solve (persistent.cu): the
+// reference's nested residual sums, the dphi ghost of a brick face taken from
+// the previous pass's snapshot, and one relaxation pass of a brick.
+#pragma once
+
+#include "corr.cuh"
+#include "graph.h"
+#include "relax_brick.cuh"
+
+namespace amr {
+
+// Bottom-up nested sums over levels [0, top).  Values of level `top` are in
+// `leaf` (per slot); S(node at m < top) = ((0 + S(c0)) + S(c1)) + ... in
+// child order (withown = false), or ((own + S(c0)) + ...) (withown = true:
+// own values in `leaf` for every level, `nest` preset to own at level top).  Result for the root is returned to
+// thread 0.  Called by one whole block.
+__device__ inline double nested_sum_block(const LevelLists& L, const int* __restrict__ child, const double* leaf,
+                                   double* nest, int top, bool withown) {
+    for (int m = top - 1; m >= 0; m--) {
+        const int* sl = L.slots + L.off[m];
+        for (int q = threadIdx.x; q < L.cnt[m]; q += blockDim.x) {
+            const int p = sl[q];
+            double s = withown ? __ldcg(leaf + p) : 0.0;
+            for (int c = 0; c < 8; c++) {
+                const int ch = child[8 * p + c];
+                if (ch < 0) continue;
+                s += (m + 1 == top && !withown) ? __ldcg(leaf + ch) : __ldcg(nest + ch);
+            }
+            nest[p] = s;
+        }
+        __threadfence_block();
+        __syncthreads();
+    }
+    return __ldcg(nest + L.slots[L.off[0]]);
+}
+
+// Ghost zones of a relaxation pass (Poisson::vcycle_relax,
+// poisson.cpp:88-130): in mode 0 they come from the brick's own dphi array (filled
+// just before by the face ghost kernel).  In mode 1 the block fills them
+// itself -- what Poisson::enforce_dphi_boundaries (poisson.cpp:890-929) would
+// copy: a same-level neighbour's first interior layer from the snapshot the
+// previous pass published, the parent's value across a coarse-fine face
+// (PoissonAMRBound::get_dphi), 0 on a domain face, the mirror on z = 0 -- and
+// also stores them into its global ghost cells, so the arrays end the loop
+// exactly as the reference leaves them.  Every pass publishes its new first
+// interior layers for the next pass.
+template <int NX, typename CT>
+__device__ __forceinline__ CT ghost_dphi(const Geom& g, const BrickTable& bt, const DevState& st, const CT* snap_rd,
+                                         size_t stride, int b, int face, int t1, int t2) {
+    constexpr int P = NX + 2;
+    const int kind = bt.ftype[6 * b + face];
+    const int nbr = bt.fnbr[6 * b + face];
+    const CT* D = Corr<CT>::dphi(st);
+    if (kind == FACE_SIB) return __ldcg(snap_rd + (size_t)nbr * stride + ((face ^ 1) * NX + (t1 - 1)) * NX + (t2 - 1));
+    if (kind == FACE_OUTFLOW) return CT(0);
+    const int ax = face >> 1;
+    int q[3];
+    q[ax] = (face & 1) ? 1 : P - 2;
+    q[ax == 0 ? 1 : 0] = t1;
+    q[ax == 2 ? 1 : 2] = t2;
+    if (kind == FACE_REFLECT) {  // own value mirrored through z = 0, before this pass
+        const int kk = q[2] == 1 ? P - 2 : 1;
+        return D[(size_t)b * P * P * P + (kk * P + q[1]) * P + q[0]];
+    }
+    const int v = (face & 1) ? 1 : -1;
+    int r[3];
+    for (int d = 0; d < 3; d++) {
+        const int rel = bt.off[3 * b + d] + (d == ax ? v * (P - 2) : 0) - 2 * bt.off[3 * nbr + d] - (g.bw - 1);
+        r[d] = (rel + q[d]) / 2;
+    }
+    return D[(size_t)nbr * P * P * P + (r[2] * P + r[1]) * P + r[0]];
+}
+
+// One relaxation pass of brick b (block = NX^3 threads): mode 1 fills the
+// ghost faces from the snapshot snap_rd first; the relaxed interior goes to
+// dphi, its first interior layers to snap_wr, the last sweep's sum to
+// pres[b].  Called by every thread of the block.
+template <int NX, typename CT>
+__device__ __forceinline__ void op_relax_pass(const Geom& g, const BrickTable& bt, const DevState& st, int b,
+                                              int mode, const CT* snap_rd, CT* snap_wr, size_t stride,
+                                              double* pres, RelaxSmem<NX, CT>& sm) {
+    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX;
+    CT* D = Corr<CT>::dphi(st);
+    const size_t base = (size_t)b * P3;
+    const int t = threadIdx.x;
+    if (mode == 1 && t < 6 * F) {
+        const int face = t / F, qq = t % F;
+        const int t1 = qq % NX + 1, t2 = qq / NX + 1;
+        const CT gv = ghost_dphi<NX, CT>(g, bt, st, snap_rd, stride, b, face, t1, t2);
+        const int ax = face >> 1;
+        int d[3];
+        d[ax] = (face & 1) ? P - 1 : 0;
+        d[ax == 0 ? 1 : 0] = t1;
+        d[ax == 2 ? 1 : 2] = t2;
+        D[base + (d[2] * P + d[1]) * P + d[0]] = gv;
+    }
+    if (mode == 1) __syncthreads();
+    const int c = ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
+    const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
+    CT v;
+    const double resid = relax_brick<NX, CT>(sm, D + base, Corr<CT>::dphi1(st) + base, &v);
+    D[base + c] = v;
+    // publish first interior layers: layer of face f holds the cells adjacent to it
+    CT* sw = snap_wr + (size_t)b * stride;
+    if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = v;
+    if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = v;
+    if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = v;
+    if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = v;
+    if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = v;
+    if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v;
+    if (t == 0) pres[b] = resid;
+}
+
+}  // namespace amr
