@@ -31,7 +31,7 @@ class AmrConfig(ctypes.Structure):
         ("bw", ctypes.c_int), ("nx", ctypes.c_int), ("nf", ctypes.c_int), ("physics", ctypes.c_int),
         ("precision", ctypes.c_int), ("z_reflect", ctypes.c_int), ("mirror_refine_y", ctypes.c_int),
         ("max_refine_level", ctypes.c_int), ("min_level", ctypes.c_int), ("min_grid_life", ctypes.c_int),
-        ("max_bricks", ctypes.c_int), ("reserved", ctypes.c_int),
+        ("max_bricks", ctypes.c_int), ("persistent_solve", ctypes.c_int),
         ("grid_dim", ctypes.c_double), ("origin", ctypes.c_double * 3), ("minmod_theta", ctypes.c_double),
         ("cfl", ctypes.c_double), ("gamma", ctypes.c_double), ("rho_floor", ctypes.c_double),
         ("ei_floor", ctypes.c_double), ("maxdtinc", ctypes.c_double), ("grav_g", ctypes.c_double),
@@ -101,6 +101,8 @@ def load_library(path=LIB_PATH):
             lib.amr_grav_step.argtypes = [P, D, D, D, I]
             lib.amr_graph_solve.argtypes = [P, D, I, dp, ip]
             lib.amr_graph_grav_step.argtypes = [P, D, D, I, dp]
+        if hasattr(lib, "amr_solve_phases"):
+            lib.amr_solve_phases.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong), I]
         _lib = lib
     return _lib
 
@@ -335,6 +337,17 @@ class AMR:
         self._check(self.lib.amr_graph_solve(self.ctx, float(tol), int(max_cycles), ctypes.byref(e),
                                              ctypes.byref(n)))
         return e.value, n.value
+
+    SOLVE_PHASES = ("source", "restrict", "phi_faces", "phi_edges", "phi_vertices", "init", "vcycle_down",
+                    "dphi_faces", "relax_first", "relax", "coarse_correction", "retire", "forces", "adjust_force",
+                    "error")
+
+    def solve_phases(self):
+        n = len(self.SOLVE_PHASES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_longlong * n)()
+        self._check(self.lib.amr_solve_phases(self.ctx, ms, cnt, n))
+        return {k: {"ms": ms[i], "count": cnt[i]} for i, k in enumerate(self.SOLVE_PHASES)}
 
     def graph_grav_step(self, tol, dynamic_range=1.0e6, step_index=0):
         dt = ctypes.c_double()

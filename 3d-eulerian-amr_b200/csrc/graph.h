@@ -34,6 +34,17 @@ struct Control {
     int steps;
     int pad;
     int snap_par[MAX_LEVELS];  // which face-snapshot buffer the next pass reads
+    // persistent solve: device time of each phase class (from one barrier's
+    // exit to the next, i.e. the slowest block's work plus the barrier), as
+    // seen by block 0, and the number of such phases
+    unsigned long long phase_ns[16];
+    unsigned long long phase_n[16];
+};
+
+// phase classes of the persistent solve
+enum SolvePhase {
+    PH_SOURCE = 0, PH_RESTRICT, PH_PHI_FACES, PH_PHI_EDGES, PH_PHI_VERTICES, PH_INIT, PH_VDOWN, PH_DPHI_FACES,
+    PH_RELAX_FIRST, PH_RELAX, PH_CORRECT, PH_RETIRE, PH_FORCES, PH_ADJUST_FORCE, PH_ERROR, PH_COUNT
 };
 
 // snap: [2][cap][6][nx][nx] first-interior layers published by every pass

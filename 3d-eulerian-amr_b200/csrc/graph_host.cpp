@@ -19,6 +19,7 @@
 #include "context.h"
 #include "graph.h"
 #include "kernels.h"
+#include "persistent.h"
 #include "poisson.h"
 
 using namespace amr;
@@ -61,6 +62,12 @@ struct GraphState {
     // tally while recording): top level of the step / solve graph, one
     // V-cycle body outside its relaxation loops, one relaxation loop body
     long long k_step = 0, k_solve = 0, k_vbody = 0, k_rbody = 0;
+    // persistent solve: cooperative blocks, [3][cap] per-brick sums,
+    // [blocks][cap] nested-sum scratch, barrier word
+    int pblocks = 0;
+    double* d_pres3 = nullptr;
+    double* d_pnest = nullptr;
+    GridBarrier* d_bar = nullptr;
     long long rec_in_bodies = 0;  // kernels recorded inside outermost WHILE bodies
     long long rec_nested = 0;     // kernels recorded inside the bodies of the body being recorded
     int while_depth = 0;
@@ -82,6 +89,16 @@ int ensure_state(amr_ctx* c) {
     CUDA_TRY(cudaMalloc(&g->d_snap, sizeof(double) * 2 * SNAP_STRIDE * (size_t)c->cap));
     CUDA_TRY(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CUDA_TRY(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned int) * 4, c->stream));
+    if (c->cfg.persistent_solve) {
+        g->pblocks = solve_persistent_blocks(c->cfg.precision);
+        if (g->pblocks <= 0) {
+            c->err = "no cooperative launch configuration for the persistent solve";
+            return AMR_ERR_CUDA;
+        }
+        CUDA_TRY(cudaMalloc(&g->d_pres3, sizeof(double) * 3 * (size_t)c->cap));
+        CUDA_TRY(cudaMalloc(&g->d_pnest, sizeof(double) * (size_t)g->pblocks * c->cap));
+        CUDA_TRY(cudaMalloc(&g->d_bar, sizeof(GridBarrier)));
+    }
     // side streams for capturing nested loop bodies, created outside any capture
     for (int d = 0; d < 4; d++) {
         cudaStream_t s;
@@ -241,6 +258,47 @@ int rec_vcycle(amr_ctx* c, cudaStream_t s, int depth, cudaGraphConditionalHandle
     return launched(c, __LINE__);
 }
 
+// The V-cycle loop as one persistent cooperative kernel (persistent.cu).
+int rec_persistent(amr_ctx* c, cudaStream_t s, double tol) {
+    GraphState* g = c->gs;
+    SolveArgs a{};
+    a.g = c->geom;
+    a.bt = c->bt;
+    a.st = c->st;
+    a.L = g->L;
+    a.aux = PoissonAux{c->d_bphi, c->d_perr};
+    a.parents = c->d_slots;
+    const int nlev = (int)c->level_slots.size();
+    if (nlev > MAX_LEVELS || c->tree.prm.max_level + 1 > MAX_LEVELS) {
+        c->err = "too many levels for the persistent solve";
+        return AMR_ERR_ARG;
+    }
+    for (int l = 0; l < nlev; l++) {
+        a.poff[l] = c->off_parent[l];
+        a.pcnt[l] = (int)c->parent_slots[l].size();
+        a.voff[l] = c->off_vrange[l];
+    }
+    a.fitems = c->d_reflux;
+    a.force_levels = c->tree.prm.max_level + 1;
+    for (int l = 0; l <= a.force_levels; l++) a.foff[l] = c->off_reflux[l];
+    a.vitems = c->d_vitems;
+    a.vranges = c->d_vranges;
+    a.nlevels = max_level_present(c) + 1;
+    a.tol = tol;
+    a.ctl = g->d_ctl;
+    a.pres = g->d_pres3;
+    a.nest = g->d_pnest;
+    a.snap = g->d_snap;
+    a.stride = SNAP_STRIDE;
+    a.snap_half = SNAP_STRIDE * (size_t)c->cap;
+    a.bar = g->d_bar;
+    CUDA_TRY(cudaMemsetAsync(g->d_bar, 0, sizeof(GridBarrier), s));
+    CUDA_TRY(launch_solve_persistent(a, g->pblocks, s));
+    g->k_vbody = 0;
+    g->k_rbody = 0;
+    return launched(c, __LINE__);
+}
+
 // solve(): boundaries, forces, V-cycles while the L1 error > tol, restriction.
 int rec_solve(amr_ctx* c, cudaStream_t s, double tol, int depth) {
     GraphState* g = c->gs;
@@ -252,13 +310,17 @@ int rec_solve(amr_ctx* c, cudaStream_t s, double tol, int depth) {
         return AMR_ERR_STATE;
     }
     TRY(rec_forces(c, s));
-    TRY(add_while(
-        c, s, depth,
-        [&](cudaStream_t q, cudaGraphConditionalHandle h) {
-            launch_open_loop(h, g->d_ctl, 1, q);
-            return launched(c, __LINE__);
-        },
-        [&](cudaStream_t q, cudaGraphConditionalHandle h) { return rec_vcycle(c, q, depth + 1, h, tol); }));
+    if (c->cfg.persistent_solve) {
+        TRY(rec_persistent(c, s, tol));
+    } else {
+        TRY(add_while(
+            c, s, depth,
+            [&](cudaStream_t q, cudaGraphConditionalHandle h) {
+                launch_open_loop(h, g->d_ctl, 1, q);
+                return launched(c, __LINE__);
+            },
+            [&](cudaStream_t q, cudaGraphConditionalHandle h) { return rec_vcycle(c, q, depth + 1, h, tol); }));
+    }
     for (int l = c->tree.prm.max_level; l >= 0; l--)
         launch_inject(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l], (int)c->parent_slots[l].size(), s);
     return launched(c, __LINE__);
@@ -411,12 +473,31 @@ void graph_release(amr_ctx* c) {
     if (g->d_nest) cudaFree(g->d_nest);
     if (g->d_snap) cudaFree(g->d_snap);
     if (g->d_counter) cudaFree(g->d_counter);
+    if (g->d_pres3) cudaFree(g->d_pres3);
+    if (g->d_pnest) cudaFree(g->d_pnest);
+    if (g->d_bar) cudaFree(g->d_bar);
     delete g;
     c->gs = nullptr;
 }
 }  // namespace amr
 
 extern "C" {
+
+// Device time per phase class of the persistent solve, accumulated over all
+// persistent solves of the context (ms[PH_COUNT], counts[PH_COUNT]).
+int amr_solve_phases(amr_ctx* c, double* ms, long long* counts, int n) {
+    if (!c || !ms || !counts || n < PH_COUNT) return AMR_ERR_ARG;
+    if (!c->gs) {
+        for (int p = 0; p < PH_COUNT; p++) ms[p] = 0.0, counts[p] = 0;
+        return AMR_OK;
+    }
+    TRY(read_ctl(c));
+    for (int p = 0; p < PH_COUNT; p++) {
+        ms[p] = c->gs->h_ctl->phase_ns[p] * 1e-6;
+        counts[p] = (long long)c->gs->h_ctl->phase_n[p];
+    }
+    return AMR_OK;
+}
 
 // The Poisson solve as one graph launch (see amr_poisson_solve).
 int amr_graph_solve(amr_ctx* c, double tol, int max_cycles, double* l1_error, int* cycles) {
@@ -435,6 +516,10 @@ int amr_graph_solve(amr_ctx* c, double tol, int max_cycles, double* l1_error, in
     count_replay(c, g->k_solve);
     if (l1_error) *l1_error = g->h_ctl->err;
     if (cycles) *cycles = g->h_ctl->cycles;
+    if (g->h_ctl->status == 3) {
+        c->err = "persistent solve: a grid barrier timed out";
+        return AMR_ERR_TIMEOUT;
+    }
     if (g->h_ctl->status) {
         c->err = g->h_ctl->status == 2 ? "Poisson solve exceeded max_cycles" : "relaxation loop exceeded its cap";
         return AMR_ERR_NOCONVERGE;
@@ -464,6 +549,10 @@ int amr_graph_grav_step(amr_ctx* c, double tol, double dynamic_range, int step_i
     CUDA_TRY(cudaGraphLaunch(g->step_exec, c->stream));
     TRY(read_ctl(c));
     count_replay(c, g->k_step);
+    if (g->h_ctl->status == 3) {
+        c->err = "persistent solve: a grid barrier timed out";
+        return AMR_ERR_TIMEOUT;
+    }
     if (g->h_ctl->status) {
         c->err = "solve inside the captured step did not converge";
         return AMR_ERR_NOCONVERGE;

@@ -1,0 +1,335 @@
+// Persistent multigrid solve: the whole V-cycle loop of Poisson::solve (the
+// drivers' `while (err > toler) vcycle()`, binary_driver.cpp:296-330) in one
+// cooperative launch.  Every dependent step of the reference's sequence --
+// restriction of phi level by level, the phi ghost faces / edges / vertices
+// of each level, the down sweep (vcycle_down + relax_until(1.0)) and the up
+// sweep (coarse correction, relax_until(0.05), retire, ghosts) of each
+// level, the forces with their coarse-fine averages, the L1 error -- is a
+// phase separated from the next by a grid barrier instead of a kernel
+// boundary.  The phases run the same device functions as the
+// one-launch-per-step kernels (poisson_ops.cuh, graph_ops.cuh), so the
+// result is bitwise that of the plain and graph forms.
+//
+// Loop decisions (relaxation ratio, L1 error > tol) need the reference's
+// nested sums over the per-brick values; every block forms them itself, in
+// its own scratch, from the same values, so all blocks take the same
+// decision without another barrier.  Per-brick values are double-buffered
+// by pass so a block still summing one pass cannot see the next pass's.
+//
+// The grid barrier spins with a bound: a block that waits longer than
+// BARRIER_SPINS polls sets the abort word, every block leaves at its next
+// barrier, and the host reports AMR_ERR_TIMEOUT.
+#include <cuda_runtime.h>
+
+#include "graph_ops.cuh"
+#include "launch.cuh"
+#include "persistent.h"
+#include "poisson_ops.cuh"
+
+namespace amr {
+
+namespace {
+
+constexpr unsigned long long BARRIER_SPINS = 1ull << 22;
+
+__device__ __forceinline__ int ld_volatile(const int* p) { return *(const volatile int*)p; }
+__device__ __forceinline__ unsigned ld_volatile(const unsigned* p) { return *(const volatile unsigned*)p; }
+
+// Grid-wide barrier of a cooperative launch; false when the solve aborted.
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
+    __shared__ int ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int good = ld_volatile(&bar->abort) ? 0 : 1;
+        if (good) {
+            const unsigned gen = ld_volatile(&bar->gen);
+            __threadfence();
+            if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
+                atomicExch(&bar->count, 0u);
+                __threadfence();
+                atomicAdd(&bar->gen, 1u);
+            } else {
+                unsigned long long spins = 0;
+                while (ld_volatile(&bar->gen) == gen) {
+                    if (ld_volatile(&bar->abort)) {
+                        good = 0;
+                        break;
+                    }
+                    if (++spins > BARRIER_SPINS) {
+                        atomicExch(&bar->abort, 1);
+                        good = 0;
+                        break;
+                    }
+                    if (spins > 64) __nanosleep(32);
+                }
+            }
+            __threadfence();
+        }
+        ok = good;
+    }
+    __syncthreads();
+    return ok != 0;
+}
+
+template <typename CT>
+struct Solver {
+    const SolveArgs& a;
+    RelaxSmem<8, CT>& sm;
+    double* red;
+    double* nest;    // this block's scratch [cap]
+    int relax_par;   // pres buffer of the next relaxation pass
+    int status;
+    long long relax_calls;
+    int max_outer;
+    unsigned long long t_last;  // block 0: global time at the last barrier exit
+    unsigned long long ph_ns[PH_COUNT];
+    unsigned ph_n[PH_COUNT];
+
+    __device__ static unsigned long long now() {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        return t;
+    }
+
+    // barrier closing a phase of class ph
+    __device__ bool sync(int ph) {
+        const bool ok = grid_sync(a.bar);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long t = now();
+            ph_ns[ph] += t - t_last;
+            ph_n[ph]++;
+            t_last = t;
+        }
+        return ok;
+    }
+
+    // this block's share of n items
+    template <typename F>
+    __device__ void each(int n, F f) {
+        for (int q = blockIdx.x; q < n; q += gridDim.x) f(q);
+    }
+
+    __device__ const int* level(int l) const { return a.L.slots + a.L.off[l]; }
+
+    // enforce_phi_boundaries of one level: faces, then edges (reading the
+    // neighbours' face ghosts), then vertices (reading their edge ghosts)
+    __device__ bool phi_boundaries(int l) {
+        const int* sl = level(l);
+        const int n = a.L.cnt[l];
+        const int t = threadIdx.x;
+        each(n, [&](int q) {
+            if (t < 384) op_phi_faces(a.g, a.bt, a.st, a.aux, sl[q], t / 64, t % 64, 64);
+        });
+        if (!sync(PH_PHI_FACES)) return false;
+        each(n, [&](int q) {
+            if (t < a.g.pnx - 2) op_phi_edges(a.g, a.bt, a.st, a.aux, sl[q], t + 1);
+        });
+        if (!sync(PH_PHI_EDGES)) return false;
+        each(n, [&](int q) {
+            if (t == 0) op_phi_vertices(a.g, a.bt, a.st, a.aux, sl[q]);
+        });
+        return sync(PH_PHI_VERTICES);
+    }
+
+    // Poisson::vcycle_relax sum over level l (poisson.cpp:107, nested as the
+    // recursion adds it) from buffer `buf` of the per-brick sums
+    __device__ double level_sum(int l, const double* buf) {
+        if (l == 0) return __ldcg(buf + a.L.slots[a.L.off[0]]);
+        __syncthreads();
+        return nested_sum_block(a.L, a.bt.child, buf, nest, l, false);
+    }
+
+    // relax_until (poisson.cpp:66-70, 74-78): ghosts, one pass, then passes
+    // with ghosts from the previous pass's snapshot until the level sum has
+    // fallen to `ratio` of the first
+    __device__ bool relax_until(int l, double ratio) {
+        const int* sl = level(l);
+        const int n = a.L.cnt[l];
+        const int t = threadIdx.x;
+        CT* snap = reinterpret_cast<CT*>(a.snap);
+        each(n, [&](int q) {
+            if (t < 384) op_dphi_faces<CT>(a.g, a.bt, a.st, a.aux, sl[q], t / 64, t % 64, 64);
+        });
+        if (!sync(PH_DPHI_FACES)) return false;
+        int par = 0;
+        double* pres = a.pres + (size_t)relax_par * a.L.cap;
+        each(n, [&](int q) {
+            op_relax_pass<8, CT>(a.g, a.bt, a.st, sl[q], 0, snap, snap, a.stride, pres, sm);
+            __syncthreads();
+        });
+        if (!sync(PH_RELAX_FIRST)) return false;
+        const double r0 = level_sum(l, pres);
+        relax_par ^= 1;
+        relax_calls++;
+        int outer = 0;
+        for (;;) {
+            pres = a.pres + (size_t)relax_par * a.L.cap;
+            const CT* rd = snap + (size_t)par * a.snap_half;
+            CT* wr = snap + (size_t)(par ^ 1) * a.snap_half;
+            each(n, [&](int q) {
+                op_relax_pass<8, CT>(a.g, a.bt, a.st, sl[q], 1, rd, wr, a.stride, pres, sm);
+                __syncthreads();
+            });
+            if (!sync(PH_RELAX)) return false;
+            par ^= 1;
+            const double r = level_sum(l, pres);
+            relax_par ^= 1;
+            relax_calls++;
+            ++outer;
+            bool again = r / r0 > ratio;
+            if (again && outer > max_outer) {
+                again = false;
+                status = 1;
+            }
+            if (!again) break;
+        }
+        return true;
+    }
+
+    // Poisson::vcycle (poisson.cpp:1069-1074) = vcycle0 (poisson.cpp:53-84)
+    // without the two dphi ghost fills that nothing reads (see vcycle0 in
+    // poisson_host.cpp)
+    __device__ bool vcycle() {
+        const int t = threadIdx.x;
+        const int maxl = a.nlevels - 1;
+        each(a.L.nall, [&](int q) { op_set_source(a.g, a.st, a.L.all[q], t, blockDim.x); });
+        if (!sync(PH_SOURCE)) return false;
+        for (int l = maxl - 1; l >= 0; l--) {
+            const int* pl = a.parents + a.poff[l];
+            each(a.pcnt[l], [&](int q) { op_phi_from_children(a.g, a.bt, a.st, pl[q], t / 64, t % 64); });
+            if (!sync(PH_RESTRICT)) return false;
+        }
+        for (int l = 0; l <= maxl; l++)
+            if (!phi_boundaries(l)) return false;
+        each(a.L.nall, [&](int q) { op_init_vcycle<CT>(a.g, a.st, a.L.all[q], t, blockDim.x); });
+        if (!sync(PH_INIT)) return false;
+        for (int l = maxl; l >= 0; l--) {
+            const int* sl = level(l);
+            each(a.L.cnt[l], [&](int q) {
+                op_vdown<CT>(a.g, a.bt, a.st, sl[q], a.vitems, a.vranges + 4 * (a.voff[l] + q));
+                __syncthreads();
+            });
+            if (!sync(PH_VDOWN)) return false;
+            if (!relax_until(l, 1.0)) return false;
+        }
+        for (int l = 0; l <= maxl; l++) {
+            const int* sl = level(l);
+            if (l > 0) {
+                each(a.L.cnt[l], [&](int q) { op_coarse_correction<CT>(a.g, a.bt, a.st, sl[q], t); });
+                if (!sync(PH_CORRECT)) return false;
+            }
+            if (!relax_until(l, 0.05)) return false;
+            each(a.L.cnt[l], [&](int q) { op_retire<CT>(a.g, a.st, sl[q], t, blockDim.x); });
+            if (!sync(PH_RETIRE)) return false;
+            if (!phi_boundaries(l)) return false;
+        }
+        return true;
+    }
+
+    // compute_forces + adjust_{x,y,z}_force level by level, finest first
+    __device__ bool forces() {
+        const int t = threadIdx.x;
+        each(a.L.nall, [&](int q) { op_forces(a.g, a.bt, a.st, a.L.all[q], t, blockDim.x); });
+        if (!sync(PH_FORCES)) return false;
+        for (int l = a.force_levels - 1; l >= 0; l--) {
+            const int n = a.foff[l + 1] - a.foff[l];
+            if (n <= 0) continue;
+            const RefluxItem* it = a.fitems + a.foff[l];
+            each(n, [&](int q) { op_adjust_force(a.g, a.st, it[q], t); });
+            if (!sync(PH_ADJUST_FORCE)) return false;
+        }
+        return true;
+    }
+
+    // Poisson::solution_error (poisson.cpp:637-669), nested over the tree;
+    // the per-brick sums with 256 threads, as the error kernels form them
+    __device__ bool error(double* err) {
+        const int nl = a.nlevels;
+        double* perr = a.pres + 2 * (size_t)a.L.cap;
+        each(a.L.nall, [&](int q) {
+            op_solution_error<CT>(a.g, a.bt, a.st, a.L.all[q], perr, red, 256);
+            __syncthreads();
+        });
+        if (!sync(PH_ERROR)) return false;
+        // deepest level: nest = own; then own + children level by level
+        const int* sl = a.L.slots + a.L.off[nl - 1];
+        for (int q = threadIdx.x; q < a.L.cnt[nl - 1]; q += blockDim.x) nest[sl[q]] = __ldcg(perr + sl[q]);
+        __syncthreads();
+        *err = nested_sum_block(a.L, a.bt.child, perr, nest, nl - 1, true);
+        return true;
+    }
+};
+
+template <typename CT>
+__global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
+    __shared__ RelaxSmem<8, CT> sm;
+    __shared__ double red[16];
+    __shared__ double s_err;
+    // loop limits are read from the control block (set by the host before
+    // every launch; a captured graph keeps its arguments)
+    const int max_cycles = *(volatile int*)&a.ctl->max_cycles;
+    Solver<CT> s{a, sm, red, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0, *(volatile int*)&a.ctl->max_outer};
+    s.t_last = Solver<CT>::now();
+    for (int p = 0; p < PH_COUNT; p++) {
+        s.ph_ns[p] = 0;
+        s.ph_n[p] = 0;
+    }
+    int cycles = 0;
+    bool ok = true;
+    double err = 0.0;
+    for (;;) {
+        if (!(ok = s.vcycle())) break;
+        if (!(ok = s.forces())) break;
+        if (!(ok = s.error(&err))) break;
+        if (threadIdx.x == 0) s_err = err;
+        __syncthreads();
+        err = s_err;
+        cycles++;
+        if (!(err > a.tol)) break;
+        if (cycles >= max_cycles) {
+            s.status = 2;
+            break;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        Control* c = a.ctl;
+        if (!ok) {
+            c->status = 3;
+        } else {
+            c->err = err;
+            c->cycles = cycles;
+            c->cycles_total += cycles;
+            c->relax_calls += s.relax_calls;
+            if (s.status) c->status = s.status;
+            for (int p = 0; p < PH_COUNT; p++) {
+                c->phase_ns[p] += s.ph_ns[p];
+                c->phase_n[p] += s.ph_n[p];
+            }
+        }
+    }
+}
+
+}  // namespace
+
+int solve_persistent_blocks(int precision) {
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+    const cudaError_t e =
+        precision == AMR_PREC_MIXED
+            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_persistent<float>, 512, 0)
+            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_persistent<double>, 512, 0);
+    if (e != cudaSuccess || per <= 0) return -1;
+    return sms * per;
+}
+
+cudaError_t launch_solve_persistent(const SolveArgs& a, int blocks, cudaStream_t s) {
+    ++g_launch_tally;
+    void* args[] = {const_cast<SolveArgs*>(&a)};
+    if (a.g.precision == AMR_PREC_MIXED)
+        return cudaLaunchCooperativeKernel((const void*)k_solve_persistent<float>, dim3(blocks), dim3(512), args, 0,
+                                           s);
+    return cudaLaunchCooperativeKernel((const void*)k_solve_persistent<double>, dim3(blocks), dim3(512), args, 0, s);
+}
+
+}  // namespace amr

@@ -1,0 +1,50 @@
+// Persistent multigrid solve (persistent.cu): arguments and launch.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "amr_internal.h"
+#include "graph.h"
+#include "poisson_ops.cuh"
+
+namespace amr {
+
+// Grid barrier state; zero it before every launch.
+struct GridBarrier {
+    unsigned int count;
+    unsigned int gen;
+    int abort;
+    int pad;
+};
+
+struct SolveArgs {
+    Geom g;
+    BrickTable bt;
+    DevState st;
+    LevelLists L;
+    PoissonAux aux;
+    const int* parents;  // bricks with children, per level: parents + poff[l], pcnt[l]
+    int poff[MAX_LEVELS];
+    int pcnt[MAX_LEVELS];
+    const RefluxItem* fitems;  // coarse-fine items sorted by coarse level (force averages)
+    int foff[MAX_LEVELS + 1];
+    int force_levels;
+    const RefluxItem* vitems;  // items grouped by coarse brick for the down sweep
+    const int* vranges;
+    int voff[MAX_LEVELS];
+    int nlevels;  // levels present
+    double tol;
+    Control* ctl;  // also holds the loop limits max_cycles, max_outer
+    double* pres;  // [3][cap]: two relaxation buffers, one for the L1 error
+    double* nest;  // [blocks][cap] per-block nested-sum scratch
+    void* snap;    // [2][cap][stride] face snapshots (CT entries)
+    size_t stride;
+    size_t snap_half;
+    GridBarrier* bar;
+};
+
+// Blocks of one cooperative launch on the current device (all resident).
+int solve_persistent_blocks(int precision);
+cudaError_t launch_solve_persistent(const SolveArgs& a, int blocks, cudaStream_t s);
+
+}  // namespace amr

@@ -181,13 +181,15 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
     form: "fp64"  plain FP64, host-orchestrated (reference operation order)
           "graph" FP64, whole RK3 step replayed from a captured CUDA graph with
                   every loop decided on the device (bitwise equal to fp64)
-          "mixed" the graph form with the multigrid correction (smoothing,
-                  restriction, prolongation of dphi) and the KT flux in FP32;
-                  residual, potential and conserved update in FP64
+          "persistent" the graph form with each solve's V-cycle loop as one
+                  persistent cooperative kernel (bitwise equal to fp64)
+          "mixed" the persistent form with the multigrid correction
+                  (smoothing, restriction, prolongation of dphi) and the KT
+                  flux in FP32; residual, potential and conserved update FP64
     """
     prec = amr.PREC_MIXED if form == "mixed" else amr.PREC_FP64
     a = amr.AMR(physics=amr.PHYSICS_EULER_GRAVITY, max_refine_level=LEVELS, grid_dim=0.5, z_reflect=0,
-                max_bricks=8192, precision=prec)
+                max_bricks=8192, precision=prec, persistent_solve=1 if form in ("persistent", "mixed") else 0)
     ini.build_tree(a, "polytrope", 1.0e-6, 0.5, 0, LEVELS, device=True)
     stream = torch.cuda.ExternalStream(a.stream_handle())
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -495,7 +497,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="mixed", choices=["fp64", "graph", "mixed"])
+    ap.add_argument("--form", default="mixed", choices=["fp64", "graph", "persistent", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--json-out", default=None)
@@ -517,13 +519,14 @@ def main():
                                 device_id=torch.device("cuda", local))
     amr, ini = load_amr()
     head = run_form(amr, ini, args.form, args, world, local, torch, dist, e2e=True, profile=True)
-    plain = graph64 = None
+    plain = graph64 = pers64 = None
     errors = None
     pcheck = None
     if not args.no_compare and args.form != "fp64":
         plain = run_form(amr, ini, "fp64", args, world, local, torch, dist)
         if args.form == "mixed":
             graph64 = run_form(amr, ini, "graph", args, world, local, torch, dist)
+            pers64 = run_form(amr, ini, "persistent", args, world, local, torch, dist)
             errors = state_errors(head["final"], plain["final"], 2)
             errors["steps"] = args.warmup + args.steps
             errors["against"] = "plain FP64 form (parity-tested against the reference CPU code)"
@@ -560,6 +563,9 @@ def main():
             "fp64_graph": None if graph64 is None else {"value": graph64["value"],
                                                          "ms_per_step": graph64["ms_per_step"],
                                                          "gpu_launches": graph64["gpu_launches"]},
+            "fp64_persistent": None if pers64 is None else {"value": pers64["value"],
+                                                             "ms_per_step": pers64["ms_per_step"],
+                                                             "gpu_launches": pers64["gpu_launches"]},
             "errors_vs_fp64": errors,
             "poisson_precision": pcheck,
             "helmholtz_eos": eos,

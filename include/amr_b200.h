@@ -60,7 +60,8 @@ typedef struct amr_config {
     int min_level;        /* MINLEVEL (defs.h:22) */
     int min_grid_life;    /* MIN_GRID_LIFE (defs.h:23) */
     int max_bricks;       /* device brick pool capacity; 0 = host-only context */
-    int reserved;
+    int persistent_solve; /* 1: the graph forms run each Poisson solve's V-cycle loop as one
+                             persistent cooperative kernel (same results bit for bit) */
     double grid_dim;      /* GRID_DIM */
     double origin[3];     /* Grid::origin (grid/grid.h:23) */
     double minmod_theta;  /* MINMOD_THETA (euler_defs.h:21) */
@@ -186,6 +187,13 @@ int amr_graph_grav_step(amr_ctx* ctx, double tol, double dynamic_range, int step
  * forces solution_error source phys_boundary coarse_correction phi_time other.
  */
 int amr_get_stream(amr_ctx* ctx, void** stream);  /* the context's cudaStream_t */
+/* Persistent solve (persistent_solve = 1): device time and count per phase
+ * class, summed over the context's persistent solves; n >= 15.  Classes:
+ * source restrict phi_faces phi_edges phi_vertices init vcycle_down
+ * dphi_faces relax_first relax coarse_correction retire forces
+ * adjust_force error.  A phase's time runs from one grid barrier's exit to
+ * the next as block 0 sees it (slowest block's work + the barrier). */
+int amr_solve_phases(amr_ctx* ctx, double* ms, long long* counts, int n);
 int amr_profile_enable(amr_ctx* ctx, int on);
 int amr_profile_reset(amr_ctx* ctx);
 int amr_profile_get(amr_ctx* ctx, int cls, double* ms, long long* launches, const char** name);

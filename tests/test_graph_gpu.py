@@ -3,7 +3,9 @@
 amr_graph_solve / amr_graph_grav_step run the same kernels as
 amr_poisson_solve / amr_grav_step, with the loop decisions (relaxation
 ratios, the L1 error test, the CFL step) taken on the device from the same
-nested sums; every array must come out identical.
+nested sums; every array must come out identical.  With persistent_solve the
+V-cycle loop of each solve is one cooperative kernel whose phases are
+separated by grid barriers; it too must reproduce the plain form exactly.
 """
 
 import numpy as np
@@ -12,9 +14,9 @@ import pytest
 from cases import VARIANTS, load_golden, same_tree
 
 
-def make(gpu, maxlevel):
+def make(gpu, maxlevel, persistent=0):
     return gpu.AMR(max_refine_level=maxlevel, max_bricks=2048, physics=gpu.PHYSICS_EULER_GRAVITY,
-                   **VARIANTS["g05"])
+                   persistent_solve=persistent, **VARIANTS["g05"])
 
 
 def load_state(a, g):
@@ -26,9 +28,10 @@ def load_state(a, g):
 
 
 @pytest.mark.gpu
-def test_graph_solve_is_bitwise_plain(gpu):
+@pytest.mark.parametrize("persistent", [0, 1])
+def test_graph_solve_is_bitwise_plain(gpu, persistent):
     g = load_golden("poisson_poly_L2")
-    a, b = make(gpu, 2), make(gpu, 2)
+    a, b = make(gpu, 2), make(gpu, 2, persistent)
     load_state(a, g)
     load_state(b, g)
     ea, na = a.poisson_solve(1.0e-7)
@@ -44,9 +47,10 @@ def test_graph_solve_is_bitwise_plain(gpu):
 
 
 @pytest.mark.gpu
-def test_graph_grav_steps_are_bitwise_plain(gpu):
+@pytest.mark.parametrize("persistent", [0, 1])
+def test_graph_grav_steps_are_bitwise_plain(gpu, persistent):
     g = load_golden("grav_poly_L2")
-    a, b = make(gpu, 2), make(gpu, 2)
+    a, b = make(gpu, 2), make(gpu, 2, persistent)
     load_state(a, g)
     load_state(b, g)
     last = 0.0
