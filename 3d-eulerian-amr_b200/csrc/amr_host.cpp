@@ -268,6 +268,30 @@ int rebuild_topology(amr_ctx* c) {
             }
         }
     }
+    // child positions within the next level's list, for the level sums
+    {
+        std::vector<int> pos(c->cap > 0 ? c->cap : 1, -1), cp;
+        c->max_level_cnt = 0;
+        for (int l = 0; l <= maxl; l++) {
+            const std::vector<int>& ls = c->level_slots[l];
+            c->max_level_cnt = std::max(c->max_level_cnt, (int)ls.size());
+            for (int q = 0; q < (int)ls.size(); q++) pos[ls[q]] = q;
+        }
+        for (int l = 0; l <= maxl; l++)
+            for (int s : c->level_slots[l])
+                for (int q = 0; q < 8; q++) {
+                    const int ch = c->h_child[8 * s + q];
+                    cp.push_back(ch >= 0 ? pos[ch] : -1);
+                }
+        if ((int)cp.size() > c->cpos_cap) {
+            if (c->d_cpos) cudaFree(c->d_cpos);
+            c->cpos_cap = (int)cp.size() * 2 + 64;
+            CUDA_TRY(cudaMalloc(&c->d_cpos, sizeof(int) * c->cpos_cap));
+        }
+        if (!cp.empty())
+            CUDA_TRY(cudaMemcpyAsync(c->d_cpos, cp.data(), sizeof(int) * cp.size(), cudaMemcpyHostToDevice,
+                                     c->stream));
+    }
     // per coarse brick, in level-list order: its x, then y, then z items
     {
         std::vector<RefluxItem> vitems;
@@ -553,7 +577,7 @@ int amr_destroy(amr_ctx* c) {
                         c->st.phi0, c->st.dphi, c->st.dphi1,  c->st.S,      c->st.fx,      c->st.fy,
                         c->st.fz,   c->bt.level, c->bt.off,   c->bt.h,      c->bt.ftype,   c->bt.fnbr,
                         c->bt.parent, c->bt.cidx, c->bt.child, c->d_fo,     c->d_dt,       c->d_red,
-                        c->d_flags, c->d_stage, c->d_slots,  c->d_reflux, c->d_vitems, c->d_vranges,
+                        c->d_flags, c->d_stage, c->d_slots,  c->d_reflux, c->d_vitems, c->d_vranges, c->d_cpos,
                         c->st.fdphi, c->st.fdphi1};
         for (void* p : ptrs)
             if (p) cudaFree(p);

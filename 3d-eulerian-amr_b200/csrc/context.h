@@ -67,6 +67,9 @@ struct amr_ctx {
     // d_vranges[4 (off_vrange[l] + q) + 0..3] = first x, y, z item, end
     amr::RefluxItem* d_vitems = nullptr;
     int* d_vranges = nullptr;
+    // [8 e + c]: list position of child c of level-list entry e (-1: none)
+    int* d_cpos = nullptr;
+    int cpos_cap = 0, max_level_cnt = 0;
     int vitems_cap = 0, vranges_cap = 0;
     std::vector<int> off_vrange;
     int vcycle_max_outer = 1000;

@@ -17,7 +17,16 @@ struct LevelLists {
     int cap;           // brick pool capacity (slot range)
     int off[MAX_LEVELS];
     int cnt[MAX_LEVELS];
+    // cpos[8 e + c]: position, in the next level's list, of child c of the
+    // brick at entry e of the packed level lists (e = off[m] - off[0] + q),
+    // or -1
+    const int* cpos;
+    int max_cnt;  // largest level count
 };
+
+// level sums formed in shared memory when every level has at most this
+// many bricks
+constexpr int NEST_SMEM = 768;
 
 // Loop state shared between graph kernels and the host.
 struct Control {

@@ -126,6 +126,8 @@ void fill_lists(amr_ctx* c) {
         L.off[m] = ok ? c->off_level[m] : 0;
         L.cnt[m] = ok ? (int)c->level_slots[m].size() : 0;
     }
+    L.cpos = c->d_cpos;
+    L.max_cnt = c->max_level_cnt;
 }
 
 cudaStream_t body_stream(amr_ctx* c, int depth) {

@@ -22,6 +22,7 @@ __global__ void __launch_bounds__(NX* NX* NX)
                 cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest, unsigned int* counter,
                 CT* snap, size_t stride, size_t snap_half) {
     __shared__ RelaxSmem<NX, CT> sm;
+    __shared__ double nbuf[2 * NEST_SMEM];
     __shared__ bool last;
     const int b = L.slots[L.off[level] + blockIdx.x];
     const int t = threadIdx.x;
@@ -37,7 +38,9 @@ __global__ void __launch_bounds__(NX* NX* NX)
     __syncthreads();
     if (!last) return;
     __threadfence();
-    const double r = level == 0 ? __ldcg(pres + b) : nested_sum_block(L, bt.child, pres, nest, level, false);
+    const double r = level == 0                 ? __ldcg(pres + b)
+                     : L.max_cnt <= NEST_SMEM ? nested_sum_smem(L, pres, level, false, nbuf)
+                                              : nested_sum_block(L, bt.child, pres, nest, level, false);
     if (t == 0) {
         *counter = 0u;
         ctl->relax_calls++;
@@ -71,6 +74,7 @@ __global__ void k_error_dev(Geom g, BrickTable bt, DevState st, LevelLists L, in
     const double h3 = h * h * h, hinv = 1.0 / h;
     const size_t base = (size_t)b * g.pnx3;
     __shared__ double red[32];
+    __shared__ double nbuf[2 * NEST_SMEM];
     __shared__ bool last;
     double sum = 0.0;
     for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
@@ -102,11 +106,16 @@ __global__ void k_error_dev(Geom g, BrickTable bt, DevState st, LevelLists L, in
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // deepest level: nest = own
-    const int* sl = L.slots + L.off[nlevels - 1];
-    for (int q = threadIdx.x; q < L.cnt[nlevels - 1]; q += blockDim.x) nest[sl[q]] = __ldcg(pres + sl[q]);
-    __syncthreads();
-    const double e = nested_sum_block(L, bt.child, pres, nest, nlevels - 1, true);
+    double e;
+    if (L.max_cnt <= NEST_SMEM) {
+        e = nested_sum_smem(L, pres, nlevels - 1, true, nbuf);
+    } else {
+        // deepest level: nest = own
+        const int* sl = L.slots + L.off[nlevels - 1];
+        for (int q = threadIdx.x; q < L.cnt[nlevels - 1]; q += blockDim.x) nest[sl[q]] = __ldcg(pres + sl[q]);
+        __syncthreads();
+        e = nested_sum_block(L, bt.child, pres, nest, nlevels - 1, true);
+    }
     if (threadIdx.x == 0) {
         *counter = 0u;
         ctl->err = e;

@@ -45,6 +45,40 @@ __device__ inline double nested_sum_block(const LevelLists& L, const int* __rest
 // also stores them into its global ghost cells, so the arrays end the loop
 // exactly as the reference leaves them.  Every pass publishes its new first
 // interior layers for the next pass.
+// The same nested sum staged level by level in shared memory (buf:
+// 2 * NEST_SMEM doubles) through the child-position table: leaves are the
+// bricks of level `top` with values leaf[slot]; S(p) = ((own + S(c0)) +
+// S(c1)) + ... in child order, own = leaf[p] when withown, else 0.  Same
+// additions in the same order as nested_sum_block; the result is returned
+// to every thread.  Needs L.max_cnt <= NEST_SMEM.
+__device__ inline double nested_sum_smem(const LevelLists& L, const double* leaf, int top, bool withown,
+                                         double* buf) {
+    double* vb = buf;
+    double* ub = buf + NEST_SMEM;
+    const int e0 = L.off[0];
+    for (int q = threadIdx.x; q < L.cnt[top]; q += blockDim.x) vb[q] = __ldcg(leaf + L.slots[L.off[top] + q]);
+    __syncthreads();
+    for (int m = top - 1; m >= 0; m--) {
+        for (int q = threadIdx.x; q < L.cnt[m]; q += blockDim.x) {
+            const int* cp = L.cpos + 8 * (L.off[m] - e0 + q);
+            double s = withown ? __ldcg(leaf + L.slots[L.off[m] + q]) : 0.0;
+#pragma unroll
+            for (int c = 0; c < 8; c++) {
+                const int pos = cp[c];
+                if (pos >= 0) s += vb[pos];
+            }
+            ub[q] = s;
+        }
+        __syncthreads();
+        double* t = vb;
+        vb = ub;
+        ub = t;
+    }
+    const double r = vb[0];
+    __syncthreads();
+    return r;
+}
+
 template <int NX, typename CT>
 __device__ __forceinline__ CT ghost_dphi(const Geom& g, const BrickTable& bt, const DevState& st, const CT* snap_rd,
                                          size_t stride, int b, int face, int t1, int t2) {
@@ -110,6 +144,49 @@ __device__ __forceinline__ void op_relax_pass(const Geom& g, const BrickTable& b
     if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = v;
     if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v;
     if (t == 0) pres[b] = resid;
+}
+
+// op_relax_pass for half a block (NX^3/2 threads, local index lt, barrier
+// `bar`): the same pass with two cells per thread (relax_brick_half), so
+// that one block relaxes two bricks at once.
+template <int NX, typename CT>
+__device__ __forceinline__ void op_relax_pass_half(const Geom& g, const BrickTable& bt, const DevState& st, int b,
+                                                   int mode, const CT* snap_rd, CT* snap_wr, size_t stride,
+                                                   double* pres, RelaxSmem<NX, CT>& sm, int lt, int bar) {
+    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX, HT = NX * NX * NX / 2;
+    CT* D = Corr<CT>::dphi(st);
+    const size_t base = (size_t)b * P3;
+    if (mode == 1) {
+        for (int q = lt; q < 6 * F; q += HT) {
+            const int face = q / F, qq = q % F;
+            const int t1 = qq % NX + 1, t2 = qq / NX + 1;
+            const CT gv = ghost_dphi<NX, CT>(g, bt, st, snap_rd, stride, b, face, t1, t2);
+            const int ax = face >> 1;
+            int d[3];
+            d[ax] = (face & 1) ? P - 1 : 0;
+            d[ax == 0 ? 1 : 0] = t1;
+            d[ax == 2 ? 1 : 2] = t2;
+            D[base + (d[2] * P + d[1]) * P + d[0]] = gv;
+        }
+        named_sync(bar, HT);
+    }
+    CT v[2];
+    const double resid = relax_brick_half<NX, CT>(sm, D + base, Corr<CT>::dphi1(st) + base, v, lt, bar);
+    CT* sw = snap_wr + (size_t)b * stride;
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int t = lt + h * HT;
+        const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
+        const int c = (ck * P + cj) * P + ci;
+        D[base + c] = v[h];
+        if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = v[h];
+        if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = v[h];
+        if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = v[h];
+        if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = v[h];
+        if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = v[h];
+        if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v[h];
+    }
+    if (lt == 0) pres[b] = resid;
 }
 
 }  // namespace amr

@@ -74,9 +74,10 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
 template <typename CT>
 struct Solver {
     const SolveArgs& a;
-    RelaxSmem<8, CT>& sm;
+    RelaxSmem<8, CT>* sm;  // two: one per half block
     double* red;
-    double* nest;    // this block's scratch [cap]
+    double* nbuf;    // 2 * NEST_SMEM doubles of shared memory for the level sums
+    double* nest;    // this block's scratch [cap] (level sums of larger trees)
     int relax_par;   // pres buffer of the next relaxation pass
     int status;
     long long relax_calls;
@@ -109,6 +110,24 @@ struct Solver {
         for (int q = blockIdx.x; q < n; q += gridDim.x) f(q);
     }
 
+    // one relaxation pass over the n bricks sl[]: one brick per block, or
+    // two per block (one per half, two cells per thread) when the level has
+    // more bricks than there are blocks; the results are the same either way
+    __device__ void relax_pass(const int* sl, int n, int mode, const CT* rd, CT* wr, double* pres) {
+        if (n <= (int)gridDim.x) {
+            each(n, [&](int q) {
+                op_relax_pass<8, CT>(a.g, a.bt, a.st, sl[q], mode, rd, wr, a.stride, pres, sm[0]);
+                __syncthreads();
+            });
+        } else {
+            const int h = threadIdx.x >> 8, lt = threadIdx.x & 255;
+            for (int q = 2 * blockIdx.x + h; q < n; q += 2 * gridDim.x) {
+                op_relax_pass_half<8, CT>(a.g, a.bt, a.st, sl[q], mode, rd, wr, a.stride, pres, sm[h], lt, 1 + h);
+                named_sync(1 + h, 256);
+            }
+        }
+    }
+
     __device__ const int* level(int l) const { return a.L.slots + a.L.off[l]; }
 
     // enforce_phi_boundaries of one level: faces, then edges (reading the
@@ -121,12 +140,13 @@ struct Solver {
             if (t < 384) op_phi_faces(a.g, a.bt, a.st, a.aux, sl[q], t / 64, t % 64, 64);
         });
         if (!sync(PH_PHI_FACES)) return false;
+        const int m = a.g.pnx - 2;
         each(n, [&](int q) {
-            if (t < a.g.pnx - 2) op_phi_edges(a.g, a.bt, a.st, a.aux, sl[q], t + 1);
+            if (t < 12 * m) op_phi_edge(a.g, a.bt, a.st, a.aux, sl[q], t / m, t % m + 1);
         });
         if (!sync(PH_PHI_EDGES)) return false;
         each(n, [&](int q) {
-            if (t == 0) op_phi_vertices(a.g, a.bt, a.st, a.aux, sl[q]);
+            if (t < 8) op_phi_vertex(a.g, a.bt, a.st, a.aux, sl[q], t);
         });
         return sync(PH_PHI_VERTICES);
     }
@@ -136,6 +156,7 @@ struct Solver {
     __device__ double level_sum(int l, const double* buf) {
         if (l == 0) return __ldcg(buf + a.L.slots[a.L.off[0]]);
         __syncthreads();
+        if (a.L.max_cnt <= NEST_SMEM) return nested_sum_smem(a.L, buf, l, false, nbuf);
         return nested_sum_block(a.L, a.bt.child, buf, nest, l, false);
     }
 
@@ -153,10 +174,7 @@ struct Solver {
         if (!sync(PH_DPHI_FACES)) return false;
         int par = 0;
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
-        each(n, [&](int q) {
-            op_relax_pass<8, CT>(a.g, a.bt, a.st, sl[q], 0, snap, snap, a.stride, pres, sm);
-            __syncthreads();
-        });
+        relax_pass(sl, n, 0, snap, snap, pres);
         if (!sync(PH_RELAX_FIRST)) return false;
         const double r0 = level_sum(l, pres);
         relax_par ^= 1;
@@ -166,10 +184,7 @@ struct Solver {
             pres = a.pres + (size_t)relax_par * a.L.cap;
             const CT* rd = snap + (size_t)par * a.snap_half;
             CT* wr = snap + (size_t)(par ^ 1) * a.snap_half;
-            each(n, [&](int q) {
-                op_relax_pass<8, CT>(a.g, a.bt, a.st, sl[q], 1, rd, wr, a.stride, pres, sm);
-                __syncthreads();
-            });
+            relax_pass(sl, n, 1, rd, wr, pres);
             if (!sync(PH_RELAX)) return false;
             par ^= 1;
             const double r = level_sum(l, pres);
@@ -251,6 +266,10 @@ struct Solver {
             __syncthreads();
         });
         if (!sync(PH_ERROR)) return false;
+        if (a.L.max_cnt <= NEST_SMEM) {
+            *err = nested_sum_smem(a.L, perr, nl - 1, true, nbuf);
+            return true;
+        }
         // deepest level: nest = own; then own + children level by level
         const int* sl = a.L.slots + a.L.off[nl - 1];
         for (int q = threadIdx.x; q < a.L.cnt[nl - 1]; q += blockDim.x) nest[sl[q]] = __ldcg(perr + sl[q]);
@@ -262,13 +281,15 @@ struct Solver {
 
 template <typename CT>
 __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
-    __shared__ RelaxSmem<8, CT> sm;
+    __shared__ RelaxSmem<8, CT> sm[2];
     __shared__ double red[16];
+    __shared__ double nbuf[2 * NEST_SMEM];
     __shared__ double s_err;
     // loop limits are read from the control block (set by the host before
     // every launch; a captured graph keeps its arguments)
     const int max_cycles = *(volatile int*)&a.ctl->max_cycles;
-    Solver<CT> s{a, sm, red, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0, *(volatile int*)&a.ctl->max_outer};
+    Solver<CT> s{a, sm, red, nbuf, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0,
+                 *(volatile int*)&a.ctl->max_outer};
     s.t_last = Solver<CT>::now();
     for (int p = 0; p < PH_COUNT; p++) {
         s.ph_ns[p] = 0;

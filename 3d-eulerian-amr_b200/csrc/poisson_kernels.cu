@@ -187,12 +187,15 @@ template <typename CT>
 __global__ void k_dphi_faces(Geom g, BrickTable bt, DevState st, PoissonAux aux, const int* __restrict__ slots) {
     op_dphi_faces<CT>(g, bt, st, aux, slots[blockIdx.x], blockIdx.y, threadIdx.x, blockDim.x);
 }
+// thread = (edge, position along it)
 __global__ void k_phi_edges(Geom g, BrickTable bt, DevState st, PoissonAux aux, const int* __restrict__ slots) {
-    const int k = threadIdx.x + 1;
-    if (k <= g.pnx - 2) op_phi_edges(g, bt, st, aux, slots[blockIdx.x], k);
+    const int m = g.pnx - 2;
+    const int t = threadIdx.x;
+    if (t < 12 * m) op_phi_edge(g, bt, st, aux, slots[blockIdx.x], t / m, t % m + 1);
 }
+// thread = vertex
 __global__ void k_phi_vertices(Geom g, BrickTable bt, DevState st, PoissonAux aux, const int* __restrict__ slots) {
-    if (threadIdx.x == 0) op_phi_vertices(g, bt, st, aux, slots[blockIdx.x]);
+    if (threadIdx.x < 8) op_phi_vertex(g, bt, st, aux, slots[blockIdx.x], threadIdx.x);
 }
 __global__ void k_phi_from_children(Geom g, BrickTable bt, DevState st, const int* __restrict__ slots) {
     op_phi_from_children(g, bt, st, slots[blockIdx.x], blockIdx.y, threadIdx.x);
@@ -270,7 +273,7 @@ void launch_phi_boundaries(const Geom& g, const BrickTable& bt, const DevState& 
     if (n <= 0) return;
     PoissonAux aux{bphi, err};
     launch_k(k_phi_faces, dim3(n, 6), 64, 0, s, g, bt, st, aux, slots);
-    launch_k(k_phi_edges, n, g.pnx - 2, 0, s, g, bt, st, aux, slots);
+    launch_k(k_phi_edges, n, ((12 * (g.pnx - 2) + 31) / 32) * 32, 0, s, g, bt, st, aux, slots);
     launch_k(k_phi_vertices, n, 32, 0, s, g, bt, st, aux, slots);
 }
 void launch_dphi_boundaries(const Geom& g, const BrickTable& bt, const DevState& st, const double* bphi, int* err,

@@ -286,97 +286,76 @@ __device__ __forceinline__ void op_dphi_faces(const Geom& g, const BrickTable& b
 }
 
 // edges: Poisson::enforce_phi_boundaries_edge (poisson.cpp:788-842).
-// k = 1 .. PNX-2: the twelve edge cells at that position along the edges
-__device__ __forceinline__ void op_phi_edges(const Geom& g, const BrickTable& bt, const DevState& st,
-                                             const PoissonAux& aux, int b, int k) {
+// edge e (0..11) at position k = 1 .. PNX-2 along it; the source face is
+// the x face pair when one of them is physical, else the y or z face, as in
+// the reference.  Edges read face ghosts only (this level's faces are
+// complete), so all edge cells are independent.
+__device__ __forceinline__ void op_phi_edge(const Geom& g, const BrickTable& bt, const DevState& st,
+                                            const PoissonAux& aux, int b, int e, int k) {
     const int pnx = g.pnx, N = pnx - 1, M = pnx - 2;
-    double* phi = st.phi + (size_t)b * g.pnx3;
     auto phys = [&](int f) { const int t = bt.ftype[6 * b + f]; return t == FACE_OUTFLOW || t == FACE_REFLECT; };
-    auto gp = [&](int f, int i, int j, int kk) { return get_phi_from(g, bt, st, aux, b, f, i, j, kk); };
-    double v[12];
-    if (phys(XL) || phys(XU)) {
-        v[0] = gp(XL, M, 0, k);
-        v[1] = gp(XL, M, N, k);
-        v[2] = gp(XL, M, k, 0);
-        v[3] = gp(XL, M, k, N);
-        v[4] = gp(XU, 1, 0, k);
-        v[5] = gp(XU, 1, N, k);
-        v[6] = gp(XU, 1, k, 0);
-        v[7] = gp(XU, 1, k, N);
+    int f, i, j, kk, di, dj, dk;  // source face and cell; destination cell
+    if (e < 8) {
+        const int x = e < 4 ? 0 : N, r = e & 3;
+        di = x;
+        dj = r == 0 ? 0 : (r == 1 ? N : k);
+        dk = r < 2 ? k : (r == 2 ? 0 : N);
+        if (phys(XL) || phys(XU)) {
+            f = e < 4 ? XL : XU;
+            i = e < 4 ? M : 1;
+            j = dj;
+            kk = dk;
+        } else if (r < 2) {
+            f = r == 0 ? YL : YU;
+            i = x;
+            j = r == 0 ? M : 1;
+            kk = k;
+        } else {
+            f = r == 2 ? ZL : ZU;
+            i = x;
+            j = k;
+            kk = r == 2 ? M : 1;
+        }
     } else {
-        v[0] = gp(YL, 0, M, k);
-        v[4] = gp(YL, N, M, k);
-        v[1] = gp(YU, 0, 1, k);
-        v[5] = gp(YU, N, 1, k);
-        v[2] = gp(ZL, 0, k, M);
-        v[6] = gp(ZL, N, k, M);
-        v[3] = gp(ZU, 0, k, 1);
-        v[7] = gp(ZU, N, k, 1);
+        const int r = e - 8;
+        di = k;
+        dj = (r >> 1) ? N : 0;
+        dk = (r & 1) ? N : 0;
+        if (phys(YL) || phys(YU)) {
+            f = r < 2 ? YL : YU;
+            i = k;
+            j = r < 2 ? M : 1;
+            kk = dk;
+        } else {
+            f = (r & 1) ? ZU : ZL;
+            i = k;
+            j = dj;
+            kk = (r & 1) ? 1 : M;
+        }
     }
-    if (phys(YL) || phys(YU)) {
-        v[8] = gp(YL, k, M, 0);
-        v[9] = gp(YL, k, M, N);
-        v[10] = gp(YU, k, 1, 0);
-        v[11] = gp(YU, k, 1, N);
-    } else {
-        v[8] = gp(ZL, k, 0, M);
-        v[10] = gp(ZL, k, N, M);
-        v[9] = gp(ZU, k, 0, 1);
-        v[11] = gp(ZU, k, N, 1);
-    }
-    // edges read face ghosts only (this level's faces are complete)
-    phi[pidx(pnx, 0, 0, k)] = v[0];
-    phi[pidx(pnx, 0, N, k)] = v[1];
-    phi[pidx(pnx, 0, k, 0)] = v[2];
-    phi[pidx(pnx, 0, k, N)] = v[3];
-    phi[pidx(pnx, N, 0, k)] = v[4];
-    phi[pidx(pnx, N, N, k)] = v[5];
-    phi[pidx(pnx, N, k, 0)] = v[6];
-    phi[pidx(pnx, N, k, N)] = v[7];
-    phi[pidx(pnx, k, 0, 0)] = v[8];
-    phi[pidx(pnx, k, 0, N)] = v[9];
-    phi[pidx(pnx, k, N, 0)] = v[10];
-    phi[pidx(pnx, k, N, N)] = v[11];
+    st.phi[(size_t)b * g.pnx3 + pidx(pnx, di, dj, dk)] = get_phi_from(g, bt, st, aux, b, f, i, j, kk);
 }
 
 // vertices: Poisson::enforce_phi_boundaries_vertex (poisson.cpp:844-888).
-// one thread: the eight vertex cells
-__device__ __forceinline__ void op_phi_vertices(const Geom& g, const BrickTable& bt, const DevState& st,
-                                                const PoissonAux& aux, int b) {
+// vertex c = x | y<<1 | z<<2; the source face is an x face when one of them
+// is physical, else a y face when one of them is, else a z face.
+__device__ __forceinline__ void op_phi_vertex(const Geom& g, const BrickTable& bt, const DevState& st,
+                                              const PoissonAux& aux, int b, int c) {
     const int pnx = g.pnx, N = pnx - 1, M = pnx - 2;
-    double* phi = st.phi + (size_t)b * g.pnx3;
     auto phys = [&](int f) { const int t = bt.ftype[6 * b + f]; return t == FACE_OUTFLOW || t == FACE_REFLECT; };
-    auto gp = [&](int f, int i, int j, int kk) { return get_phi_from(g, bt, st, aux, b, f, i, j, kk); };
-    double v[8];  // index = x | y<<1 | z<<2 of the corner
+    const int x = c & 1, y = (c >> 1) & 1, z = (c >> 2) & 1;
+    int f, i = x * N, j = y * N, k = z * N;
     if (phys(XL) || phys(XU)) {
-        v[0] = gp(XL, M, 0, 0);
-        v[2] = gp(XL, M, N, 0);
-        v[4] = gp(XL, M, 0, N);
-        v[6] = gp(XL, M, N, N);
-        v[1] = gp(XU, 1, 0, 0);
-        v[3] = gp(XU, 1, N, 0);
-        v[5] = gp(XU, 1, 0, N);
-        v[7] = gp(XU, 1, N, N);
+        f = x ? XU : XL;
+        i = x ? 1 : M;
     } else if (phys(YL) || phys(YU)) {
-        v[0] = gp(YL, 0, M, 0);
-        v[1] = gp(YL, N, M, 0);
-        v[4] = gp(YL, 0, M, N);
-        v[5] = gp(YL, N, M, N);
-        v[2] = gp(YU, 0, 1, 0);
-        v[3] = gp(YU, N, 1, 0);
-        v[6] = gp(YU, 0, 1, N);
-        v[7] = gp(YU, N, 1, N);
+        f = y ? YU : YL;
+        j = y ? 1 : M;
     } else {
-        v[0] = gp(ZL, 0, 0, M);
-        v[2] = gp(ZL, 0, N, M);
-        v[1] = gp(ZL, N, 0, M);
-        v[3] = gp(ZL, N, N, M);
-        v[4] = gp(ZU, 0, 0, 1);
-        v[6] = gp(ZU, 0, N, 1);
-        v[5] = gp(ZU, N, 0, 1);
-        v[7] = gp(ZU, N, N, 1);
+        f = z ? ZU : ZL;
+        k = z ? 1 : M;
     }
-    for (int c = 0; c < 8; c++) phi[pidx(pnx, (c & 1) * N, ((c >> 1) & 1) * N, ((c >> 2) & 1) * N)] = v[c];
+    st.phi[(size_t)b * g.pnx3 + pidx(pnx, x * N, y * N, z * N)] = get_phi_from(g, bt, st, aux, b, f, i, j, k);
 }
 
 // ---------------------------------------------------------------------------
