@@ -86,6 +86,7 @@ def load_library(path=LIB_PATH):
         lib.amr_check_for_refine.argtypes = [P, D, I, ip]
         lib.amr_state_max.argtypes = [P, I, dp]
         lib.amr_sub_step.argtypes = [P, D, D]
+        lib.amr_fused_sub_step.argtypes = [P, D, D, I]
         lib.amr_hydro_step.argtypes = [P, D, D]
         lib.amr_get_stream.argtypes = [P, ctypes.POINTER(ctypes.c_void_p)]
         lib.amr_profile_enable.argtypes = [P, I]
@@ -102,7 +103,8 @@ def load_library(path=LIB_PATH):
             lib.amr_graph_solve.argtypes = [P, D, I, dp, ip]
             lib.amr_graph_grav_step.argtypes = [P, D, D, I, dp]
         if hasattr(lib, "amr_solve_phases"):
-            lib.amr_solve_phases.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong), I]
+            lib.amr_solve_phases.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong), dp, I]
+            lib.amr_solve_last_ms.argtypes = [P, ctypes.POINTER(ctypes.c_float)]
         _lib = lib
     return _lib
 
@@ -272,6 +274,9 @@ class AMR:
     def sub_step(self, dt, beta):
         self._check(self.lib.amr_sub_step(self.ctx, float(dt), float(beta)))
 
+    def fused_sub_step(self, dt, beta, blocks_per_sm=0):
+        self._check(self.lib.amr_fused_sub_step(self.ctx, float(dt), float(beta), int(blocks_per_sm)))
+
     def hydro_step(self, dt, min_refine_density):
         self._check(self.lib.amr_hydro_step(self.ctx, float(dt), float(min_refine_density)))
 
@@ -289,7 +294,7 @@ class AMR:
 
     def profile_get(self):
         out = {}
-        for cls in range(19):
+        for cls in range(20):
             ms = ctypes.c_double()
             n = ctypes.c_longlong()
             name = ctypes.c_char_p()
@@ -346,8 +351,14 @@ class AMR:
         n = len(self.SOLVE_PHASES)
         ms = (ctypes.c_double * n)()
         cnt = (ctypes.c_longlong * n)()
-        self._check(self.lib.amr_solve_phases(self.ctx, ms, cnt, n))
-        return {k: {"ms": ms[i], "count": cnt[i]} for i, k in enumerate(self.SOLVE_PHASES)}
+        by = (ctypes.c_double * n)()
+        self._check(self.lib.amr_solve_phases(self.ctx, ms, cnt, by, n))
+        return {k: {"ms": ms[i], "count": cnt[i], "bytes": by[i]} for i, k in enumerate(self.SOLVE_PHASES)}
+
+    def solve_last_ms(self):
+        v = ctypes.c_float()
+        self._check(self.lib.amr_solve_last_ms(self.ctx, ctypes.byref(v)))
+        return v.value
 
     def graph_grav_step(self, tol, dynamic_range=1.0e6, step_index=0):
         dt = ctypes.c_double()

@@ -48,6 +48,7 @@ struct Control {
     // seen by block 0, and the number of such phases
     unsigned long long phase_ns[16];
     unsigned long long phase_n[16];
+    double phase_bytes[16];  // algorithmic HBM bytes of those phases
 };
 
 // phase classes of the persistent solve

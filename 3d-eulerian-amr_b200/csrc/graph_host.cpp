@@ -68,6 +68,7 @@ struct GraphState {
     double* d_pres3 = nullptr;
     double* d_pnest = nullptr;
     GridBarrier* d_bar = nullptr;
+    cudaEvent_t ev_ps[2] = {nullptr, nullptr};  // around the last persistent launch
     long long rec_in_bodies = 0;  // kernels recorded inside outermost WHILE bodies
     long long rec_nested = 0;     // kernels recorded inside the bodies of the body being recorded
     int while_depth = 0;
@@ -98,6 +99,8 @@ int ensure_state(amr_ctx* c) {
         CUDA_TRY(cudaMalloc(&g->d_pres3, sizeof(double) * 3 * (size_t)c->cap));
         CUDA_TRY(cudaMalloc(&g->d_pnest, sizeof(double) * (size_t)g->pblocks * c->cap));
         CUDA_TRY(cudaMalloc(&g->d_bar, sizeof(GridBarrier)));
+        CUDA_TRY(cudaEventCreate(&g->ev_ps[0]));
+        CUDA_TRY(cudaEventCreate(&g->ev_ps[1]));
     }
     // side streams for capturing nested loop bodies, created outside any capture
     for (int d = 0; d < 4; d++) {
@@ -295,7 +298,11 @@ int rec_persistent(amr_ctx* c, cudaStream_t s, double tol) {
     a.snap_half = SNAP_STRIDE * (size_t)c->cap;
     a.bar = g->d_bar;
     CUDA_TRY(cudaMemsetAsync(g->d_bar, 0, sizeof(GridBarrier), s));
+    // event nodes bracketing the launch: the elapsed time of the latest
+    // replay is the kernel's duration on this stream
+    CUDA_TRY(cudaEventRecordWithFlags(g->ev_ps[0], s, cudaEventRecordExternal));
     CUDA_TRY(launch_solve_persistent(a, g->pblocks, s));
+    CUDA_TRY(cudaEventRecordWithFlags(g->ev_ps[1], s, cudaEventRecordExternal));
     g->k_vbody = 0;
     g->k_rbody = 0;
     return launched(c, __LINE__);
@@ -478,6 +485,8 @@ void graph_release(amr_ctx* c) {
     if (g->d_pres3) cudaFree(g->d_pres3);
     if (g->d_pnest) cudaFree(g->d_pnest);
     if (g->d_bar) cudaFree(g->d_bar);
+    for (cudaEvent_t e : g->ev_ps)
+        if (e) cudaEventDestroy(e);
     delete g;
     c->gs = nullptr;
 }
@@ -487,17 +496,31 @@ extern "C" {
 
 // Device time per phase class of the persistent solve, accumulated over all
 // persistent solves of the context (ms[PH_COUNT], counts[PH_COUNT]).
-int amr_solve_phases(amr_ctx* c, double* ms, long long* counts, int n) {
-    if (!c || !ms || !counts || n < PH_COUNT) return AMR_ERR_ARG;
+int amr_solve_phases(amr_ctx* c, double* ms, long long* counts, double* bytes, int n) {
+    if (!c || !ms || !counts || !bytes || n < PH_COUNT) return AMR_ERR_ARG;
     if (!c->gs) {
-        for (int p = 0; p < PH_COUNT; p++) ms[p] = 0.0, counts[p] = 0;
+        for (int p = 0; p < PH_COUNT; p++) ms[p] = 0.0, counts[p] = 0, bytes[p] = 0.0;
         return AMR_OK;
     }
     TRY(read_ctl(c));
     for (int p = 0; p < PH_COUNT; p++) {
         ms[p] = c->gs->h_ctl->phase_ns[p] * 1e-6;
         counts[p] = (long long)c->gs->h_ctl->phase_n[p];
+        bytes[p] = c->gs->h_ctl->phase_bytes[p];
     }
+    return AMR_OK;
+}
+
+// Duration of the most recent persistent solve launch (CUDA events recorded
+// around it on the launching stream).
+int amr_solve_last_ms(amr_ctx* c, float* ms) {
+    if (!c || !ms) return AMR_ERR_ARG;
+    if (!c->gs || !c->gs->ev_ps[0]) {
+        c->err = "no persistent solve has run";
+        return AMR_ERR_STATE;
+    }
+    CUDA_TRY(cudaEventSynchronize(c->gs->ev_ps[1]));
+    CUDA_TRY(cudaEventElapsedTime(ms, c->gs->ev_ps[0], c->gs->ev_ps[1]));
     return AMR_OK;
 }
 

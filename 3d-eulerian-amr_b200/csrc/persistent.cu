@@ -85,6 +85,7 @@ struct Solver {
     unsigned long long t_last;  // block 0: global time at the last barrier exit
     unsigned long long ph_ns[PH_COUNT];
     unsigned ph_n[PH_COUNT];
+    double ph_bytes[PH_COUNT];
 
     __device__ static unsigned long long now() {
         unsigned long long t;
@@ -93,15 +94,41 @@ struct Solver {
     }
 
     // barrier closing a phase of class ph
-    __device__ bool sync(int ph) {
+    __device__ bool sync(int ph, int units) {
         const bool ok = grid_sync(a.bar);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             const unsigned long long t = now();
             ph_ns[ph] += t - t_last;
             ph_n[ph]++;
+            ph_bytes[ph] += (double)units * phase_bytes(ph);
             t_last = t;
         }
         return ok;
+    }
+
+    // Algorithmic HBM bytes of one unit (brick, parent or coarse-fine item)
+    // of a phase: the arrays the phase must read and write once, at their
+    // storage width (the correction dphi, dphi1 in CT).
+    __device__ static double phase_bytes(int ph) {
+        constexpr double NX = 8, PNX = 10, H = NX / 2, C = sizeof(CT);
+        switch (ph) {
+            case PH_SOURCE: return 16 * PNX * PNX * PNX;                                  // rho -> S
+            case PH_RESTRICT: return 8 * (8 * PNX * PNX * PNX + 8 * H * H * H);           // 8 children -> parent
+            case PH_PHI_FACES: return 16 * 6 * NX * NX;                                   // source cell -> ghost
+            case PH_PHI_EDGES: return 16 * 12 * NX;
+            case PH_PHI_VERTICES: return 16 * 8;
+            case PH_INIT: return 2 * C * PNX * PNX * PNX;                                 // dphi, dphi1 = 0
+            case PH_VDOWN: return 8 * (PNX * PNX * PNX + NX * NX * NX) + 2 * C * NX * NX * NX;  // phi, S -> dphi, dphi1
+            case PH_DPHI_FACES: return 2 * C * 6 * NX * NX;
+            case PH_RELAX_FIRST:
+            case PH_RELAX: return C * (PNX * PNX * PNX + 2 * NX * NX * NX + 12 * NX * NX);  // dphi, dphi1 -> dphi, layers
+            case PH_CORRECT: return C * (2 * NX * NX * NX + H * H * H);
+            case PH_RETIRE: return (16 + C) * NX * NX * NX;                               // phi += dphi
+            case PH_FORCES: return 8 * (PNX * PNX * PNX + 3 * (PNX - 1) * (PNX - 1) * (PNX - 1));
+            case PH_ADJUST_FORCE: return 8 * 5 * H * H;
+            case PH_ERROR: return 8 * (3 * PNX * PNX * PNX + NX * NX * NX) + C * NX * NX * NX;
+            default: return 0;
+        }
     }
 
     // this block's share of n items
@@ -139,16 +166,16 @@ struct Solver {
         each(n, [&](int q) {
             if (t < 384) op_phi_faces(a.g, a.bt, a.st, a.aux, sl[q], t / 64, t % 64, 64);
         });
-        if (!sync(PH_PHI_FACES)) return false;
+        if (!sync(PH_PHI_FACES, n)) return false;
         const int m = a.g.pnx - 2;
         each(n, [&](int q) {
             if (t < 12 * m) op_phi_edge(a.g, a.bt, a.st, a.aux, sl[q], t / m, t % m + 1);
         });
-        if (!sync(PH_PHI_EDGES)) return false;
+        if (!sync(PH_PHI_EDGES, n)) return false;
         each(n, [&](int q) {
             if (t < 8) op_phi_vertex(a.g, a.bt, a.st, a.aux, sl[q], t);
         });
-        return sync(PH_PHI_VERTICES);
+        return sync(PH_PHI_VERTICES, n);
     }
 
     // Poisson::vcycle_relax sum over level l (poisson.cpp:107, nested as the
@@ -171,11 +198,11 @@ struct Solver {
         each(n, [&](int q) {
             if (t < 384) op_dphi_faces<CT>(a.g, a.bt, a.st, a.aux, sl[q], t / 64, t % 64, 64);
         });
-        if (!sync(PH_DPHI_FACES)) return false;
+        if (!sync(PH_DPHI_FACES, n)) return false;
         int par = 0;
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
         relax_pass(sl, n, 0, snap, snap, pres);
-        if (!sync(PH_RELAX_FIRST)) return false;
+        if (!sync(PH_RELAX_FIRST, n)) return false;
         const double r0 = level_sum(l, pres);
         relax_par ^= 1;
         relax_calls++;
@@ -185,7 +212,7 @@ struct Solver {
             const CT* rd = snap + (size_t)par * a.snap_half;
             CT* wr = snap + (size_t)(par ^ 1) * a.snap_half;
             relax_pass(sl, n, 1, rd, wr, pres);
-            if (!sync(PH_RELAX)) return false;
+            if (!sync(PH_RELAX, n)) return false;
             par ^= 1;
             const double r = level_sum(l, pres);
             relax_par ^= 1;
@@ -208,34 +235,34 @@ struct Solver {
         const int t = threadIdx.x;
         const int maxl = a.nlevels - 1;
         each(a.L.nall, [&](int q) { op_set_source(a.g, a.st, a.L.all[q], t, blockDim.x); });
-        if (!sync(PH_SOURCE)) return false;
+        if (!sync(PH_SOURCE, a.L.nall)) return false;
         for (int l = maxl - 1; l >= 0; l--) {
             const int* pl = a.parents + a.poff[l];
             each(a.pcnt[l], [&](int q) { op_phi_from_children(a.g, a.bt, a.st, pl[q], t / 64, t % 64); });
-            if (!sync(PH_RESTRICT)) return false;
+            if (!sync(PH_RESTRICT, a.pcnt[l])) return false;
         }
         for (int l = 0; l <= maxl; l++)
             if (!phi_boundaries(l)) return false;
         each(a.L.nall, [&](int q) { op_init_vcycle<CT>(a.g, a.st, a.L.all[q], t, blockDim.x); });
-        if (!sync(PH_INIT)) return false;
+        if (!sync(PH_INIT, a.L.nall)) return false;
         for (int l = maxl; l >= 0; l--) {
             const int* sl = level(l);
             each(a.L.cnt[l], [&](int q) {
                 op_vdown<CT>(a.g, a.bt, a.st, sl[q], a.vitems, a.vranges + 4 * (a.voff[l] + q));
                 __syncthreads();
             });
-            if (!sync(PH_VDOWN)) return false;
+            if (!sync(PH_VDOWN, a.L.cnt[l])) return false;
             if (!relax_until(l, 1.0)) return false;
         }
         for (int l = 0; l <= maxl; l++) {
             const int* sl = level(l);
             if (l > 0) {
                 each(a.L.cnt[l], [&](int q) { op_coarse_correction<CT>(a.g, a.bt, a.st, sl[q], t); });
-                if (!sync(PH_CORRECT)) return false;
+                if (!sync(PH_CORRECT, a.L.cnt[l])) return false;
             }
             if (!relax_until(l, 0.05)) return false;
             each(a.L.cnt[l], [&](int q) { op_retire<CT>(a.g, a.st, sl[q], t, blockDim.x); });
-            if (!sync(PH_RETIRE)) return false;
+            if (!sync(PH_RETIRE, a.L.cnt[l])) return false;
             if (!phi_boundaries(l)) return false;
         }
         return true;
@@ -245,13 +272,13 @@ struct Solver {
     __device__ bool forces() {
         const int t = threadIdx.x;
         each(a.L.nall, [&](int q) { op_forces(a.g, a.bt, a.st, a.L.all[q], t, blockDim.x); });
-        if (!sync(PH_FORCES)) return false;
+        if (!sync(PH_FORCES, a.L.nall)) return false;
         for (int l = a.force_levels - 1; l >= 0; l--) {
             const int n = a.foff[l + 1] - a.foff[l];
             if (n <= 0) continue;
             const RefluxItem* it = a.fitems + a.foff[l];
             each(n, [&](int q) { op_adjust_force(a.g, a.st, it[q], t); });
-            if (!sync(PH_ADJUST_FORCE)) return false;
+            if (!sync(PH_ADJUST_FORCE, n)) return false;
         }
         return true;
     }
@@ -265,7 +292,7 @@ struct Solver {
             op_solution_error<CT>(a.g, a.bt, a.st, a.L.all[q], perr, red, 256);
             __syncthreads();
         });
-        if (!sync(PH_ERROR)) return false;
+        if (!sync(PH_ERROR, a.L.nall)) return false;
         if (a.L.max_cnt <= NEST_SMEM) {
             *err = nested_sum_smem(a.L, perr, nl - 1, true, nbuf);
             return true;
@@ -294,6 +321,7 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
     for (int p = 0; p < PH_COUNT; p++) {
         s.ph_ns[p] = 0;
         s.ph_n[p] = 0;
+        s.ph_bytes[p] = 0.0;
     }
     int cycles = 0;
     bool ok = true;
@@ -325,6 +353,7 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
             for (int p = 0; p < PH_COUNT; p++) {
                 c->phase_ns[p] += s.ph_ns[p];
                 c->phase_n[p] += s.ph_n[p];
+                c->phase_bytes[p] += s.ph_bytes[p];
             }
         }
     }

@@ -216,6 +216,9 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
         one_step()
     res = {"form": form}
     st0 = a.stats()
+    persistent = form in ("persistent", "mixed")
+    ph0 = a.solve_phases() if persistent else None
+    solve_ms = []
     k0 = a.launch_count()
     sampler = ClockSampler(local)
     barrier()
@@ -234,11 +237,22 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
         torch.cuda.nvtx.range_pop()
         ev1.synchronize()
         times.append(ev0.elapsed_time(ev1))
+        if persistent:
+            solve_ms.append(a.solve_last_ms())  # the step's last persistent solve kernel
         cells += n_cells
     barrier()
     res["clocks"] = sampler.stop()
     st1 = a.stats()
     res["gpu_launches"] = a.launch_count() - k0
+    if persistent:
+        ph1 = a.solve_phases()
+        d = {k: {"ms": ph1[k]["ms"] - ph0[k]["ms"], "count": ph1[k]["count"] - ph0[k]["count"],
+                 "bytes": ph1[k]["bytes"] - ph0[k]["bytes"]} for k in ph1}
+        launches = 3 * args.steps  # one persistent solve per RK substep
+        res["persistent"] = {"ms_per_launch": statistics.mean(solve_ms),
+                             "bytes_per_launch": sum(v["bytes"] for v in d.values()) / launches,
+                             "phase_ms_per_step": {k: round(v["ms"] / args.steps, 4) for k, v in d.items()},
+                             "phases_per_step": {k: v["count"] / args.steps for k, v in d.items()}}
     # state after warm-up + timed steps, for the error of one form against another
     res["final"] = {"U": a.download_state(), "phi": a.download_poisson()[0], "level": a.get_tree()["level"],
                     "loc": a.get_tree()["loc"]}
@@ -469,6 +483,116 @@ def poisson_precision_check(amr, ini, rel_tol=1e-10):
     return out
 
 
+FUSED_BYTES_PER_BRICK = 8 * NF * 3 * NX ** 3  # read U, U0, write U (interiors), FP64
+
+
+def run_batched_substep(amr, ini, torch, steps, warmup, levels=5):
+    """Uneven-brick KT substep on the synthetic random-field octree: one
+    persistent fused launch per substep (ghost zones, limiter, flux,
+    coarse-fine correction, RK combination), FP64 and FP32 flux, against the
+    one-launch-per-step substep; an autotuning pass over the resident blocks
+    per SM."""
+    F = ini.random_field()
+    thr = float(np.percentile(F, 90))
+    out = {"levels": levels + 1, "threshold": "90th percentile of the density field", "seed": 20261203}
+    ctxs = {}
+    for name, prec in (("fp64", amr.PREC_FP64), ("fp32_flux", amr.PREC_MIXED)):
+        a = amr.AMR(physics=amr.PHYSICS_EULER, max_refine_level=levels, grid_dim=0.5, z_reflect=0,
+                    max_bricks=40000, precision=prec)
+        t0 = time.time()
+        t, _ = ini.build_tree(a, "random", thr, 0.5, 0, levels, device=True)
+        out.setdefault("build_s", round(time.time() - t0, 1))
+        out["bricks"] = a.nbricks
+        out["per_level"] = np.bincount(t["level"]).tolist()
+        out["leaf_cells"] = int(a.get_zone_cnt())
+        ctxs[name] = a
+    a64 = ctxs["fp64"]
+    dt = a64.max_dt()
+    stream = torch.cuda.ExternalStream(a64.stream_handle())
+
+    def time_substeps(a, fn, k):
+        for _ in range(warmup):
+            fn(a)
+        ts = []
+        for _ in range(k):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn(a)
+            e1.record(stream)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return statistics.median(ts)
+
+    # one-launch-per-step substep (ghost fill by level, flux, reflux, update)
+    a64.store()
+    plain_ms = time_substeps(a64, lambda a: a.sub_step(dt, 0.25), steps)
+    # autotune the fused launch: resident blocks per SM
+    tune = {}
+    for bps in (1, 2, 0):
+        tune[bps] = time_substeps(a64, lambda a: a.fused_sub_step(dt, 0.25, bps), steps)
+    best = min(tune, key=tune.get)
+    # fused kernel alone (profiled class: CUDA events around the launch)
+    a64.profile(True)
+    a64.profile_reset()
+    for _ in range(steps):
+        a64.fused_sub_step(dt, 0.25, best)
+    a64.synchronize()
+    pr = a64.profile_get()["fused_substep"]
+    a64.profile(False)
+    kms = pr["ms"] / pr["launches"]
+    nb = out["bricks"]
+    peak, peak_kind = peaks()
+    achieved = FUSED_BYTES_PER_BRICK * nb / (kms * 1e-3) / 1e9
+    # FP32 flux: speed and error against FP64 after one substep from the same state
+    a32 = ctxs["fp32_flux"]
+    a32.store()
+    f32_ms = time_substeps(a32, lambda a: a.fused_sub_step(dt, 0.25, best), steps)
+    errs = {}
+    b64, b32 = a64, a32
+    U0 = b64.download_state()
+    b32.upload_state(U0)
+    b32.store()
+    b64.store()
+    b64.fused_sub_step(dt, 1.0, best)
+    b32.fused_sub_step(dt, 1.0, best)
+    u64 = b64.download_state()[:, :, 2:-2, 2:-2, 2:-2]
+    u32 = b32.download_state()[:, :, 2:-2, 2:-2, 2:-2]
+    for f, nm in enumerate(("rho", "sx", "sy", "sz", "et", "tau")):
+        errs[nm] = float(np.abs(u32[:, f] - u64[:, f]).sum() / max(np.abs(u64[:, f]).sum(), 1e-300))
+    cells = nb * NX ** 3
+    out.update({
+        "dt": dt, "plain_substep_ms": plain_ms, "fused_substep_ms": tune[best], "fused_fp32_flux_substep_ms": f32_ms,
+        "speedup_vs_plain": plain_ms / tune[best],
+        "brick_cell_updates_per_s": cells / (tune[best] * 1e-3),
+        "leaf_cell_updates_per_s": out["leaf_cells"] / (tune[best] * 1e-3),
+        "autotune_ms_by_blocks_per_sm": {str(k): v for k, v in tune.items()}, "autotune_best": best,
+        "roofline": {"bound": "hbm", "kernel": "k_substep_fused", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": FUSED_BYTES_PER_BRICK * nb, "ms_per_launch": kms},
+        "fp32_flux_rel_l1_vs_fp64": errs,
+        "l2": "state (%.1f GB with the RK store) larger than L2, no flush" % (2 * nb * NF * (NX + 4) ** 3 * 8 / 1e9),
+    })
+    for a in ctxs.values():
+        a.close()
+    return out
+
+
+def roofline_persistent(res):
+    """Roofline of the persistent solve kernel, the step's dominant kernel:
+    algorithmic bytes per launch (the arrays each phase must read and write
+    once, summed by the kernel over its phases) over the launch's duration
+    from CUDA events on the launching stream."""
+    p = res["persistent"]
+    peak, peak_kind = peaks()
+    achieved = p["bytes_per_launch"] / (p["ms_per_launch"] * 1e-3) / 1e9
+    return {"bound": "hbm", "kernel": "k_solve_persistent", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+            "algorithmic_bytes_per_launch": p["bytes_per_launch"], "ms_per_launch": p["ms_per_launch"],
+            "phase_ms_per_step": p["phase_ms_per_step"], "phases_per_step": p["phases_per_step"],
+            "note": "latency-bound: the reference's V-cycle is a chain of dependent per-level steps "
+                    "(about 700 grid barriers per step here); the relaxation sweeps run in shared memory"}
+
+
 def roofline_of(prof):
     known = {k: v for k, v in prof.items() if k in BYTES_PER_BRICK and v["launches"] > 0}
     dom = max(prof.items(), key=lambda kv: kv[1]["ms"])[0]
@@ -502,6 +626,7 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
     ap.add_argument("--json-out", default=None)
     ap.add_argument("--no-eos", action="store_true", help="skip the Helmholtz EOS throughput section")
+    ap.add_argument("--no-batched", action="store_true", help="skip the random-field octree substep section")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -542,6 +667,9 @@ def main():
                    "sample": "reference CPU code (oracle/_ref): one full RK3 step of this workload after one "
                              "untimed step (which solves from phi = 0), %d bricks, %d V-cycles" %
                              (s["bricks"], s["vcycles"][0])}
+    batched = None
+    if rank == 0 and not args.no_batched:
+        batched = run_batched_substep(amr, ini, torch, max(args.steps, 3), max(args.warmup, 3))
     eos = None
     if rank == 0 and not args.no_eos:
         eos = run_eos(torch, max(args.steps, 3), max(args.warmup, 3), not args.no_cpu_baseline)
@@ -555,7 +683,8 @@ def main():
             "config": {"workload": WORKLOAD, "form": args.form, "levels": LEVELS, "bricks": head["bricks"],
                        "leaf_cells_per_step": head["cells"] / args.steps / world, "tol_l1": TOL,
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"},
-            "roofline": roofline_of(head["profile"]), "cpu_baseline": cpu, "e2e": head.get("e2e"),
+            "roofline": roofline_persistent(head) if "persistent" in head else roofline_of(head["profile"]),
+            "class_roofline": roofline_of(head["profile"]), "cpu_baseline": cpu, "e2e": head.get("e2e"),
             "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
             "relax_calls_per_step": head["relax_calls_per_step"],
             "fp64_plain": None if plain is None else {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
@@ -569,6 +698,7 @@ def main():
             "errors_vs_fp64": errors,
             "poisson_precision": pcheck,
             "helmholtz_eos": eos,
+            "batched_substep": batched,
         }
         line = json.dumps(out)
         print(line)

@@ -138,6 +138,15 @@ int amr_state_max(amr_ctx* ctx, int field, double* vmax);
 /* ---- driver sequences ----------------------------------------------------- */
 /* HydroDriver::sub_step (euler/hydro_driver.cpp:200-214). */
 int amr_sub_step(amr_ctx* ctx, double dt, double beta);
+/* amr_sub_step (Euler physics without gravity) as one persistent launch:
+ * ghost zones computed where needed, fluxes (FP32 in the mixed form),
+ * coarse-fine corrections and the RK combination per brick, finest level
+ * first; the result goes to a second state array that then becomes the
+ * state.  Interiors are bitwise those of amr_sub_step in the FP64 form; the
+ * new state's ghost zones are not filled (amr_enforce_boundaries fills
+ * them).  blocks_per_sm > 0 caps the resident blocks per SM (0: as many as
+ * fit). */
+int amr_fused_sub_step(amr_ctx* ctx, double dt, double beta, int blocks_per_sm);
 /* HydroDriver::step (euler/hydro_driver.cpp:171-194): store, RK3 substeps
  * with restriction, boundaries, regrid (min_refine_density), time += dt. */
 int amr_hydro_step(amr_ctx* ctx, double dt, double min_refine_density);
@@ -182,18 +191,23 @@ int amr_graph_grav_step(amr_ctx* ctx, double tol, double dynamic_range, int step
 /* ---- instrumentation ------------------------------------------------------
  * The reference times steps with omp_get_wtime (binary_driver.cpp:115,303);
  * here device time per kernel class comes from CUDA events on the context
- * stream.  Classes 0..18: ghost_fill flux reflux add_difs inject max_dt
+ * stream.  Classes 0..19: ghost_fill flux reflux add_difs inject max_dt
  * refine_flags prolong relax vcycle_down phi_boundaries dphi_boundaries
- * forces solution_error source phys_boundary coarse_correction phi_time other.
+ * forces solution_error source phys_boundary coarse_correction phi_time other
+ * fused_substep.
  */
 int amr_get_stream(amr_ctx* ctx, void** stream);  /* the context's cudaStream_t */
-/* Persistent solve (persistent_solve = 1): device time and count per phase
- * class, summed over the context's persistent solves; n >= 15.  Classes:
- * source restrict phi_faces phi_edges phi_vertices init vcycle_down
- * dphi_faces relax_first relax coarse_correction retire forces
- * adjust_force error.  A phase's time runs from one grid barrier's exit to
- * the next as block 0 sees it (slowest block's work + the barrier). */
-int amr_solve_phases(amr_ctx* ctx, double* ms, long long* counts, int n);
+/* Persistent solve (persistent_solve = 1): device time, count and
+ * algorithmic HBM bytes per phase class, summed over the context's
+ * persistent solves; n >= 15.  Classes: source restrict phi_faces phi_edges
+ * phi_vertices init vcycle_down dphi_faces relax_first relax
+ * coarse_correction retire forces adjust_force error.  A phase's time runs
+ * from one grid barrier's exit to the next as block 0 sees it (slowest
+ * block's work + the barrier). */
+int amr_solve_phases(amr_ctx* ctx, double* ms, long long* counts, double* bytes, int n);
+/* Duration (CUDA events on the launching stream) of the most recent
+ * persistent solve kernel. */
+int amr_solve_last_ms(amr_ctx* ctx, float* ms);
 int amr_profile_enable(amr_ctx* ctx, int on);
 int amr_profile_reset(amr_ctx* ctx);
 int amr_profile_get(amr_ctx* ctx, int cls, double* ms, long long* launches, const char** name);
