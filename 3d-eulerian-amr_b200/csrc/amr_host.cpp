@@ -13,6 +13,7 @@
 #include "profiler.h"
 #include "kernels.h"
 #include "poisson.h"
+#include "hydro_fused.h"
 
 using namespace amr;
 
@@ -578,6 +579,7 @@ int amr_destroy(amr_ctx* c) {
                         c->st.fz,   c->bt.level, c->bt.off,   c->bt.h,      c->bt.ftype,   c->bt.fnbr,
                         c->bt.parent, c->bt.cidx, c->bt.child, c->d_fo,     c->d_dt,       c->d_red,
                         c->d_flags, c->d_stage, c->d_slots,  c->d_reflux, c->d_vitems, c->d_vranges, c->d_cpos,
+                        c->d_U1, c->d_fwork, c->d_pubmask, c->d_pub, c->d_fdone, c->d_fctl,
                         c->st.fdphi, c->st.fdphi1};
         for (void* p : ptrs)
             if (p) cudaFree(p);
@@ -885,6 +887,114 @@ int amr_sub_step(amr_ctx* c, double dt, double beta) {
     return AMR_OK;
 }
 
+namespace {
+
+// Work list (finest level first, depth-first within a level) and publish
+// masks of the fused substep, rebuilt when the topology changes.
+int fused_setup(amr_ctx* c) {
+    const int cap = c->cap;
+    if (!c->d_U1) {
+        CUDA_TRY(cudaMalloc(&c->d_U1, sizeof(double) * (size_t)cap * c->geom.ucount));
+        CUDA_TRY(cudaMemcpyAsync(c->d_U1, c->st.U, sizeof(double) * (size_t)cap * c->geom.ucount,
+                                 cudaMemcpyDeviceToDevice, c->stream));
+        CUDA_TRY(cudaMalloc(&c->d_pubmask, (size_t)cap));
+        CUDA_TRY(cudaMalloc(&c->d_pub, sizeof(double) * (size_t)cap * 6 * c->geom.nf * c->geom.nx * c->geom.nx));
+        CUDA_TRY(cudaMalloc(&c->d_fdone, sizeof(int) * (size_t)cap));
+        CUDA_TRY(cudaMemsetAsync(c->d_fdone, 0, sizeof(int) * (size_t)cap, c->stream));
+        CUDA_TRY(cudaMalloc(&c->d_fctl, sizeof(unsigned int) * 2));
+    }
+    if (c->fused_version == c->topo_version) return AMR_OK;
+    std::vector<int2> work;
+    const int maxl = (int)c->level_slots.size() - 1;
+    for (int l = maxl; l >= 0; l--)
+        for (int q = 0; q < (int)c->level_slots[l].size(); q++) {
+            const int s = c->level_slots[l][q];
+            const int vr = c->off_vrange[l] + q;
+            work.push_back(make_int2(s, vr));
+        }
+    std::vector<unsigned char> mask((size_t)cap, 0);
+    for (int l = 0; l <= maxl; l++)
+        for (const RefluxItem& it : c->reflux[l])
+            mask[it.child] |= (unsigned char)(1u << (2 * it.dir + (it.ic == c->geom.bw ? 0 : 1)));
+    if ((int)work.size() > c->fwork_cap) {
+        if (c->d_fwork) cudaFree(c->d_fwork);
+        c->fwork_cap = (int)work.size() * 2 + 64;
+        CUDA_TRY(cudaMalloc(&c->d_fwork, sizeof(int2) * c->fwork_cap));
+    }
+    CUDA_TRY(cudaMemcpyAsync(c->d_fwork, work.data(), sizeof(int2) * work.size(), cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->d_pubmask, mask.data(), mask.size(), cudaMemcpyHostToDevice, c->stream));
+    c->nfwork = (int)work.size();
+    c->fused_version = c->topo_version;
+    return AMR_OK;
+}
+
+}  // namespace
+
+// amr_sub_step of the Euler driver as one persistent launch (plus the root's
+// flow-off): ghost zones, fluxes, coarse-fine corrections and the RK
+// combination per brick, the result written to the second state array which
+// then becomes the state.  Interiors are bitwise those of amr_sub_step (FP64
+// form); the ghost zones of the new state are not filled.
+int amr_fused_sub_step(amr_ctx* c, double dt, double beta, int blocks_per_sm) {
+    NEED_DEVICE(c);
+    if (c->cfg.physics != AMR_PHYSICS_EULER || c->geom.nf != 6) {
+        c->err = "fused substep: Euler physics without gravity only";
+        return AMR_ERR_ARG;
+    }
+    TRY(fused_setup(c));
+    CUDA_TRY(cudaMemsetAsync(c->d_fctl, 0, sizeof(unsigned int) * 2, c->stream));
+    FusedArgs a{};
+    a.g = c->geom;
+    a.bt = c->bt;
+    a.Uin = c->st.U;
+    a.U0 = c->st.U0;
+    a.Uout = c->d_U1;
+    a.work = c->d_fwork;
+    a.nwork = c->nfwork;
+    a.next = c->d_fctl;
+    a.done = c->d_fdone;
+    a.epoch = ++c->fused_epoch;
+    a.pubmask = c->d_pubmask;
+    a.pub = c->d_pub;
+    a.vitems = c->d_vitems;
+    a.vranges = c->d_vranges;
+    a.dt = dt;
+    a.beta = beta;
+    a.root = c->tree.root()->slot;
+    a.Fx = c->st.Fx;
+    a.Fy = c->st.Fy;
+    a.Fz = c->st.Fz;
+    a.err = reinterpret_cast<int*>(c->d_fctl + 1);
+    cudaError_t e;
+    {
+        ProfScope ps_(c->prof, KC_FUSED, c->stream, (long long)c->nfwork);
+        e = c->geom.precision == AMR_PREC_MIXED ? launch_substep_fused_f32(a, blocks_per_sm, c->stream, &c->fused_blocks)
+                                                : launch_substep_fused_f64(a, blocks_per_sm, c->stream, &c->fused_blocks);
+    }
+    if (e != cudaSuccess) {
+        c->err = std::string("fused substep launch: ") + cudaGetErrorString(e);
+        return AMR_ERR_CUDA;
+    }
+    {
+        ProfScope ps_(c->prof, KC_ADD_DIFS, c->stream);
+        launch_flow_off(c->geom, c->st, c->tree.root()->slot, c->tree.root()->h, dt, beta, c->d_fo, c->stream);
+    }
+    std::swap(c->st.U, c->d_U1);
+    for (Node* n : c->order) n->age++;  // GridNode::add_difs, grid_node.cpp:338
+    unsigned int err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&err, c->d_fctl + 1, sizeof(unsigned int), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (err & 1u) {
+        c->err = "fused substep: a wait for a child's face fluxes timed out";
+        return AMR_ERR_TIMEOUT;
+    }
+    if (err & 2u) {
+        c->err = "fused substep: coarse-fine ghost chain deeper than three levels";
+        return AMR_ERR_STATE;
+    }
+    return check_launch(c);
+}
+
 // HydroDriver::step (euler/hydro_driver.cpp:171-194), RK_ORDER 3.
 int amr_hydro_step(amr_ctx* c, double dt, double min_refine_density) {
     NEED_DEVICE(c);
@@ -912,7 +1022,7 @@ extern "C" {
 static const char* kClassNames[amr::KC_COUNT] = {
     "ghost_fill", "flux", "reflux", "add_difs", "inject", "max_dt", "refine_flags", "prolong",
     "relax", "vcycle_down", "phi_boundaries", "dphi_boundaries", "forces", "solution_error",
-    "source", "phys_boundary", "coarse_correction", "phi_time", "other"};
+    "source", "phys_boundary", "coarse_correction", "phi_time", "other", "fused_substep"};
 
 int amr_get_stream(amr_ctx* c, void** stream) {
     NEED_DEVICE(c);

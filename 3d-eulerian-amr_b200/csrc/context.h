@@ -70,6 +70,16 @@ struct amr_ctx {
     // [8 e + c]: list position of child c of level-list entry e (-1: none)
     int* d_cpos = nullptr;
     int cpos_cap = 0, max_level_cnt = 0;
+    // fused hydro substep: second state array, work list finest level first,
+    // publish masks and buffer, done stamps, counters
+    double* d_U1 = nullptr;
+    int2* d_fwork = nullptr;
+    unsigned char* d_pubmask = nullptr;
+    double* d_pub = nullptr;
+    int* d_fdone = nullptr;
+    unsigned int* d_fctl = nullptr;  // [0] work counter, [1] error word
+    int fwork_cap = 0, nfwork = 0, fused_epoch = 0, fused_blocks = 0;
+    long long fused_version = -1;  // topology the work list was built for
     int vitems_cap = 0, vranges_cap = 0;
     std::vector<int> off_vrange;
     int vcycle_max_outer = 1000;

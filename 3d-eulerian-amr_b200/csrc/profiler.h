@@ -14,7 +14,7 @@ namespace amr {
 enum KernelClass {
     KC_GHOST = 0, KC_FLUX, KC_REFLUX, KC_ADD_DIFS, KC_INJECT, KC_MAX_DT, KC_REFINE, KC_PROLONG,
     KC_RELAX, KC_VDOWN, KC_PHI_BOUND, KC_DPHI_BOUND, KC_FORCES, KC_ERROR, KC_SOURCE, KC_PHYS_BOUND,
-    KC_CORRECT, KC_PHI_TIME, KC_OTHER, KC_COUNT
+    KC_CORRECT, KC_PHI_TIME, KC_OTHER, KC_FUSED, KC_COUNT
 };
 
 struct Profiler {

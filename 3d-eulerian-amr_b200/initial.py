@@ -202,17 +202,32 @@ def octant_flags(U_interior, thr):
     return out
 
 
-def build_tree(amr, ic, min_refine_density, grid_dim, z_reflect, max_level, device=True):
+def _evaluate_padded(ic, t, bw, nx, grid_dim, z_reflect, max_level, ghosts):
+    if ghosts:
+        return evaluate(ic, t, bw, nx, grid_dim, z_reflect, max_level, ghosts=True)
+    Ui = evaluate(ic, t, bw, nx, grid_dim, z_reflect, max_level, ghosts=False)
+    g = nx + 2 * bw
+    U = np.zeros((Ui.shape[0], Ui.shape[1], g, g, g))
+    U[:, :, bw:-bw, bw:-bw, bw:-bw] = Ui
+    return U
+
+
+def build_tree(amr, ic, min_refine_density, grid_dim, z_reflect, max_level, device=True, ghosts=None):
     """Tree construction of the reference drivers (hydro_driver.cpp:84-107
     condensed): max_level rounds of initialize + check_for_refine, a final
     initialize, then restriction and ghost zones.  With device=False the
-    density test runs on the host (host-only contexts)."""
+    density test runs on the host (host-only contexts).  ghosts=False
+    evaluates interiors only (the ghost fill sets the face ghosts; edge and
+    corner ghosts are never read); the default is False for the random
+    field (large trees) and True otherwise."""
+    if ghosts is None:
+        ghosts = ic != "random"
     amr.init()
     amr.set_time(0.0)
     bw, nx = amr.bw, amr.nx
     for _ in range(max_level):
         t = amr.get_tree()
-        U = evaluate(ic, t, bw, nx, grid_dim, z_reflect, max_level, ghosts=True)
+        U = _evaluate_padded(ic, t, bw, nx, grid_dim, z_reflect, max_level, ghosts)
         if device:
             amr.upload_state(U)
             amr.check_for_refine(min_refine_density, True)
@@ -220,7 +235,7 @@ def build_tree(amr, ic, min_refine_density, grid_dim, z_reflect, max_level, devi
             fl = octant_flags(U[:, :, bw:-bw, bw:-bw, bw:-bw], min_refine_density)
             amr.refine_from_flags(fl, True)
     t = amr.get_tree()
-    U = evaluate(ic, t, bw, nx, grid_dim, z_reflect, max_level, ghosts=True)
+    U = _evaluate_padded(ic, t, bw, nx, grid_dim, z_reflect, max_level, ghosts)
     if device:
         amr.upload_state(U)
         amr.inject_from_children()
