@@ -27,7 +27,6 @@
 
 namespace amr {
 
-constexpr int FUSED_THREADS = 192;  // 3 directions x 64 pencils
 constexpr unsigned long long FUSED_WAIT_SPINS = 1ull << 24;
 
 __device__ __forceinline__ void fused_load(const FusedArgs& A, int b, const int* c, double* u) {
@@ -115,167 +114,182 @@ __device__ __forceinline__ void fused_wait(const FusedArgs& A, int child) {
     __threadfence();
 }
 
-// Phase 1 of brick b for pencil thread t < 192: the pencil's nine face
-// fluxes in FT (stored in FP64), the coarse-fine replacements, the brick's
-// published faces, and the pencil's flux differences into T[d][l][cell].
+// Block layout: 512 threads; per brick the "cross" -- the 8^3 interior and
+// the six 2-deep ghost slabs the dimension-split stencil reads -- is held in
+// shared memory as primitives (FT), and one direction's 9 x 64 face fluxes
+// (FP64) at a time.
+constexpr int FUSED_BLOCK = 512;
+constexpr int CROSS = 512 + 6 * 2 * 64;  // interior + ghost slabs
+constexpr int FACES = 9 * 64;            // faces of one direction
+
+// cross index of the cell at position n (0..11) along direction d of pencil
+// (t1, t2): interior (z*8 + y)*8 + x, or slab ((face*2 + depth)*8 + t2)*8 + t1
+__device__ __forceinline__ int cross_index(int d, int n, int t1, int t2) {
+    if (n < 2) return 512 + (((2 * d) * 2 + n) * 8 + t2) * 8 + t1;
+    if (n >= 10) return 512 + (((2 * d + 1) * 2 + (n - 10)) * 8 + t2) * 8 + t1;
+    const int i = n - 2;
+    const int x = d == 0 ? i : t1, y = d == 1 ? i : (d == 0 ? t1 : t2), z = d == 2 ? i : t2;
+    return (z * 8 + y) * 8 + x;
+}
+
 template <typename FT>
-__device__ __forceinline__ void fused_pencil(const FusedArgs& A, int b, int vr, double* T) {
+__device__ __forceinline__ void fused_brick(const FusedArgs& A, int b, int vr, FT* P, double* Fs) {
     const Geom& g = A.g;
-    const int nx = g.nx, gnx = g.gnx, bw = g.bw, npen = nx * nx, half = nx / 2;
-    const int d = threadIdx.x / npen;
-    const int p = threadIdx.x % npen;
-    const int t1 = p % nx, t2 = p / nx;
-    const double hinv = 1.0 / A.bt.h[b];
-    const FT th = (FT)g.theta, gam = (FT)g.gamma;
-    // coarse-fine faces of this pencil (at most one per child boundary)
-    int ov_fi[3], ov_child[3], ov_side[3], ov_a[3], ov_c[3], nov = 0;
-    if (vr >= 0) {
-        const int* rg = A.vranges + 4 * vr;
-        for (int q = rg[d]; q < rg[d + 1] && nov < 3; q++) {
-            const RefluxItem it = A.vitems[q];
-            const int a = t1 - it.cj * half, c = t2 - it.ck * half;
-            if (a < 0 || a >= half || c < 0 || c >= half) continue;
-            ov_fi[nov] = it.i0 - bw;
-            ov_child[nov] = it.child;
-            ov_side[nov] = it.ic == bw ? 0 : 1;
-            ov_a[nov] = a;
-            ov_c[nov] = c;
-            nov++;
-        }
-    }
-    int cell[3];
-    cell[d == 0 ? 1 : 0] = t1 + bw;
-    cell[d == 2 ? 1 : 2] = t2 + bw;
-    auto load = [&](int n, FT* w) {
+    const int nx = 8, gnx = 12, bw = 2, npen = 64, half = 4;
+    const int tid = threadIdx.x;
+    // (a) the cross as primitives: interior cells, then ghost cells resolved
+    //     as the level-ordered ghost fill would have set them
+    for (int q = tid; q < CROSS; q += FUSED_BLOCK) {
         double u[NF_EULER];
-        cell[d] = n;
-        if (n >= bw && n < gnx - bw)
-            fused_load(A, b, cell, u);
-        else
-            fused_cell<3>(A, b, cell, u);
+        int c[3];
+        if (q < 512) {
+            c[0] = q % 8 + bw;
+            c[1] = (q / 8) % 8 + bw;
+            c[2] = q / 64 + bw;
+            fused_load(A, b, c, u);
+        } else {
+            const int r = q - 512, t1 = r % 8, t2 = (r / 8) % 8, depth = (r / 64) % 2, face = r / 128;
+            const int ax = face >> 1;
+            c[ax] = (face & 1) ? gnx - bw + depth : depth;
+            c[ax == 0 ? 1 : 0] = t1 + bw;
+            c[ax == 2 ? 1 : 2] = t2 + bw;
+            fused_cell<3>(A, b, c, u);
+        }
+        FT w[NF_EULER];
 #pragma unroll
         for (int l = 0; l < NF_EULER; l++) w[l] = (FT)u[l];
         st_to_prim(w);
-    };
-    FT w[4][NF_EULER];
-    for (int n = 0; n < 3; n++) load(n, w[n + 1]);
-    FT sR[NF_EULER];
-    for (int n = 3; n < bw + 1; n++) {
 #pragma unroll
-        for (int m = 0; m < 3; m++)
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) w[m][l] = w[m + 1][l];
-        load(n, w[3]);
+        for (int l = 0; l < NF_EULER; l++) P[l * CROSS + q] = w[l];
     }
-#pragma unroll
-    for (int l = 0; l < NF_EULER; l++) sR[l] = minmod_theta(w[3][l] - w[2][l], w[2][l] - w[1][l], th);
+    __syncthreads();
+    const double hinv = 1.0 / A.bt.h[b];
+    const FT th = (FT)g.theta, gam = (FT)g.gamma;
     const unsigned char pm = A.pubmask[b];
     double* pubb = A.pub + (size_t)b * 6 * NF_EULER * npen;
-    double Fprev[NF_EULER];
-    for (int f = bw; f <= gnx - bw; f++) {
+    const int* rg = vr >= 0 ? A.vranges + 4 * vr : nullptr;
+    double D[NF_EULER];  // this thread's cell (tid): flux differences, x then y then z
 #pragma unroll
-        for (int m = 0; m < 3; m++)
+    for (int l = 0; l < NF_EULER; l++) D[l] = 0.0;
+    for (int d = 0; d < 3; d++) {
+        // (b) face fluxes of direction d, one thread per face
+        for (int q = tid; q < FACES; q += FUSED_BLOCK) {
+            const int p = q % npen, fi = q / npen;
+            const int t1 = p % nx, t2 = p / nx;
+            FT w[4][NF_EULER];  // cells f-2 .. f+1 (f = fi + bw)
 #pragma unroll
-            for (int l = 0; l < NF_EULER; l++) w[m][l] = w[m + 1][l];
-        load(f + 1, w[3]);
-        FT ql[NF_EULER], qr[NF_EULER], sL[NF_EULER];
+            for (int m = 0; m < 4; m++) {
+                const int ci = cross_index(d, fi + m, t1, t2);
 #pragma unroll
-        for (int l = 0; l < NF_EULER; l++) {
-            sL[l] = sR[l];
-            sR[l] = minmod_theta(w[3][l] - w[2][l], w[2][l] - w[1][l], th);
-            ql[l] = w[1][l] + sL[l] / FT(2);
-            qr[l] = w[2][l] - sR[l] / FT(2);
-        }
-        st_to_con(ql);
-        st_to_con(qr);
-        FT fl[NF_EULER], fr[NF_EULER];
-        const FT al = st_flux(ql, d, gam, fl);
-        const FT ar = st_flux(qr, d, gam, fr);
-        const FT a = r_max(al, ar);
-        const int fi = f - bw;
-        double F[NF_EULER];
-#pragma unroll
-        for (int l = 0; l < NF_EULER; l++) F[l] = (double)(((fl[l] + fr[l]) - (qr[l] - ql[l]) * a) * FT(0.5));
-        // coarse-fine correction: mean of the child's four faces
-        for (int o = 0; o < nov; o++) {
-            if (ov_fi[o] != fi) continue;
-            fused_wait(A, ov_child[o]);
-            const double* Fc = A.pub + ((size_t)ov_child[o] * 6 + 2 * d + ov_side[o]) * NF_EULER * npen;
-            const int j = 2 * ov_a[o], k = 2 * ov_c[o];
+                for (int l = 0; l < NF_EULER; l++) w[m][l] = P[l * CROSS + ci];
+            }
+            FT ql[NF_EULER], qr[NF_EULER];
 #pragma unroll
             for (int l = 0; l < NF_EULER; l++) {
-                const double* C = Fc + l * npen;
-                double v = +__ldcg(C + k * nx + j);
-                v += __ldcg(C + k * nx + j + 1);
-                v += __ldcg(C + (k + 1) * nx + j);
-                v += __ldcg(C + (k + 1) * nx + j + 1);
-                F[l] = v * 0.25;
+                const FT sL = minmod_theta(w[2][l] - w[1][l], w[1][l] - w[0][l], th);  // slope of cell f-1
+                const FT sR = minmod_theta(w[3][l] - w[2][l], w[2][l] - w[1][l], th);  // slope of cell f
+                ql[l] = w[1][l] + sL / FT(2);
+                qr[l] = w[2][l] - sR / FT(2);
             }
+            st_to_con(ql);
+            st_to_con(qr);
+            FT fl[NF_EULER], fr[NF_EULER];
+            const FT al = st_flux(ql, d, gam, fl);
+            const FT ar = st_flux(qr, d, gam, fr);
+            const FT a = r_max(al, ar);
+            double F[NF_EULER];
+#pragma unroll
+            for (int l = 0; l < NF_EULER; l++) F[l] = (double)(((fl[l] + fr[l]) - (qr[l] - ql[l]) * a) * FT(0.5));
+            // coarse-fine correction: mean of the child's four faces
+            if (rg) {
+                for (int it_q = rg[d]; it_q < rg[d + 1]; it_q++) {
+                    const RefluxItem it = A.vitems[it_q];
+                    const int aa = t1 - it.cj * half, cc = t2 - it.ck * half;
+                    if (it.i0 - bw != fi || aa < 0 || aa >= half || cc < 0 || cc >= half) continue;
+                    fused_wait(A, it.child);
+                    const int side = it.ic == bw ? 0 : 1;
+                    const double* Fc = A.pub + ((size_t)it.child * 6 + 2 * d + side) * NF_EULER * npen;
+                    const int j = 2 * aa, k = 2 * cc;
+#pragma unroll
+                    for (int l = 0; l < NF_EULER; l++) {
+                        const double* C = Fc + l * npen;
+                        double v = +__ldcg(C + k * nx + j);
+                        v += __ldcg(C + k * nx + j + 1);
+                        v += __ldcg(C + (k + 1) * nx + j);
+                        v += __ldcg(C + (k + 1) * nx + j + 1);
+                        F[l] = v * 0.25;
+                    }
+                }
+            }
+            if (fi == 0 && (pm & (1u << (2 * d))))
+#pragma unroll
+                for (int l = 0; l < NF_EULER; l++) pubb[(2 * d * NF_EULER + l) * npen + p] = F[l];
+            if (fi == nx && (pm & (1u << (2 * d + 1))))
+#pragma unroll
+                for (int l = 0; l < NF_EULER; l++) pubb[((2 * d + 1) * NF_EULER + l) * npen + p] = F[l];
+            if (b == A.root) {
+                double* Fr = (d == 0 ? A.Fx : (d == 1 ? A.Fy : A.Fz)) + (size_t)b * g.nf * npen * (nx + 1);
+#pragma unroll
+                for (int l = 0; l < NF_EULER; l++) Fr[l * npen * (nx + 1) + flux_index(d, nx, fi, t1, t2)] = F[l];
+            }
+#pragma unroll
+            for (int l = 0; l < NF_EULER; l++) Fs[l * FACES + q] = F[l];
         }
-        if (fi == 0 && (pm & (1u << (2 * d))))
+        __syncthreads();
+        // (c) this thread's cell: D -= (F(i+1) - F(i)) / h along d
+        {
+            const int x = tid % 8, y = (tid / 8) % 8, z = tid / 64;
+            const int i = d == 0 ? x : (d == 1 ? y : z);
+            const int p = d == 0 ? z * 8 + y : (d == 1 ? z * 8 + x : y * 8 + x);
 #pragma unroll
-            for (int l = 0; l < NF_EULER; l++) pubb[(2 * d * NF_EULER + l) * npen + p] = F[l];
-        if (fi == nx && (pm & (1u << (2 * d + 1))))
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) pubb[((2 * d + 1) * NF_EULER + l) * npen + p] = F[l];
-        if (b == A.root) {
-            double* Fr = (d == 0 ? A.Fx : (d == 1 ? A.Fy : A.Fz)) + (size_t)b * g.nf * npen * (nx + 1);
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) Fr[l * npen * (nx + 1) + flux_index(d, nx, fi, t1, t2)] = F[l];
+            for (int l = 0; l < NF_EULER; l++)
+                D[l] -= (Fs[l * FACES + (i + 1) * npen + p] - Fs[l * FACES + i * npen + p]) * hinv;
         }
-        if (fi > 0) {
-            // cell fi-1 along the pencil: (F(fi) - F(fi-1)) / h
-            const int i = fi - 1;
-            const int x = d == 0 ? i : t1, y = d == 1 ? i : (d == 0 ? t1 : t2), z = d == 2 ? i : t2;
-            const int cc = (z * nx + y) * nx + x;
+        __syncthreads();
+    }
+    // faces published: stamp the brick done for the coarser bricks
+    __threadfence();
+    __syncthreads();
+    if (tid == 0 && pm) atomicExch(A.done + b, A.epoch);
+    // (d) Grid::add_difs (grid.cpp:406-420) for this thread's cell
+    {
+        const int x = tid % 8, y = (tid / 8) % 8, z = tid / 64;
+        const int ci = cell_index(gnx, x + bw, y + bw, z + bw);
+        const double* U = A.Uin + (size_t)b * g.ucount;
+        const double* U0 = A.U0 + (size_t)b * g.ucount;
+        double* Uo = A.Uout + (size_t)b * g.ucount;
+        double u[NF_EULER];
 #pragma unroll
-            for (int l = 0; l < NF_EULER; l++) T[(d * NF_EULER + l) * nx * nx * nx + cc] = (F[l] - Fprev[l]) * hinv;
+        for (int l = 0; l < NF_EULER; l++) {
+            const double Dl = D[l] + 0.0;  // State::source() is zero for the Euler state
+            u[l] = (U[(size_t)l * g.gnx3 + ci] + Dl * A.dt) * A.beta + U0[(size_t)l * g.gnx3 + ci] * (1.0 - A.beta);
         }
+        st_floor(u, g.gamma, g.rho_floor, g.ei_floor);
 #pragma unroll
-        for (int l = 0; l < NF_EULER; l++) Fprev[l] = F[l];
+        for (int l = 0; l < NF_EULER; l++) Uo[(size_t)l * g.gnx3 + ci] = u[l];
     }
 }
 
 template <typename FT>
-__global__ void __launch_bounds__(FUSED_THREADS) k_substep_fused(FusedArgs A) {
-    extern __shared__ double T[];  // [3][nf][nx^3] flux differences
+__global__ void __launch_bounds__(FUSED_BLOCK, 2) k_substep_fused(FusedArgs A) {
+    extern __shared__ double smem[];  // [nf][CROSS] primitives (FT), then [nf][FACES] fluxes (FP64)
+    FT* P = reinterpret_cast<FT*>(smem);
+    double* Fs = smem + (NF_EULER * CROSS * sizeof(FT) + sizeof(double) - 1) / sizeof(double);
     __shared__ int s_item;
-    const Geom& g = A.g;
-    const int nx = g.nx, bw = g.bw, gnx = g.gnx;
     for (;;) {
         if (threadIdx.x == 0) s_item = (int)atomicAdd(A.next, 1u);
         __syncthreads();
         const int w = s_item;
         if (w >= A.nwork) break;
-        const int b = A.work[w].x, vr = A.work[w].y;
-        fused_pencil<FT>(A, b, vr, T);
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0 && A.pubmask[b]) atomicExch(A.done + b, A.epoch);
-        // Grid::add_difs (grid.cpp:406-420) with the x, y, z differences
-        const double dt = A.dt, beta = A.beta;
-        const double* U = A.Uin + (size_t)b * g.ucount;
-        const double* U0 = A.U0 + (size_t)b * g.ucount;
-        double* Uo = A.Uout + (size_t)b * g.ucount;
-        for (int t = threadIdx.x; t < nx * nx * nx; t += blockDim.x) {
-            const int i = t % nx, j = (t / nx) % nx, k = t / (nx * nx);
-            const int ci = cell_index(gnx, i + bw, j + bw, k + bw);
-            double u[NF_EULER];
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) {
-                double D = 0.0;
-                D -= T[(0 * NF_EULER + l) * nx * nx * nx + t];
-                D -= T[(1 * NF_EULER + l) * nx * nx * nx + t];
-                D -= T[(2 * NF_EULER + l) * nx * nx * nx + t];
-                D += 0.0;  // State::source() is zero for the Euler state
-                u[l] = (U[(size_t)l * g.gnx3 + ci] + D * dt) * beta + U0[(size_t)l * g.gnx3 + ci] * (1.0 - beta);
-            }
-            st_floor(u, g.gamma, g.rho_floor, g.ei_floor);
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) Uo[(size_t)l * g.gnx3 + ci] = u[l];
-        }
+        fused_brick<FT>(A, A.work[w].x, A.work[w].y, P, Fs);
         __syncthreads();
     }
+}
+
+template <typename FT>
+constexpr size_t fused_smem_bytes() {
+    return ((NF_EULER * CROSS * sizeof(FT) + sizeof(double) - 1) / sizeof(double)) * sizeof(double) +
+           sizeof(double) * NF_EULER * FACES;
 }
 
 }  // namespace amr

@@ -13,14 +13,14 @@ int fused_blocks(const void* kernel, size_t smem) {
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, FUSED_THREADS, smem) != cudaSuccess || per <= 0)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, FUSED_BLOCK, smem) != cudaSuccess || per <= 0)
         return -1;
     return sms * per;
 }
 }  // namespace
 
 cudaError_t launch_substep_fused_f32(const FusedArgs& a, int blocks_per_sm_cap, cudaStream_t s, int* blocks_used) {
-    const size_t smem = sizeof(double) * 3 * NF_EULER * a.g.nx * a.g.nx * a.g.nx;
+    const size_t smem = fused_smem_bytes<float>();
     const void* k = (const void*)k_substep_fused<float>;
     int blocks = fused_blocks(k, smem);
     if (blocks <= 0) return cudaErrorInvalidConfiguration;
@@ -32,7 +32,7 @@ cudaError_t launch_substep_fused_f32(const FusedArgs& a, int blocks_per_sm_cap, 
     }
     blocks = std::min(blocks, std::max(a.nwork, 1));
     if (blocks_used) *blocks_used = blocks;
-    launch_k(k_substep_fused<float>, blocks, FUSED_THREADS, smem, s, a);
+    launch_k(k_substep_fused<float>, blocks, FUSED_BLOCK, smem, s, a);
     return cudaGetLastError();
 }
 

@@ -577,6 +577,60 @@ def run_batched_substep(amr, ini, torch, steps, warmup, levels=5):
     return out
 
 
+def run_case(case):
+    """One small run of a single kernel family, for profiler captures:
+    solve_L3      one Poisson solve (L1 tol 1e-6) of the 3-level star, mixed
+                  persistent form (k_solve_persistent)
+    substep_L4    two fused substeps on the 5-level random-field octree
+                  (k_substep_fused, FP64)
+    eos_1M        2^20 points, forward and inverse Helmholtz EOS"""
+    import torch
+    amr, ini = load_amr()
+    if case == "solve_L3":
+        a = amr.AMR(physics=amr.PHYSICS_EULER_GRAVITY, max_refine_level=3, grid_dim=0.5, z_reflect=0,
+                    max_bricks=2048, precision=amr.PREC_MIXED, persistent_solve=1)
+        ini.build_tree(a, "polytrope", 1.0e-6, 0.5, 0, 3, device=True)
+        err, cyc = a.graph_solve(1e-6, 1000)
+        a.synchronize()
+        print(json.dumps({"case": case, "bricks": a.nbricks, "vcycles": cyc, "l1": err}))
+        a.close()
+    elif case == "substep_L4":
+        F = ini.random_field()
+        a = amr.AMR(physics=amr.PHYSICS_EULER, max_refine_level=4, grid_dim=0.5, z_reflect=0, max_bricks=8192)
+        ini.build_tree(a, "random", float(np.percentile(F, 90)), 0.5, 0, 4, device=True)
+        dt = a.max_dt()
+        a.store()
+        for beta in (1.0, 0.25):
+            a.fused_sub_step(dt, beta)
+        a.synchronize()
+        print(json.dumps({"case": case, "bricks": a.nbricks, "dt": dt}))
+        a.close()
+    elif case == "eos_1M":
+        helm_table = _load_module("helm_table", os.path.join(PKG, "helm_table.py"))
+        helm_mod = _load_module("helm_b200", os.path.join(PKG, "helm.py"))
+        tdir = tempfile.mkdtemp(prefix="helm_table_")
+        h = helm_mod.Helm(helm_table.ensure_table(tdir))
+        n = 1 << 20
+        g = torch.Generator(device="cpu").manual_seed(5)
+        rho = torch.pow(10.0, -2 + 11 * torch.rand(n, dtype=torch.float64, generator=g)).cuda()
+        T = torch.pow(10.0, 4 + 5 * torch.rand(n, dtype=torch.float64, generator=g)).cuda()
+        abar = (12 + 4 * torch.rand(n, dtype=torch.float64, generator=g)).cuda()
+        zbar = abar / 2
+        p, e, cs = (torch.empty_like(rho) for _ in range(3))
+        st = torch.empty(n, dtype=torch.int32, device="cuda")
+        h.eos_device(rho, T, abar, zbar, p, e, cs, st)
+        Tg = T * 1.5
+        h.invert_T_device(rho, e, abar, zbar, Tg, st)
+        torch.cuda.synchronize()
+        print(json.dumps({"case": case, "points": n, "bad": int((st != 0).sum())}))
+        h.close()
+        import shutil
+        shutil.rmtree(tdir, ignore_errors=True)
+    else:
+        raise SystemExit("unknown case " + case)
+    return 0
+
+
 def roofline_persistent(res):
     """Roofline of the persistent solve kernel, the step's dominant kernel:
     algorithmic bytes per launch (the arrays each phase must read and write
@@ -627,7 +681,11 @@ def main():
     ap.add_argument("--json-out", default=None)
     ap.add_argument("--no-eos", action="store_true", help="skip the Helmholtz EOS throughput section")
     ap.add_argument("--no-batched", action="store_true", help="skip the random-field octree substep section")
+    ap.add_argument("--case", default=None, choices=["solve_L3", "substep_L4", "eos_1M"],
+                    help="run one small case for a profiler capture and exit")
     args = ap.parse_args()
+    if args.case:
+        return run_case(args.case)
     if args.impl == "reference":
         return reference_arm(args)
 
