@@ -989,7 +989,7 @@ int amr_fused_sub_step(amr_ctx* c, double dt, double beta, int blocks_per_sm) {
         return AMR_ERR_TIMEOUT;
     }
     if (err & 2u) {
-        c->err = "fused substep: coarse-fine ghost chain deeper than three levels";
+        c->err = "fused substep: coarse-fine ghost of a coarse-fine ghost (tree not properly nested)";
         return AMR_ERR_STATE;
     }
     return check_launch(c);

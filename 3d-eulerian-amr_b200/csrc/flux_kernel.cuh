@@ -23,13 +23,29 @@ __device__ __forceinline__ int flux_index(int d, int nx, int fi, int t1, int t2)
 
 __device__ __forceinline__ int cell_index(int gnx, int i, int j, int k) { return (k * gnx + j) * gnx + i; }
 
+template <typename T, int d>
+__device__ __forceinline__ void flux_pencil_dir(const Geom& g, const DevState& st, int b, int p);
+
+// The direction is made a compile-time constant per thread, so the state
+// arrays indexed by it (normal velocity, normal momentum flux) stay in
+// registers.
 template <typename T>
 __device__ __forceinline__ void flux_pencils(const Geom& g, const DevState& st, int b) {
+    const int npen = g.nx * g.nx;
+    const int d = threadIdx.x / npen;
+    const int p = threadIdx.x % npen;
+    if (d == 0)
+        flux_pencil_dir<T, 0>(g, st, b, p);
+    else if (d == 1)
+        flux_pencil_dir<T, 1>(g, st, b, p);
+    else if (d == 2)
+        flux_pencil_dir<T, 2>(g, st, b, p);
+}
+
+template <typename T, int d>
+__device__ __forceinline__ void flux_pencil_dir(const Geom& g, const DevState& st, int b, int p) {
     const int nx = g.nx, gnx = g.gnx, bw = g.bw;
     const int npen = nx * nx;
-    const int d = threadIdx.x / npen;
-    if (d >= 3) return;
-    const int p = threadIdx.x % npen;
     const int t1 = p % nx, t2 = p / nx;  // interior transverse indices
     const double* U = st.U + (size_t)b * g.ucount;
     int stride, base;

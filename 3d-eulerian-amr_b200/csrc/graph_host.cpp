@@ -91,7 +91,7 @@ int ensure_state(amr_ctx* c) {
     CUDA_TRY(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CUDA_TRY(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned int) * 4, c->stream));
     if (c->cfg.persistent_solve) {
-        g->pblocks = solve_persistent_blocks(c->cfg.precision);
+        g->pblocks = solve_persistent_blocks(c->cfg.precision, c->cfg.persistent_solve);
         if (g->pblocks <= 0) {
             c->err = "no cooperative launch configuration for the persistent solve";
             return AMR_ERR_CUDA;

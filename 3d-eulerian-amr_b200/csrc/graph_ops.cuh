@@ -89,21 +89,19 @@ __device__ __forceinline__ CT ghost_dphi(const Geom& g, const BrickTable& bt, co
     if (kind == FACE_SIB) return __ldcg(snap_rd + (size_t)nbr * stride + ((face ^ 1) * NX + (t1 - 1)) * NX + (t2 - 1));
     if (kind == FACE_OUTFLOW) return CT(0);
     const int ax = face >> 1;
-    int q[3];
-    q[ax] = (face & 1) ? 1 : P - 2;
-    q[ax == 0 ? 1 : 0] = t1;
-    q[ax == 2 ? 1 : 2] = t2;
+    const int qa = (face & 1) ? 1 : P - 2;  // the source layer along the face normal
+    const int q0 = ax == 0 ? qa : t1;
+    const int q1 = ax == 1 ? qa : (ax == 0 ? t1 : t2);
+    const int q2 = ax == 2 ? qa : t2;
     if (kind == FACE_REFLECT) {  // own value mirrored through z = 0, before this pass
-        const int kk = q[2] == 1 ? P - 2 : 1;
-        return D[(size_t)b * P * P * P + (kk * P + q[1]) * P + q[0]];
+        const int kk = q2 == 1 ? P - 2 : 1;
+        return D[(size_t)b * P * P * P + (kk * P + q1) * P + q0];
     }
     const int v = (face & 1) ? 1 : -1;
-    int r[3];
-    for (int d = 0; d < 3; d++) {
-        const int rel = bt.off[3 * b + d] + (d == ax ? v * (P - 2) : 0) - 2 * bt.off[3 * nbr + d] - (g.bw - 1);
-        r[d] = (rel + q[d]) / 2;
-    }
-    return D[(size_t)nbr * P * P * P + (r[2] * P + r[1]) * P + r[0]];
+    const int r0 = (bt.off[3 * b + 0] + (ax == 0 ? v * (P - 2) : 0) - 2 * bt.off[3 * nbr + 0] - (g.bw - 1) + q0) / 2;
+    const int r1 = (bt.off[3 * b + 1] + (ax == 1 ? v * (P - 2) : 0) - 2 * bt.off[3 * nbr + 1] - (g.bw - 1) + q1) / 2;
+    const int r2 = (bt.off[3 * b + 2] + (ax == 2 ? v * (P - 2) : 0) - 2 * bt.off[3 * nbr + 2] - (g.bw - 1) + q2) / 2;
+    return D[(size_t)nbr * P * P * P + (r2 * P + r1) * P + r0];
 }
 
 // One relaxation pass of brick b (block = NX^3 threads): mode 1 fills the

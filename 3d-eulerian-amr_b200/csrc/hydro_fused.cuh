@@ -29,76 +29,102 @@ namespace amr {
 
 constexpr unsigned long long FUSED_WAIT_SPINS = 1ull << 24;
 
-__device__ __forceinline__ void fused_load(const FusedArgs& A, int b, const int* c, double* u) {
-    const double* U = A.Uin + (size_t)b * A.g.ucount + cell_index(A.g.gnx, c[0], c[1], c[2]);
-#pragma unroll
-    for (int l = 0; l < NF_EULER; l++) u[l] = U[(size_t)l * A.g.gnx3];
+// Six conserved fields of one cell, indexed only by compile-time constants
+// (stays in registers).
+struct Cell6 {
+    double v[NF_EULER];
+};
+
+// State::enforce_outflow (euler/state.cpp:45-84) on a register cell, the
+// same arithmetic as st_enforce_outflow without a run-time array index.
+__device__ __forceinline__ void fused_outflow(Cell6& u, int bface) {
+    const int m = 1 + (bface >> 1);
+    const double um = m == 1 ? u.v[1] : (m == 2 ? u.v[2] : u.v[3]);
+    bool zero;
+    if (bface == ZU || bface == ZL) {
+        zero = (bface == ZU) ? (u.v[3] > 0.0) : (u.v[3] < 0.0);
+    } else {
+        const double v = um / u.v[0];
+        zero = (bface & 1) ? (v > 0.0) : (v < 0.0);
+    }
+    if (zero) {
+        u.v[4] = u.v[4] - 0.5 * um * um / u.v[0];
+        if (m == 1) u.v[1] = 0.0;
+        else if (m == 2) u.v[2] = 0.0;
+        else u.v[3] = 0.0;
+    }
 }
 
-// Cell c (GNX frame) of brick b: the interior value, or the face-ghost value
-// k_ghost_fill would store there (at most one coordinate outside the
-// interior).  DEPTH bounds the coarse-fine hops.
+__device__ __forceinline__ int axis_of(int x, int y, int z, int a) { return a == 0 ? x : (a == 1 ? y : z); }
+
+__device__ __forceinline__ void fused_load(const FusedArgs& A, int b, int x, int y, int z, Cell6& u) {
+    const double* U = A.Uin + (size_t)b * A.g.ucount + cell_index(A.g.gnx, x, y, z);
+#pragma unroll
+    for (int l = 0; l < NF_EULER; l++) u.v[l] = U[(size_t)l * A.g.gnx3];
+}
+
+// Cell (x, y, z) (GNX frame) of brick b: the interior value, or the
+// face-ghost value k_ghost_fill would store there (at most one coordinate
+// outside the interior).  DEPTH bounds the coarse-fine hops: a coarse-fine
+// ghost reads the parent's cells, whose ghosts across the same face are
+// same-level or domain ghosts under proper nesting, so DEPTH = 1 suffices;
+// a deeper chain sets err bit 1.
 template <int DEPTH>
-__device__ bool fused_cell(const FusedArgs& A, int b, const int* c, double* u) {
-    const Geom& g = A.g;
-    const int bw = g.bw, gnx = g.gnx;
-    int ax = -1, upper = 0;
-    for (int d = 0; d < 3; d++) {
-        if (c[d] < bw) ax = d, upper = 0;
-        else if (c[d] >= gnx - bw) ax = d, upper = 1;
-    }
+__device__ __forceinline__ void fused_cell(const FusedArgs& A, int b, int x, int y, int z, Cell6& u) {
+    const int bw = 2, gnx = 12;
+    const int ax = (x < bw || x >= gnx - bw) ? 0 : ((y < bw || y >= gnx - bw) ? 1 : ((z < bw || z >= gnx - bw) ? 2 : -1));
     if (ax < 0) {
-        fused_load(A, b, c, u);
-        return true;
+        fused_load(A, b, x, y, z, u);
+        return;
     }
+    const int gi = axis_of(x, y, z, ax);
+    const int upper = gi >= gnx - bw ? 1 : 0;
     const int face = 2 * ax + upper;
     const int kind = A.bt.ftype[6 * b + face];
     const int nbr = A.bt.fnbr[6 * b + face];
-    const int gi = c[ax];
-    int s[3] = {c[0], c[1], c[2]};
+    int sx = x, sy = y, sz = z, src = b;
+    int s;
     if (kind == FACE_SIB) {
-        s[ax] = upper ? gi - (gnx - 2 * bw) : gi + (gnx - 2 * bw);
-        fused_load(A, nbr, s, u);
-        return true;
+        s = upper ? gi - (gnx - 2 * bw) : gi + (gnx - 2 * bw);
+        src = nbr;
+    } else if (kind == FACE_OUTFLOW) {
+        s = upper ? gnx - bw - 1 : bw;
+    } else if (kind == FACE_REFLECT) {
+        s = 2 * bw - 1 - gi;
+    } else {
+        s = -1;
     }
-    if (kind == FACE_OUTFLOW) {
-        s[ax] = upper ? gnx - bw - 1 : bw;
-        fused_load(A, b, s, u);
-        st_enforce_outflow(u, face ^ 1);
-        return true;
-    }
-    if (kind == FACE_REFLECT) {
-        s[ax] = 2 * bw - 1 - gi;
-        fused_load(A, b, s, u);
-        u[3] = -u[3];
-        return true;
+    if (s >= 0) {
+        if (ax == 0) sx = s;
+        else if (ax == 1) sy = s;
+        else sz = s;
+        fused_load(A, src, sx, sy, sz, u);
+        if (kind == FACE_OUTFLOW) fused_outflow(u, face ^ 1);
+        if (kind == FACE_REFLECT) u.v[3] = -u.v[3];
+        return;
     }
     if constexpr (DEPTH == 0) {
         atomicOr(A.err, 2);
-        for (int l = 0; l < NF_EULER; l++) u[l] = 0.0;
-        return false;
+#pragma unroll
+        for (int l = 0; l < NF_EULER; l++) u.v[l] = 0.0;
     } else {
         // GridAMRBound::operator() (grid_amr_bound.cpp:27-78)
-        int pi[3], par = 0;
-        for (int d = 0; d < 3; d++) {
-            const int fine = A.bt.off[3 * b + d] - 2 * A.bt.off[3 * nbr + d] + c[d];
-            pi[d] = fine / 2;
-            if (d == ax) par = fine % 2;
-        }
-        int pp[3] = {pi[0], pi[1], pi[2]}, pm[3] = {pi[0], pi[1], pi[2]};
-        pp[ax] += 1;
-        pm[ax] -= 1;
-        double uc[NF_EULER], up[NF_EULER], um[NF_EULER];
-        bool ok = fused_cell<DEPTH - 1>(A, nbr, pi, uc);
-        ok &= fused_cell<DEPTH - 1>(A, nbr, pp, up);
-        ok &= fused_cell<DEPTH - 1>(A, nbr, pm, um);
+        const int fx = A.bt.off[3 * b + 0] - 2 * A.bt.off[3 * nbr + 0] + x;
+        const int fy = A.bt.off[3 * b + 1] - 2 * A.bt.off[3 * nbr + 1] + y;
+        const int fz = A.bt.off[3 * b + 2] - 2 * A.bt.off[3 * nbr + 2] + z;
+        const int px = fx / 2, py = fy / 2, pz = fz / 2;
+        const int par = axis_of(fx, fy, fz, ax) % 2;
+        const int dx = ax == 0, dy = ax == 1, dz = ax == 2;
+        Cell6 uc, up, um;
+        fused_cell<DEPTH - 1>(A, nbr, px, py, pz, uc);
+        fused_cell<DEPTH - 1>(A, nbr, px + dx, py + dy, pz + dz, up);
+        fused_cell<DEPTH - 1>(A, nbr, px - dx, py - dy, pz - dz, um);
 #pragma unroll
         for (int l = 0; l < NF_EULER; l++) {
-            double m = minmod2(up[l] - uc[l], uc[l] - um[l]);
+            double m = minmod2(up.v[l] - uc.v[l], uc.v[l] - um.v[l]);
             if (par == 1) m = -m;
-            u[l] = uc[l] - m * 0.25;
+            u.v[l] = uc.v[l] - m * 0.25;
         }
-        return ok;
     }
 }
 
@@ -118,7 +144,7 @@ __device__ __forceinline__ void fused_wait(const FusedArgs& A, int child) {
 // the six 2-deep ghost slabs the dimension-split stencil reads -- is held in
 // shared memory as primitives (FT), and one direction's 9 x 64 face fluxes
 // (FP64) at a time.
-constexpr int FUSED_BLOCK = 512;
+constexpr int FUSED_BLOCK = 256;  // two cells per thread in the per-cell phases
 constexpr int CROSS = 512 + 6 * 2 * 64;  // interior + ghost slabs
 constexpr int FACES = 9 * 64;            // faces of one direction
 
@@ -140,24 +166,23 @@ __device__ __forceinline__ void fused_brick(const FusedArgs& A, int b, int vr, F
     // (a) the cross as primitives: interior cells, then ghost cells resolved
     //     as the level-ordered ghost fill would have set them
     for (int q = tid; q < CROSS; q += FUSED_BLOCK) {
-        double u[NF_EULER];
-        int c[3];
+        Cell6 u;
         if (q < 512) {
-            c[0] = q % 8 + bw;
-            c[1] = (q / 8) % 8 + bw;
-            c[2] = q / 64 + bw;
-            fused_load(A, b, c, u);
+            fused_load(A, b, q % 8 + bw, (q / 8) % 8 + bw, q / 64 + bw, u);
         } else {
-            const int r = q - 512, t1 = r % 8, t2 = (r / 8) % 8, depth = (r / 64) % 2, face = r / 128;
+            const int r = q - 512, t1 = r % 8 + bw, t2 = (r / 8) % 8 + bw, depth = (r / 64) % 2, face = r / 128;
             const int ax = face >> 1;
-            c[ax] = (face & 1) ? gnx - bw + depth : depth;
-            c[ax == 0 ? 1 : 0] = t1 + bw;
-            c[ax == 2 ? 1 : 2] = t2 + bw;
-            fused_cell<3>(A, b, c, u);
+            const int n = (face & 1) ? gnx - bw + depth : depth;
+            if (ax == 0)
+                fused_cell<1>(A, b, n, t1, t2, u);
+            else if (ax == 1)
+                fused_cell<1>(A, b, t1, n, t2, u);
+            else
+                fused_cell<1>(A, b, t1, t2, n, u);
         }
         FT w[NF_EULER];
 #pragma unroll
-        for (int l = 0; l < NF_EULER; l++) w[l] = (FT)u[l];
+        for (int l = 0; l < NF_EULER; l++) w[l] = (FT)u.v[l];
         st_to_prim(w);
 #pragma unroll
         for (int l = 0; l < NF_EULER; l++) P[l * CROSS + q] = w[l];
@@ -168,9 +193,15 @@ __device__ __forceinline__ void fused_brick(const FusedArgs& A, int b, int vr, F
     const unsigned char pm = A.pubmask[b];
     double* pubb = A.pub + (size_t)b * 6 * NF_EULER * npen;
     const int* rg = vr >= 0 ? A.vranges + 4 * vr : nullptr;
-    double D[NF_EULER];  // this thread's cell (tid): flux differences, x then y then z
+    double D[2][NF_EULER];  // this thread's cells tid, tid + 256: flux differences, x then y then z
 #pragma unroll
-    for (int l = 0; l < NF_EULER; l++) D[l] = 0.0;
+    for (int h = 0; h < 2; h++)
+#pragma unroll
+        for (int l = 0; l < NF_EULER; l++) D[h][l] = 0.0;
+    // unrolled: the direction is a compile-time constant in each copy, so the
+    // state arrays indexed by it (normal velocity, normal momentum flux) stay
+    // in registers
+#pragma unroll
     for (int d = 0; d < 3; d++) {
         // (b) face fluxes of direction d, one thread per face
         for (int q = tid; q < FACES; q += FUSED_BLOCK) {
@@ -238,12 +269,16 @@ __device__ __forceinline__ void fused_brick(const FusedArgs& A, int b, int vr, F
         __syncthreads();
         // (c) this thread's cell: D -= (F(i+1) - F(i)) / h along d
         {
-            const int x = tid % 8, y = (tid / 8) % 8, z = tid / 64;
-            const int i = d == 0 ? x : (d == 1 ? y : z);
-            const int p = d == 0 ? z * 8 + y : (d == 1 ? z * 8 + x : y * 8 + x);
 #pragma unroll
-            for (int l = 0; l < NF_EULER; l++)
-                D[l] -= (Fs[l * FACES + (i + 1) * npen + p] - Fs[l * FACES + i * npen + p]) * hinv;
+            for (int h = 0; h < 2; h++) {
+                const int cc = tid + h * FUSED_BLOCK;
+                const int x = cc % 8, y = (cc / 8) % 8, z = cc / 64;
+                const int i = d == 0 ? x : (d == 1 ? y : z);
+                const int p = d == 0 ? z * 8 + y : (d == 1 ? z * 8 + x : y * 8 + x);
+#pragma unroll
+                for (int l = 0; l < NF_EULER; l++)
+                    D[h][l] -= (Fs[l * FACES + (i + 1) * npen + p] - Fs[l * FACES + i * npen + p]) * hinv;
+            }
         }
         __syncthreads();
     }
@@ -251,9 +286,11 @@ __device__ __forceinline__ void fused_brick(const FusedArgs& A, int b, int vr, F
     __threadfence();
     __syncthreads();
     if (tid == 0 && pm) atomicExch(A.done + b, A.epoch);
-    // (d) Grid::add_difs (grid.cpp:406-420) for this thread's cell
-    {
-        const int x = tid % 8, y = (tid / 8) % 8, z = tid / 64;
+    // (d) Grid::add_difs (grid.cpp:406-420) for this thread's cells
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+        const int cc = tid + h * FUSED_BLOCK;
+        const int x = cc % 8, y = (cc / 8) % 8, z = cc / 64;
         const int ci = cell_index(gnx, x + bw, y + bw, z + bw);
         const double* U = A.Uin + (size_t)b * g.ucount;
         const double* U0 = A.U0 + (size_t)b * g.ucount;
@@ -261,7 +298,7 @@ __device__ __forceinline__ void fused_brick(const FusedArgs& A, int b, int vr, F
         double u[NF_EULER];
 #pragma unroll
         for (int l = 0; l < NF_EULER; l++) {
-            const double Dl = D[l] + 0.0;  // State::source() is zero for the Euler state
+            const double Dl = D[h][l] + 0.0;  // State::source() is zero for the Euler state
             u[l] = (U[(size_t)l * g.gnx3 + ci] + Dl * A.dt) * A.beta + U0[(size_t)l * g.gnx3 + ci] * (1.0 - A.beta);
         }
         st_floor(u, g.gamma, g.rho_floor, g.ei_floor);

@@ -36,34 +36,32 @@ __device__ __forceinline__ int ld_volatile(const int* p) { return *(const volati
 __device__ __forceinline__ unsigned ld_volatile(const unsigned* p) { return *(const volatile unsigned*)p; }
 
 // Grid-wide barrier of a cooperative launch; false when the solve aborted.
-__device__ __forceinline__ bool grid_sync(GridBarrier* bar) {
+// The arrival counter only grows: barrier k of the launch completes when it
+// reaches k * gridDim.x (target, kept by thread 0), so an arrival is one
+// fire-and-forget release add and the wait one acquire load per poll.
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned& target) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        int good = ld_volatile(&bar->abort) ? 0 : 1;
-        if (good) {
-            const unsigned gen = ld_volatile(&bar->gen);
-            __threadfence();
-            if (atomicAdd(&bar->count, 1u) == gridDim.x - 1) {
-                atomicExch(&bar->count, 0u);
-                __threadfence();
-                atomicAdd(&bar->gen, 1u);
-            } else {
-                unsigned long long spins = 0;
-                while (ld_volatile(&bar->gen) == gen) {
-                    if (ld_volatile(&bar->abort)) {
-                        good = 0;
-                        break;
-                    }
-                    if (++spins > BARRIER_SPINS) {
-                        atomicExch(&bar->abort, 1);
-                        good = 0;
-                        break;
-                    }
-                    if (spins > 64) __nanosleep(32);
-                }
+        int good = 1;
+        target += gridDim.x;
+        __threadfence();
+        asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&bar->count), "r"(1u) : "memory");
+        unsigned long long spins = 0;
+        for (;;) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(&bar->count) : "memory");
+            if ((int)(v - target) >= 0) break;
+            if ((spins & 63) == 63 && ld_volatile(&bar->abort)) {
+                good = 0;
+                break;
             }
-            __threadfence();
+            if (++spins > BARRIER_SPINS) {
+                atomicExch(&bar->abort, 1);
+                good = 0;
+                break;
+            }
+            if (spins > 32) __nanosleep(20);
         }
         ok = good;
     }
@@ -82,10 +80,12 @@ struct Solver {
     int status;
     long long relax_calls;
     int max_outer;
+    unsigned bar_target = 0;    // thread 0: arrivals that complete the next barrier
     unsigned long long t_last;  // block 0: global time at the last barrier exit
-    unsigned long long ph_ns[PH_COUNT];
-    unsigned ph_n[PH_COUNT];
-    double ph_bytes[PH_COUNT];
+    // block 0's phase accounting, in shared memory
+    unsigned long long* ph_ns;
+    unsigned* ph_n;
+    double* ph_bytes;
 
     __device__ static unsigned long long now() {
         unsigned long long t;
@@ -95,7 +95,7 @@ struct Solver {
 
     // barrier closing a phase of class ph
     __device__ bool sync(int ph, int units) {
-        const bool ok = grid_sync(a.bar);
+        const bool ok = grid_sync(a.bar, bar_target);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             const unsigned long long t = now();
             ph_ns[ph] += t - t_last;
@@ -317,12 +317,19 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
     const int max_cycles = *(volatile int*)&a.ctl->max_cycles;
     Solver<CT> s{a, sm, red, nbuf, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0,
                  *(volatile int*)&a.ctl->max_outer};
+    __shared__ unsigned long long s_ph_ns[PH_COUNT];
+    __shared__ unsigned s_ph_n[PH_COUNT];
+    __shared__ double s_ph_bytes[PH_COUNT];
+    s.ph_ns = s_ph_ns;
+    s.ph_n = s_ph_n;
+    s.ph_bytes = s_ph_bytes;
     s.t_last = Solver<CT>::now();
-    for (int p = 0; p < PH_COUNT; p++) {
-        s.ph_ns[p] = 0;
-        s.ph_n[p] = 0;
-        s.ph_bytes[p] = 0.0;
+    if (threadIdx.x < PH_COUNT) {
+        s_ph_ns[threadIdx.x] = 0;
+        s_ph_n[threadIdx.x] = 0;
+        s_ph_bytes[threadIdx.x] = 0.0;
     }
+    __syncthreads();
     int cycles = 0;
     bool ok = true;
     double err = 0.0;
@@ -361,7 +368,7 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
 
 }  // namespace
 
-int solve_persistent_blocks(int precision) {
+int solve_persistent_blocks(int precision, int per_sm_cap) {
     int dev = 0, sms = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
@@ -370,6 +377,7 @@ int solve_persistent_blocks(int precision) {
             ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_persistent<float>, 512, 0)
             : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_persistent<double>, 512, 0);
     if (e != cudaSuccess || per <= 0) return -1;
+    if (per_sm_cap > 0 && per_sm_cap < per) per = per_sm_cap;
     return sms * per;
 }
 

@@ -11,8 +11,8 @@ namespace amr {
 
 // Grid barrier state; zero it before every launch.
 struct GridBarrier {
-    unsigned int count;
-    unsigned int gen;
+    unsigned int count;  // arrivals since the launch began
+    unsigned int pad0;
     int abort;
     int pad;
 };
@@ -43,8 +43,9 @@ struct SolveArgs {
     GridBarrier* bar;
 };
 
-// Blocks of one cooperative launch on the current device (all resident).
-int solve_persistent_blocks(int precision);
+// Blocks of one cooperative launch on the current device (all resident),
+// at most per_sm_cap per SM when per_sm_cap > 0.
+int solve_persistent_blocks(int precision, int per_sm_cap);
 cudaError_t launch_solve_persistent(const SolveArgs& a, int blocks, cudaStream_t s);
 
 }  // namespace amr

@@ -200,8 +200,7 @@ __device__ inline double get_phi_from(const Geom& g, const BrickTable& bt, const
         // PoissonPhysBound::get_phi (poisson_phys_bound.cpp:86-98): the face
         // table indexed by the two transverse indices
         const int ax = face >> 1;
-        const int idx[3] = {i, j, k};
-        const int a = idx[ax == 0 ? 1 : 0], c = idx[ax == 2 ? 1 : 2];
+        const int a = ax == 0 ? j : i, c = ax == 2 ? j : k;
         return aux.bphi[((size_t)b * 6 + face) * pnx * pnx + a * pnx + c];
     }
     if (kind == FACE_REFLECT) {
@@ -256,13 +255,10 @@ __device__ __forceinline__ void op_phi_faces(const Geom& g, const BrickTable& bt
     const int ax = face >> 1;
     for (int t = t0; t < m * m; t += nt) {
         const int t1 = t % m + 1, t2 = t / m + 1;
-        int dst[3], src[3];
-        dst[ax] = (face & 1) ? pnx - 1 : 0;
-        src[ax] = (face & 1) ? 1 : pnx - 2;
-        dst[ax == 0 ? 1 : 0] = src[ax == 0 ? 1 : 0] = t1;
-        dst[ax == 2 ? 1 : 2] = src[ax == 2 ? 1 : 2] = t2;
-        const double v = get_phi_from(g, bt, st, aux, b, face, src[0], src[1], src[2]);
-        st.phi[(size_t)b * g.pnx3 + pidx(pnx, dst[0], dst[1], dst[2])] = v;
+        const int da = (face & 1) ? pnx - 1 : 0, sa = (face & 1) ? 1 : pnx - 2;  // ghost / source layer
+        const int c0 = ax == 0 ? -1 : t1, c1 = ax == 1 ? -1 : (ax == 0 ? t1 : t2), c2 = ax == 2 ? -1 : t2;
+        const double v = get_phi_from(g, bt, st, aux, b, face, c0 < 0 ? sa : c0, c1 < 0 ? sa : c1, c2 < 0 ? sa : c2);
+        st.phi[(size_t)b * g.pnx3 + pidx(pnx, c0 < 0 ? da : c0, c1 < 0 ? da : c1, c2 < 0 ? da : c2)] = v;
     }
 }
 
@@ -275,13 +271,10 @@ __device__ __forceinline__ void op_dphi_faces(const Geom& g, const BrickTable& b
     CT* D = Corr<CT>::dphi(st);
     for (int t = t0; t < m * m; t += nt) {
         const int t1 = t % m + 1, t2 = t / m + 1;
-        int dst[3], src[3];
-        dst[ax] = (face & 1) ? pnx - 1 : 0;
-        src[ax] = (face & 1) ? 1 : pnx - 2;
-        dst[ax == 0 ? 1 : 0] = src[ax == 0 ? 1 : 0] = t1;
-        dst[ax == 2 ? 1 : 2] = src[ax == 2 ? 1 : 2] = t2;
-        const CT v = get_dphi_from<CT>(g, bt, st, aux, b, face, src[0], src[1], src[2]);
-        D[(size_t)b * g.pnx3 + pidx(pnx, dst[0], dst[1], dst[2])] = v;
+        const int da = (face & 1) ? pnx - 1 : 0, sa = (face & 1) ? 1 : pnx - 2;  // ghost / source layer
+        const int c0 = ax == 0 ? -1 : t1, c1 = ax == 1 ? -1 : (ax == 0 ? t1 : t2), c2 = ax == 2 ? -1 : t2;
+        const CT v = get_dphi_from<CT>(g, bt, st, aux, b, face, c0 < 0 ? sa : c0, c1 < 0 ? sa : c1, c2 < 0 ? sa : c2);
+        D[(size_t)b * g.pnx3 + pidx(pnx, c0 < 0 ? da : c0, c1 < 0 ? da : c1, c2 < 0 ? da : c2)] = v;
     }
 }
 

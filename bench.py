@@ -189,7 +189,7 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
     """
     prec = amr.PREC_MIXED if form == "mixed" else amr.PREC_FP64
     a = amr.AMR(physics=amr.PHYSICS_EULER_GRAVITY, max_refine_level=LEVELS, grid_dim=0.5, z_reflect=0,
-                max_bricks=8192, precision=prec, persistent_solve=1 if form in ("persistent", "mixed") else 0)
+                max_bricks=8192, precision=prec, persistent_solve=2 if form in ("persistent", "mixed") else 0)
     ini.build_tree(a, "polytrope", 1.0e-6, 0.5, 0, LEVELS, device=True)
     stream = torch.cuda.ExternalStream(a.stream_handle())
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
@@ -588,7 +588,7 @@ def run_case(case):
     amr, ini = load_amr()
     if case == "solve_L3":
         a = amr.AMR(physics=amr.PHYSICS_EULER_GRAVITY, max_refine_level=3, grid_dim=0.5, z_reflect=0,
-                    max_bricks=2048, precision=amr.PREC_MIXED, persistent_solve=1)
+                    max_bricks=2048, precision=amr.PREC_MIXED, persistent_solve=2)
         ini.build_tree(a, "polytrope", 1.0e-6, 0.5, 0, 3, device=True)
         err, cyc = a.graph_solve(1e-6, 1000)
         a.synchronize()

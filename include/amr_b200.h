@@ -60,8 +60,9 @@ typedef struct amr_config {
     int min_level;        /* MINLEVEL (defs.h:22) */
     int min_grid_life;    /* MIN_GRID_LIFE (defs.h:23) */
     int max_bricks;       /* device brick pool capacity; 0 = host-only context */
-    int persistent_solve; /* 1: the graph forms run each Poisson solve's V-cycle loop as one
-                             persistent cooperative kernel (same results bit for bit) */
+    int persistent_solve; /* > 0: the graph forms run each Poisson solve's V-cycle loop as one
+                             persistent cooperative kernel (same results bit for bit), with
+                             at most this many blocks per SM */
     double grid_dim;      /* GRID_DIM */
     double origin[3];     /* Grid::origin (grid/grid.h:23) */
     double minmod_theta;  /* MINMOD_THETA (euler_defs.h:21) */
