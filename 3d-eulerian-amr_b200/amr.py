@@ -31,7 +31,7 @@ class AmrConfig(ctypes.Structure):
         ("bw", ctypes.c_int), ("nx", ctypes.c_int), ("nf", ctypes.c_int), ("physics", ctypes.c_int),
         ("precision", ctypes.c_int), ("z_reflect", ctypes.c_int), ("mirror_refine_y", ctypes.c_int),
         ("max_refine_level", ctypes.c_int), ("min_level", ctypes.c_int), ("min_grid_life", ctypes.c_int),
-        ("max_bricks", ctypes.c_int), ("persistent_solve", ctypes.c_int),
+        ("max_bricks", ctypes.c_int), ("persistent_solve", ctypes.c_int), ("reconstruction", ctypes.c_int),
         ("grid_dim", ctypes.c_double), ("origin", ctypes.c_double * 3), ("minmod_theta", ctypes.c_double),
         ("cfl", ctypes.c_double), ("gamma", ctypes.c_double), ("rho_floor", ctypes.c_double),
         ("ei_floor", ctypes.c_double), ("maxdtinc", ctypes.c_double), ("grav_g", ctypes.c_double),

@@ -467,8 +467,11 @@ int amr_default_config(amr_config* cfg) {
 int amr_create(const amr_config* cfg, amr_ctx** out) {
     if (!cfg || !out) return AMR_ERR_ARG;
     *out = nullptr;
-    if (cfg->nf != 6 || cfg->bw != 2 || cfg->nx < 4 || (cfg->nx % 4) != 0 || cfg->max_refine_level < 0 ||
-        cfg->max_refine_level > 12 || cfg->max_bricks < 0)
+    // minmod reads cells f-2..f+1 of face f (bw >= 2), PPM cells f-3..f+2 (bw >= 3)
+    const int min_bw = cfg->reconstruction == AMR_RECON_PPM ? 3 : 2;
+    if (cfg->nf != 6 || cfg->bw < min_bw || cfg->bw > 4 || cfg->nx < 4 || (cfg->nx % 4) != 0 ||
+        cfg->max_refine_level < 0 || cfg->max_refine_level > 12 || cfg->max_bricks < 0 ||
+        (cfg->reconstruction != AMR_RECON_MINMOD && cfg->reconstruction != AMR_RECON_PPM))
         return AMR_ERR_ARG;
     TreeParams tp;
     tp.bw = cfg->bw;
@@ -491,6 +494,7 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
     g.ucount = g.nf * g.gnx3;
     g.z_reflect = cfg->z_reflect;
     g.precision = cfg->precision;
+    g.recon = cfg->reconstruction;
     g.grid_dim = cfg->grid_dim;
     g.h0 = tp.h0;
     for (int d = 0; d < 3; d++) g.origin[d] = cfg->origin[d];
@@ -939,6 +943,10 @@ int amr_fused_sub_step(amr_ctx* c, double dt, double beta, int blocks_per_sm) {
     NEED_DEVICE(c);
     if (c->cfg.physics != AMR_PHYSICS_EULER || c->geom.nf != 6) {
         c->err = "fused substep: Euler physics without gravity only";
+        return AMR_ERR_ARG;
+    }
+    if (c->geom.bw != 2 || c->geom.recon != AMR_RECON_MINMOD) {
+        c->err = "fused substep: minmod reconstruction with bw 2 only";
         return AMR_ERR_ARG;
     }
     TRY(fused_setup(c));

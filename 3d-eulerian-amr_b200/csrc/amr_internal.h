@@ -23,6 +23,7 @@ struct Geom {
     int gnx3, pnx3, ucount;  // gnx^3, pnx^3, nf*gnx^3
     int z_reflect;
     int precision;  // AMR_PREC_FP64 / AMR_PREC_MIXED
+    int recon;      // AMR_RECON_MINMOD / AMR_RECON_PPM (same values as RECON_* in recon.cuh)
     double grid_dim, h0;
     double origin[3];
     double theta, cfl, gamma, rho_floor, ei_floor, grav_g;

@@ -97,12 +97,13 @@ __global__ void k_ghost_fill(Geom g, BrickTable bt, DevState st, const int* __re
 
 // ---------------------------------------------------------------------------
 // KT/Rusanov fluxes, Grid::compute_{x,y,z}_flux (grid.cpp:215-302) with
-// minmod-theta reconstruction (reconstruct.cpp:60-71).  Block = one brick,
-// 3*nx*nx threads: thread = (direction, pencil).  A pencil walks its GNX
-// cells keeping a four-cell window of primitives.
+// minmod-theta (reconstruct.cpp:60-71) or PPM (reconstruct.cpp:22-58)
+// reconstruction.  Block = one brick, 3*nx*nx threads: thread = (direction,
+// pencil).  A pencil walks its GNX cells streaming the reconstruction.
 // ---------------------------------------------------------------------------
-__global__ void k_flux_minmod(Geom g, DevState st, const int* __restrict__ slots) {
-    flux_pencils<double>(g, st, slots[blockIdx.x]);
+template <int R>
+__global__ void k_flux(Geom g, DevState st, const int* __restrict__ slots) {
+    flux_pencils<double, R>(g, st, slots[blockIdx.x]);
 }
 
 // ---------------------------------------------------------------------------
@@ -323,62 +324,21 @@ __global__ void k_prolong(Geom g, BrickTable bt, DevState st, const int* __restr
 // CFL time step, Grid::max_dt (grid.cpp:422-483): largest face eigenvalue of
 // the reconstructed states over all three directions; per-brick dt out.
 // ---------------------------------------------------------------------------
+template <int R>
 __global__ void k_max_dt(Geom g, DevState st, const int* __restrict__ slots, const double* __restrict__ hs,
                          double* __restrict__ dt_out) {
     const int b = slots[blockIdx.x];
-    const int nx = g.nx, gnx = g.gnx, bw = g.bw, npen = nx * nx;
+    const int npen = g.nx * g.nx;
     __shared__ double red[32];
     double lam = 0.0;
     for (int t = threadIdx.x; t < 3 * npen; t += blockDim.x) {
         const int d = t / npen, p = t % npen;
-        const int t1 = p % nx, t2 = p / nx;
-        const double* U = st.U + (size_t)b * g.ucount;
-        int stride, base;
-        if (d == 0) {
-            stride = 1;
-            base = cell_index(gnx, 0, t1 + bw, t2 + bw);
-        } else if (d == 1) {
-            stride = gnx;
-            base = cell_index(gnx, t1 + bw, 0, t2 + bw);
-        } else {
-            stride = gnx * gnx;
-            base = cell_index(gnx, t1 + bw, t2 + bw, 0);
-        }
-        double w[4][NF_EULER];
-        for (int n = 0; n < 3; n++) {
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) w[n + 1][l] = U[l * g.gnx3 + base + n * stride];
-            st_to_prim(w[n + 1]);
-        }
-        for (int n = 3; n < bw + 1; n++) {
-            for (int m = 0; m < 3; m++)
-                for (int l = 0; l < NF_EULER; l++) w[m][l] = w[m + 1][l];
-            for (int l = 0; l < NF_EULER; l++) w[3][l] = U[l * g.gnx3 + base + n * stride];
-            st_to_prim(w[3]);
-        }
-        double sR[NF_EULER];
-#pragma unroll
-        for (int l = 0; l < NF_EULER; l++) sR[l] = minmod_theta(w[3][l] - w[2][l], w[2][l] - w[1][l], g.theta);
-        for (int f = bw; f <= gnx - bw; f++) {
-#pragma unroll
-            for (int m = 0; m < 3; m++)
-#pragma unroll
-                for (int l = 0; l < NF_EULER; l++) w[m][l] = w[m + 1][l];
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) w[3][l] = U[l * g.gnx3 + base + (f + 1) * stride];
-            st_to_prim(w[3]);
-            double ql[NF_EULER], qr[NF_EULER];
-#pragma unroll
-            for (int l = 0; l < NF_EULER; l++) {
-                const double sL = sR[l];
-                sR[l] = minmod_theta(w[3][l] - w[2][l], w[2][l] - w[1][l], g.theta);
-                ql[l] = w[1][l] + sL / 2.0;
-                qr[l] = w[2][l] - sR[l] / 2.0;
-            }
-            st_to_con(ql);
-            st_to_con(qr);
-            lam = r_max(lam, r_max(st_eigen(ql, d, g.gamma), st_eigen(qr, d, g.gamma)));
-        }
+        if (d == 0)
+            lam = max_eigen_pencil<0, R>(g, st, b, p, lam);
+        else if (d == 1)
+            lam = max_eigen_pencil<1, R>(g, st, b, p, lam);
+        else
+            lam = max_eigen_pencil<2, R>(g, st, b, p, lam);
     }
     // block max (max is exact, order-free)
     for (int o = 16; o > 0; o >>= 1) lam = r_max(lam, __shfl_xor_sync(0xffffffffu, lam, o));
@@ -456,7 +416,10 @@ void launch_flux(const Geom& g, const DevState& st, const int* slots, int n, cud
         launch_flux_f32(g, st, slots, n, s);
         return;
     }
-    launch_k(k_flux_minmod, n, 3 * g.nx * g.nx, 0, s, g, st, slots);
+    if (g.recon == RECON_PPM)
+        launch_k(k_flux<RECON_PPM>, n, 3 * g.nx * g.nx, 0, s, g, st, slots);
+    else
+        launch_k(k_flux<RECON_MINMOD>, n, 3 * g.nx * g.nx, 0, s, g, st, slots);
 }
 void launch_reflux(const Geom& g, const DevState& st, const RefluxItem* items, int n, cudaStream_t s) {
     if (n <= 0) return;
@@ -487,7 +450,10 @@ void launch_prolong(const Geom& g, const BrickTable& bt, const DevState& st, con
 void launch_max_dt(const Geom& g, const DevState& st, const int* slots, int n, const double* hs, double* dt_out,
                    cudaStream_t s) {
     if (n <= 0) return;
-    launch_k(k_max_dt, n, 192, 0, s, g, st, slots, hs, dt_out);
+    if (g.recon == RECON_PPM)
+        launch_k(k_max_dt<RECON_PPM>, n, 192, 0, s, g, st, slots, hs, dt_out);
+    else
+        launch_k(k_max_dt<RECON_MINMOD>, n, 192, 0, s, g, st, slots, hs, dt_out);
 }
 void launch_refine_flags(const Geom& g, const DevState& st, const int* slots, int n, double thr,
                          unsigned char* flags, cudaStream_t s) {

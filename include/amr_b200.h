@@ -43,6 +43,9 @@ extern "C" {
 #define AMR_PHYSICS_EULER 0         /* euler/state.cpp, no gravity */
 #define AMR_PHYSICS_EULER_GRAVITY 1 /* Euler state + Poisson self-gravity */
 
+#define AMR_RECON_MINMOD 0 /* Reconstruct::minmod (reconstruct.cpp:60-71), the EULER build */
+#define AMR_RECON_PPM 1    /* Reconstruct::ppm (reconstruct.cpp:22-58), PPM builds; needs bw >= 3 */
+
 #define AMR_PREC_FP64 0  /* plain form: FP64 throughout, reference operation order */
 #define AMR_PREC_MIXED 1 /* FP32 flux/smoother inside FP64 state and defect correction */
 
@@ -63,6 +66,7 @@ typedef struct amr_config {
     int persistent_solve; /* > 0: the graph forms run each Poisson solve's V-cycle loop as one
                              persistent cooperative kernel (same results bit for bit), with
                              at most this many blocks per SM */
+    int reconstruction;   /* AMR_RECON_*: the PPM switch of euler_defs.h:24 (reconstruct.cpp:92-102) */
     double grid_dim;      /* GRID_DIM */
     double origin[3];     /* Grid::origin (grid/grid.h:23) */
     double minmod_theta;  /* MINMOD_THETA (euler_defs.h:21) */

@@ -210,10 +210,45 @@ def enforce_boundaries(T, U):
 # ---------------------------------------------------------------------------
 # fluxes (grid.cpp:215-302, reconstruct.cpp:60-71) and corrections
 # ---------------------------------------------------------------------------
-def brick_fluxes(Ub, bw, theta, gamma):
+def ppm_faces(q, bw):
+    """Left and right states of faces bw..gnx-bw of pencils q[..., gnx]
+    (primitives along the last axis): Reconstruct::ppm
+    (reconstruct.cpp:22-58) as Reconstruct::operator() calls it,
+    ppm(q0, qr, ql) (reconstruct.cpp:94).  Inside ppm the array named qr
+    holds the interface to the right of cell i, ql the one to its left; after
+    the monotonisation the right edges are shifted up one cell (:55-57), so
+    the caller's ql[f] is the right edge of cell f-1 and its qr[f] the left
+    edge of cell f.  The Euler state has no low-order or smooth field
+    (euler/state.h:37-42), so every field is treated alike."""
+    n = q.shape[-1]
+    six = 1.0 / 6.0
+    s = np.zeros_like(q)
+    s[..., 1:-1] = minmod_theta(q[..., 2:] - q[..., 1:-1], q[..., 1:-1] - q[..., :-2], 2.0)
+    # interface to the right of cell i, i = 1..n-3
+    I = np.zeros_like(q)
+    I[..., 1:n - 2] = (q[..., 1:n - 2] + q[..., 2:n - 1]) * 0.5
+    I[..., 1:n - 2] = I[..., 1:n - 2] + (s[..., 1:n - 2] - s[..., 2:n - 1]) * six
+    # Colella-Woodward monotonisation of cells 2..n-3 (edges L = I[i-1], R = I[i])
+    c = q[..., 2:n - 2]
+    L = I[..., 1:n - 3]
+    R = I[..., 2:n - 2]
+    tmp1 = R - L
+    tmp2 = R + L
+    flat = (R - c) * (c - L) <= 0.0
+    steep_l = tmp1 * (c - 0.5 * tmp2) > six * tmp1 * tmp1
+    steep_r = -six * tmp1 * tmp1 > tmp1 * (c - 0.5 * tmp2)
+    Lm = np.where(flat, c, np.where(steep_l, 3.0 * c - 2.0 * R, L))
+    Rm = np.where(flat, c, np.where(~steep_l & steep_r, 3.0 * c - 2.0 * L, R))
+    # Lm/Rm index m holds cell m + 2; face f: left = Rm[f-1], right = Lm[f]
+    f = np.arange(bw, n - bw + 1)
+    return Rm[..., f - 3], Lm[..., f - 2]
+
+
+def brick_fluxes(Ub, bw, theta, gamma, recon="minmod"):
     """Face fluxes of one brick: F[d] of shape (nf, nx+1, nx, nx) indexed
     (field, face along d, lower transverse, higher transverse), and the max
-    face eigenvalue (Grid::max_dt's inner max)."""
+    face eigenvalue (Grid::max_dt's inner max).  recon: "minmod"
+    (reconstruct.cpp:60-71) or "ppm" (reconstruct.cpp:22-58, needs bw >= 3)."""
     gnx = Ub.shape[-1]
     nx = gnx - 2 * bw
     out, lam = [], 0.0
@@ -226,11 +261,14 @@ def brick_fluxes(Ub, bw, theta, gamma):
         else:
             V = np.transpose(Ub[:, :, bw:-bw, bw:-bw], (0, 2, 3, 1))
         q = to_prim(V)
-        s = np.zeros_like(q)
-        s[..., 1:-1] = minmod_theta(q[..., 2:] - q[..., 1:-1], q[..., 1:-1] - q[..., :-2], theta)
-        f = np.arange(bw, gnx - bw + 1)
-        ql = q[..., f - 1] + s[..., f - 1] / 2.0
-        qr = q[..., f] - s[..., f] / 2.0
+        if recon == "ppm":
+            ql, qr = ppm_faces(q, bw)
+        else:
+            s = np.zeros_like(q)
+            s[..., 1:-1] = minmod_theta(q[..., 2:] - q[..., 1:-1], q[..., 1:-1] - q[..., :-2], theta)
+            f = np.arange(bw, gnx - bw + 1)
+            ql = q[..., f - 1] + s[..., f - 1] / 2.0
+            qr = q[..., f] - s[..., f] / 2.0
         ql, qr = to_con(ql), to_con(qr)
         fl, al = flux_eigen(ql, d, gamma)
         fr, ar = flux_eigen(qr, d, gamma)
@@ -328,11 +366,11 @@ def inject_from_children(T, U, gamma):
     return U
 
 
-def max_dt(T, U, theta, gamma, cfl):
+def max_dt(T, U, theta, gamma, cfl, recon="minmod"):
     """Grid::max_dt per brick and GridNode::max_dt's recursion."""
     own = np.zeros(T.n)
     for i in range(T.n):
-        _, lam = brick_fluxes(U[i], T.bw, theta, gamma)
+        _, lam = brick_fluxes(U[i], T.bw, theta, gamma, recon)
         dtinv = lam / T.h[i]
         if dtinv == 0.0:
             dtinv = 1.0e-10
@@ -352,19 +390,19 @@ def max_dt(T, U, theta, gamma, cfl):
     return rec(0)
 
 
-def sub_step(T, U, U0, dt, beta, theta=1.3, gamma=5.0 / 3.0):
+def sub_step(T, U, U0, dt, beta, theta=1.3, gamma=5.0 / 3.0, recon="minmod"):
     """HydroDriver::sub_step (euler/hydro_driver.cpp:200-214) without
     regrid; returns the updated U."""
     U = enforce_boundaries(T, U)
-    F = [brick_fluxes(U[i], T.bw, theta, gamma)[0] for i in range(T.n)]
+    F = [brick_fluxes(U[i], T.bw, theta, gamma, recon)[0] for i in range(T.n)]
     F = reflux(T, F)
     return add_difs(T, U, U0, F, dt, beta, gamma)
 
 
-def step(T, U, dt, theta=1.3, gamma=5.0 / 3.0):
+def step(T, U, dt, theta=1.3, gamma=5.0 / 3.0, recon="minmod"):
     """HydroDriver::step (euler/hydro_driver.cpp:171-194) on a fixed tree."""
     U0 = U.copy()
     for beta in (1.0, 0.25, 2.0 / 3.0):
-        U = sub_step(T, U, U0, dt, beta, theta, gamma)
+        U = sub_step(T, U, U0, dt, beta, theta, gamma, recon)
         U = inject_from_children(T, U, gamma)
     return enforce_boundaries(T, U)

@@ -19,6 +19,9 @@ Variants:
   g05  EULER physics, GRID_DIM 0.5, no Z_REFLECT  (unit cube [-0.5,0.5]^3)
   zr   EULER physics, GRID_DIM 1.0, Z_REFLECT     (the reference's stock
        euler/euler_defs.h domain: x,y in [-1,1], z in [0,2] mirrored at z=0)
+  ppm  g05 with PPM reconstruction (euler_defs.h:24 switched on) and BW 3,
+       the ghost width PPM needs (reconstruct.cpp:22-58 reads cells i-3..i+2
+       of face i)
 
 Run:  python oracle/build_ref.py [--reference /root/reference]
 When the reference tree is absent (e.g. on a GPU box) this is a no-op and the
@@ -66,9 +69,12 @@ def _patch(src, variant):
     # defs.h:4 hard-codes the BINARY driver; select the Euler state.
     _replace(os.path.join(src, "defs.h"), "#define BINARY", "#define EULER")
     defs = os.path.join(src, "euler", "euler_defs.h")
-    if variant == "g05":
+    if variant in ("g05", "ppm"):
         _replace(defs, "#define GRID_DIM            (1.0)", "#define GRID_DIM            (0.5)")
         _replace(defs, "#define Z_REFLECT\n", "\n")
+    if variant == "ppm":
+        _replace(defs, "//#define PPM\n", "#define PPM\n")
+        _replace(defs, "#define BW \t\t\t\t\t(2)", "#define BW \t\t\t\t\t(3)")
     # euler/initialize.cpp:26,34 does not compile (r_outer undefined); the
     # harness defines initialize(GridNode*) instead.
     with open(os.path.join(src, "euler", "initialize.cpp"), "w") as f:
@@ -146,7 +152,7 @@ def build_helm(reference):
     return exe
 
 
-def build(reference="/root/reference", variants=("g05", "zr")):
+def build(reference="/root/reference", variants=("g05", "zr", "ppm")):
     if not os.path.isdir(reference):
         print("[oracle] reference tree not present; using prebuilt oracle/_ref binaries")
         return []

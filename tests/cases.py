@@ -15,7 +15,14 @@ DT_RTOL = 1.0e-13
 VARIANTS = {
     "g05": dict(grid_dim=0.5, z_reflect=0),
     "zr": dict(grid_dim=1.0, z_reflect=1),
+    # PPM reconstruction (reconstruct.cpp:22-58) with BW 3, unit cube
+    "ppm": dict(grid_dim=0.5, z_reflect=0, bw=3, reconstruction=1),
 }
+
+
+def oracle_recon(variant):
+    """Reconstruction name of amr_oracle for a variant."""
+    return "ppm" if VARIANTS[variant].get("reconstruction", 0) == 1 else "minmod"
 
 
 def load_golden(name):

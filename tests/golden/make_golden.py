@@ -28,16 +28,19 @@ CASES = {
     "hydro_bump_L2": ("g05", "hydro", ["bump", 2, 5, 3.0]),
     "hydro_bump_L3": ("g05", "hydro", ["bump", 3, 4, 3.0]),
     "hydro_bump_zr_L3": ("zr", "hydro", ["bump", 3, 4, 3.0]),
+    "hydro_ppm_bump_L2": ("ppm", "hydro", ["bump", 2, 5, 3.0]),
+    "hydro_ppm_blast_L2": ("ppm", "hydro", ["blast", 2, 20, 1e-6]),
     "poisson_poly_L2": ("g05", "poisson", ["polytrope", 2, 4]),
     "poisson_poly_L3": ("g05", "poisson", ["polytrope", 3, 3]),
     "grav_poly_L2": ("g05", "grav", ["polytrope", 2, 3, 1e-6]),
+    "grav_ppm_poly_L2": ("ppm", "grav", ["polytrope", 2, 3, 1e-6]),
 }
 # cases whose full state would make a large fixture keep only the tree and
 # per-brick, per-field sums and absolute sums of the interior cells
-SUMMARY_ONLY = {"hydro_blast_L2", "hydro_bump_L3", "poisson_poly_L3"}
+SUMMARY_ONLY = {"hydro_blast_L2", "hydro_bump_L3", "poisson_poly_L3", "hydro_ppm_blast_L2"}
 # for these the final conserved state is kept as sums only (the potential in
 # full): the initial state is needed in full to start from the same data
-FINAL_SUMMARY = {"grav_poly_L2"}
+FINAL_SUMMARY = {"grav_poly_L2", "grav_ppm_poly_L2"}
 
 
 def interior(d, U):

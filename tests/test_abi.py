@@ -41,3 +41,21 @@ def test_host_only_context_rejects_device_calls():
         assert e.code == -8
     else:
         raise AssertionError("device call on a host-only context must fail")
+
+
+def test_config_checks_reconstruction_and_ghost_width():
+    """PPM reads cells f-3..f+2 of face f (reconstruct.cpp:22-58), so it needs
+    bw >= 3; minmod needs bw >= 2; unknown reconstructions are rejected."""
+    from conftest import load_amr
+    amr = load_amr()
+    for kw in (dict(reconstruction=1, bw=2), dict(reconstruction=2, bw=3), dict(bw=1), dict(bw=5)):
+        try:
+            amr.AMR(max_bricks=0, **kw)
+        except amr.AmrError as e:
+            assert e.code == -1, kw
+        else:
+            raise AssertionError("config accepted: %r" % kw)
+    for kw in (dict(reconstruction=1, bw=3), dict(reconstruction=0, bw=3), dict(reconstruction=1, bw=4)):
+        a = amr.AMR(max_bricks=0, **kw)
+        assert a.gnx == 8 + 2 * kw["bw"]
+        a.close()

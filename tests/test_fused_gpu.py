@@ -43,7 +43,8 @@ def rk3(a, dt, fused, blocks_per_sm=0):
 
 
 def interior(a):
-    return a.download_state()[:, :, 2:-2, 2:-2, 2:-2]
+    b = a.bw
+    return a.download_state()[:, :, b:-b, b:-b, b:-b]
 
 
 @pytest.mark.gpu
@@ -83,3 +84,17 @@ def test_fused_mixed_close_to_fp64(gpu):
             assert np.abs(u32[:, f] - u64[:, f]).max() <= FLUX_RTOL * scale, f
     a.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_fused_rejects_ppm(gpu):
+    """The fused substep is written for the minmod brick (bw 2); a PPM
+    context gets AMR_ERR_ARG instead of a wrong answer."""
+    g = load_golden("hydro_ppm_bump_L2")
+    a = make(gpu, "ppm", int(g["init_level"].max()))
+    load_state(a, g)
+    a.store()
+    with pytest.raises(gpu.AmrError) as e:
+        a.fused_sub_step(a.max_dt(), 1.0, 0)
+    assert e.value.code == -1
+    a.close()

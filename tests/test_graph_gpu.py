@@ -14,15 +14,16 @@ import pytest
 from cases import VARIANTS, load_golden, same_tree
 
 
-def make(gpu, maxlevel, persistent=0):
+def make(gpu, maxlevel, persistent=0, variant="g05"):
     return gpu.AMR(max_refine_level=maxlevel, max_bricks=2048, physics=gpu.PHYSICS_EULER_GRAVITY,
-                   persistent_solve=persistent, **VARIANTS["g05"])
+                   persistent_solve=persistent, **VARIANTS[variant])
 
 
 def load_state(a, g):
     a.load_tree(g["init_level"], g["init_loc"], g["init_age"])
     U = np.zeros((a.nbricks, a.nf, a.gnx, a.gnx, a.gnx))
-    U[:, :, 2:-2, 2:-2, 2:-2] = g["init_U"]
+    b = a.bw
+    U[:, :, b:-b, b:-b, b:-b] = g["init_U"]
     a.upload_state(U)
     a.enforce_boundaries()
 
@@ -70,16 +71,19 @@ def test_graph_grav_steps_are_bitwise_plain(gpu, persistent):
 
 
 @pytest.mark.gpu
-def test_graph_steps_match_reference(gpu):
-    """The reference's 3-step coupled run, replayed through the graph form."""
-    g = load_golden("grav_poly_L2")
-    a = make(gpu, 2)
+@pytest.mark.parametrize("name", ["grav_poly_L2", "grav_ppm_poly_L2"])
+def test_graph_steps_match_reference(gpu, name):
+    """The reference's 3-step coupled run, replayed through the graph form
+    (minmod with BW 2, and PPM with BW 3)."""
+    g = load_golden(name)
+    a = make(gpu, 2, variant=str(g["variant"]))
     load_state(a, g)
     dts = [a.graph_grav_step(1.0e-6, 1.0e6, s) for s in range(3)]
     n = int(g["extra"][0])
     np.testing.assert_allclose(dts, g["extra"][1:1 + n], rtol=1e-13)
     assert same_tree(a.get_tree(), g, "final_")
-    U = a.download_state()[:, :, 2:-2, 2:-2, 2:-2]
+    b = a.bw
+    U = a.download_state()[:, :, b:-b, b:-b, b:-b]
     s = U.reshape(U.shape[0], U.shape[1], -1).sum(axis=2)
     rel = np.abs(s - g["final_Usum"]) / np.maximum(g["final_Uabs"], 1e-300)
     assert rel.max() <= 1e-11

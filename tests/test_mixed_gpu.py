@@ -55,17 +55,19 @@ def test_mixed_solve_and_steps_close_to_fp64(gpu):
 
 
 @pytest.mark.gpu
-def test_mixed_flux_matches_fp64_to_single_precision(gpu):
+@pytest.mark.parametrize("recon,bw", [(0, 2), (1, 3)])
+def test_mixed_flux_matches_fp64_to_single_precision(gpu, recon, bw):
     """One hydro RK3 step of the blast problem with FP32 fluxes: every field
-    within FLUX_RTOL (relative to its maximum) of the FP64 step."""
+    within FLUX_RTOL (relative to its maximum) of the FP64 step; minmod and
+    PPM reconstruction."""
     out = {}
     for prec in (gpu.PREC_FP64, gpu.PREC_MIXED):
         a = gpu.AMR(physics=gpu.PHYSICS_EULER, max_refine_level=2, grid_dim=0.5, z_reflect=0, max_bricks=512,
-                    precision=prec)
+                    precision=prec, reconstruction=recon, bw=bw)
         initial.build_tree(a, "blast", 1e-6, 0.5, 0, 2, device=True)
         dt = a.max_dt()
         a.hydro_step(dt, 1e-6)
-        out[prec] = a.download_state()[:, :, 2:-2, 2:-2, 2:-2]
+        out[prec] = a.download_state()[:, :, bw:-bw, bw:-bw, bw:-bw]
         a.close()
     u64, u32 = out[gpu.PREC_FP64], out[gpu.PREC_MIXED]
     assert u64.shape == u32.shape

@@ -36,13 +36,13 @@ def test_tree_build_matches_reference(name):
     assert np.array_equal(t["age"], g["init_age"])
 
 
-@pytest.mark.parametrize("name", ["poisson_poly_L2", "poisson_poly_L3", "grav_poly_L2"])
+@pytest.mark.parametrize("name", ["poisson_poly_L2", "poisson_poly_L3", "grav_poly_L2", "grav_ppm_poly_L2"])
 def test_polytrope_tree_matches_reference(name):
     """The oracle harness builds gravity trees at min_refine_density 1e-6."""
     amr = load_amr()
     g = load_golden(name)
     maxlevel = int(g["args"][1])
-    a = amr.AMR(max_bricks=0, max_refine_level=maxlevel, grid_dim=0.5, z_reflect=0)
+    a = amr.AMR(max_bricks=0, max_refine_level=maxlevel, **VARIANTS[str(g["variant"])])
     initial.build_tree(a, "polytrope", 1.0e-6, 0.5, 0, maxlevel, device=False)
     assert same_tree(a.get_tree(), g, "init_")
 
