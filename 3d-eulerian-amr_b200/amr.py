@@ -17,6 +17,9 @@ LIB_PATH = os.path.join(HERE, "lib", "libamr_b200.so")
 
 PHYSICS_EULER = 0
 PHYSICS_EULER_GRAVITY = 1
+PHYSICS_ZTWD = 2
+RECON_MINMOD = 0
+RECON_PPM = 1
 PREC_FP64 = 0
 PREC_MIXED = 1
 
@@ -102,6 +105,11 @@ def load_library(path=LIB_PATH):
             lib.amr_grav_step.argtypes = [P, D, D, D, I]
             lib.amr_graph_solve.argtypes = [P, D, I, dp, ip]
             lib.amr_graph_grav_step.argtypes = [P, D, D, I, dp]
+        if hasattr(lib, "amr_ztwd_step"):
+            lib.amr_ztwd_set_eos.argtypes = [P, P]
+            lib.amr_ztwd_set_frame.argtypes = [P, D, D, D, D]
+            lib.amr_ztwd_pot.argtypes = [P, I]
+            lib.amr_ztwd_step.argtypes = [P, D, D, D, I, dp]
         if hasattr(lib, "amr_solve_phases"):
             lib.amr_solve_phases.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong), dp, I]
             lib.amr_solve_last_ms.argtypes = [P, ctypes.POINTER(ctypes.c_float)]
@@ -369,3 +377,24 @@ class AMR:
     def grav_step(self, dt, tol, dynamic_range=1.0e6, step_index=0):
         self._check(self.lib.amr_grav_step(self.ctx, float(dt), float(tol), float(dynamic_range),
                                            int(step_index)))
+
+    # ---- ZTWD binary (AMR_PHYSICS_ZTWD) -------------------------------------
+    def ztwd_set_eos(self, helm):
+        """Table and code units of a helm.Helm context (kept alive here)."""
+        self._helm = helm
+        self._check(self.lib.amr_ztwd_set_eos(self.ctx, helm.ctx))
+
+    def ztwd_set_frame(self, omega, omega0, fR=0.0, ftheta=0.0):
+        self._check(self.lib.amr_ztwd_set_frame(self.ctx, float(omega), float(omega0), float(fR), float(ftheta)))
+
+    def ztwd_pot(self, mode):
+        """0 pot_to_grid, 1 pot_from_grid, 2 add_pot_et, 3 sub_pot_et (binary.cpp:825-936)."""
+        self._check(self.lib.amr_ztwd_pot(self.ctx, int(mode)))
+
+    def ztwd_step(self, dt, tol, dynamic_range=1.0e6, step_index=0):
+        """BinaryDriver::step; returns the step taken (after MAXDTINC retries)."""
+        used = ctypes.c_double()
+        self._check(self.lib.amr_ztwd_step(self.ctx, float(dt), float(tol), float(dynamic_range), int(step_index),
+                                           ctypes.byref(used)))
+        return used.value
+

@@ -223,7 +223,7 @@ int rebuild_topology(amr_ctx* c) {
                 }
         }
         c->n_bfaces = (int)bf.size() / 2;
-        if (c->cfg.physics == AMR_PHYSICS_EULER_GRAVITY) {
+        if (has_gravity(c)) {
             if ((int)bf.size() > c->bfaces_cap) {
                 if (c->d_bfaces) cudaFree(c->d_bfaces);
                 c->bfaces_cap = (int)bf.size() * 2 + 64;
@@ -378,10 +378,15 @@ int finish_refine(amr_ctx* c) {
     CUDA_TRY(cudaMemcpyAsync(d, slots.data(), sizeof(int) * slots.size(), cudaMemcpyHostToDevice, c->stream));
     {
         ProfScope ps_(c->prof, KC_PROLONG, c->stream);
-        launch_prolong(c->geom, c->bt, c->st, d, (int)slots.size(), c->stream);
+        if (is_ztwd(c))
+            launch_zt_prolong(c->geom, c->bt, c->st, c->zpar, d, (int)slots.size(), c->d_zerr, c->stream);
+        else
+            launch_prolong(c->geom, c->bt, c->st, d, (int)slots.size(), c->stream);
     }
-    if (c->cfg.physics == AMR_PHYSICS_EULER_GRAVITY)
+    if (has_gravity(c))
         launch_poisson_new_bricks(c->geom, c->bt, c->st, d, (int)slots.size(), c->stream);
+    if (is_ztwd(c))  // Binary::inject_from_parent: then pot_from_grid (binary.cpp:852-855)
+        launch_zt_pot(c->geom, c->bt, c->st, c->zpar, d, (int)slots.size(), 1, c->stream);
     TRY(check_launch(c));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     cudaFree(d);
@@ -469,7 +474,11 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
     *out = nullptr;
     // minmod reads cells f-2..f+1 of face f (bw >= 2), PPM cells f-3..f+2 (bw >= 3)
     const int min_bw = cfg->reconstruction == AMR_RECON_PPM ? 3 : 2;
-    if (cfg->nf != 6 || cfg->bw < min_bw || cfg->bw > 4 || cfg->nx < 4 || (cfg->nx % 4) != 0 ||
+    const bool ztwd = cfg->physics == AMR_PHYSICS_ZTWD;
+    if (cfg->physics < AMR_PHYSICS_EULER || cfg->physics > AMR_PHYSICS_ZTWD ||
+        (ztwd && (cfg->reconstruction != AMR_RECON_PPM || cfg->nx != 8)))
+        return AMR_ERR_ARG;
+    if (cfg->nf != (ztwd ? (int)ZTWD_NF : 6) || cfg->bw < min_bw || cfg->bw > 4 || cfg->nx < 4 || (cfg->nx % 4) != 0 ||
         cfg->max_refine_level < 0 || cfg->max_refine_level > 12 || cfg->max_bricks < 0 ||
         (cfg->reconstruction != AMR_RECON_MINMOD && cfg->reconstruction != AMR_RECON_PPM))
         return AMR_ERR_ARG;
@@ -525,7 +534,7 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
         rc |= dev_alloc(c, &c->st.Fx, (size_t)cap * fcount);
         rc |= dev_alloc(c, &c->st.Fy, (size_t)cap * fcount);
         rc |= dev_alloc(c, &c->st.Fz, (size_t)cap * fcount);
-        if (cfg->physics == AMR_PHYSICS_EULER_GRAVITY) {
+        if (cfg->physics != AMR_PHYSICS_EULER) {
             double** parr[8] = {&c->st.phi, &c->st.phi0, &c->st.dphi, &c->st.dphi1,
                                 &c->st.S,   &c->st.fx,   &c->st.fy,   &c->st.fz};
             for (auto p : parr) rc |= dev_alloc(c, p, (size_t)cap * g.pnx3);
@@ -546,6 +555,20 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
         rc |= dev_alloc(c, &c->d_dt, cap);
         rc |= dev_alloc(c, &c->d_red, cap);
         rc |= dev_alloc(c, &c->d_flags, 8 * (size_t)cap);
+        if (ztwd) {
+            rc |= dev_alloc(c, &c->st.W, (size_t)cap * g.ucount);
+            const size_t fc = (size_t)g.nx * g.nx * (g.nx + 1);
+            rc |= dev_alloc(c, &c->st.Vx, (size_t)cap * fc);
+            rc |= dev_alloc(c, &c->st.Vy, (size_t)cap * fc);
+            rc |= dev_alloc(c, &c->st.Vz, (size_t)cap * fc);
+            rc |= dev_alloc(c, &c->d_zerr, 1);
+            if (!rc && cudaMemsetAsync(c->d_zerr, 0, sizeof(int), c->stream) != cudaSuccess) rc = 1;
+            // State::abar (state_ztwd.cpp:27), State::rho_floor from the config
+            c->zpar.abar[0] = 4.0;
+            c->zpar.abar[1] = 14.12;
+            c->zpar.abar[2] = 17.52;
+            c->zpar.rho_floor = cfg->rho_floor;
+        }
         if (rc) {
             std::string e = c->err;
             amr_destroy(c);
@@ -584,7 +607,7 @@ int amr_destroy(amr_ctx* c) {
                         c->bt.parent, c->bt.cidx, c->bt.child, c->d_fo,     c->d_dt,       c->d_red,
                         c->d_flags, c->d_stage, c->d_slots,  c->d_reflux, c->d_vitems, c->d_vranges, c->d_cpos,
                         c->d_U1, c->d_fwork, c->d_pubmask, c->d_pub, c->d_fdone, c->d_fctl,
-                        c->st.fdphi, c->st.fdphi1};
+                        c->st.fdphi, c->st.fdphi1, c->st.W, c->st.Vx, c->st.Vy, c->st.Vz, c->d_zerr};
         for (void* p : ptrs)
             if (p) cudaFree(p);
         amr_poisson_release(c);
@@ -740,10 +763,16 @@ int amr_synchronize(amr_ctx* c) {
 // coarse-fine ghost reads a parent whose own ghosts are already filled.
 int amr_enforce_boundaries(amr_ctx* c) {
     NEED_DEVICE(c);
+    if (is_ztwd(c)) TRY(zt_ready(c));
     for (int l = 0; l <= c->tree.prm.max_level; l++)
         {
             ProfScope ps_(c->prof, KC_GHOST, c->stream, (long long)c->level_slots[l].size());
-            launch_ghost_fill(c->geom, c->bt, c->st, dslots_level(c, l), (int)c->level_slots[l].size(), c->stream);
+            if (is_ztwd(c))
+                launch_zt_ghost_fill(c->geom, c->bt, c->st, c->zpar, dslots_level(c, l),
+                                     (int)c->level_slots[l].size(), c->stream);
+            else
+                launch_ghost_fill(c->geom, c->bt, c->st, dslots_level(c, l), (int)c->level_slots[l].size(),
+                                  c->stream);
         }
     return check_launch(c);
 }
@@ -775,9 +804,14 @@ int amr_restore(amr_ctx* c) {
 // level upward so a corrected child face is final before its parent uses it.
 int amr_compute_fluxes(amr_ctx* c) {
     NEED_DEVICE(c);
+    if (is_ztwd(c)) TRY(zt_ready(c));
     {
         ProfScope ps_(c->prof, KC_FLUX, c->stream, (long long)c->all_slots.size());
-        launch_flux(c->geom, c->st, dslots_all(c), (int)c->all_slots.size(), c->stream);
+        if (is_ztwd(c))
+            launch_zt_flux(c->geom, c->bt, c->st, c->zpar, dslots_all(c), (int)c->all_slots.size(), c->d_zerr,
+                           c->stream);
+        else
+            launch_flux(c->geom, c->st, dslots_all(c), (int)c->all_slots.size(), c->stream);
     }
     for (int l = c->tree.prm.max_level; l >= 0; l--) {
         const int n = c->off_reflux[l + 1] - c->off_reflux[l];
@@ -791,6 +825,7 @@ int amr_compute_fluxes(amr_ctx* c) {
 
 int amr_add_difs(amr_ctx* c, double dt, double beta) {
     NEED_DEVICE(c);
+    if (is_ztwd(c)) TRY(zt_ready(c));
     const int grav = c->cfg.physics == AMR_PHYSICS_EULER_GRAVITY;
     {
         ProfScope ps_(c->prof, KC_ADD_DIFS, c->stream);
@@ -798,7 +833,12 @@ int amr_add_difs(amr_ctx* c, double dt, double beta) {
     }
     {
         ProfScope ps_(c->prof, KC_ADD_DIFS, c->stream, (long long)c->all_slots.size());
-        launch_add_difs(c->geom, c->st, dslots_all(c), (int)c->all_slots.size(), c->bt.h, dt, beta, grav, c->stream);
+        if (is_ztwd(c))
+            launch_zt_add_difs(c->geom, c->bt, c->st, c->zpar, dslots_all(c), (int)c->all_slots.size(), dt, beta,
+                               c->d_zerr, c->stream);
+        else
+            launch_add_difs(c->geom, c->st, dslots_all(c), (int)c->all_slots.size(), c->bt.h, dt, beta, grav,
+                            c->stream);
     }
     for (Node* n : c->order) n->age++;  // GridNode::add_difs, grid_node.cpp:338
     return check_launch(c);
@@ -807,10 +847,16 @@ int amr_add_difs(amr_ctx* c, double dt, double beta) {
 // Restriction from the finest parents to the root (children first).
 int amr_inject_from_children(amr_ctx* c) {
     NEED_DEVICE(c);
+    if (is_ztwd(c)) TRY(zt_ready(c));
     for (int l = c->tree.prm.max_level; l >= 0; l--)
         {
             ProfScope ps_(c->prof, KC_INJECT, c->stream);
-            launch_inject(c->geom, c->bt, c->st, dslots_parent(c, l), (int)c->parent_slots[l].size(), c->stream);
+            if (is_ztwd(c))
+                launch_zt_inject(c->geom, c->bt, c->st, c->zpar, dslots_parent(c, l), (int)c->parent_slots[l].size(),
+                                 c->d_zerr, c->stream);
+            else
+                launch_inject(c->geom, c->bt, c->st, dslots_parent(c, l), (int)c->parent_slots[l].size(),
+                              c->stream);
         }
     return check_launch(c);
 }
@@ -820,12 +866,17 @@ int amr_inject_from_children(amr_ctx* c) {
 int amr_max_dt(amr_ctx* c, double* dt) {
     NEED_DEVICE(c);
     if (!dt) return AMR_ERR_ARG;
+    if (is_ztwd(c)) TRY(zt_ready(c));
     const int n = (int)c->all_slots.size();
     {
         ProfScope ps_(c->prof, KC_MAX_DT, c->stream, (long long)n);
-        launch_max_dt(c->geom, c->st, dslots_all(c), n, c->bt.h, c->d_dt, c->stream);
+        if (is_ztwd(c))
+            launch_zt_max_dt(c->geom, c->bt, c->st, c->zpar, dslots_all(c), n, c->d_dt, c->d_zerr, c->stream);
+        else
+            launch_max_dt(c->geom, c->st, dslots_all(c), n, c->bt.h, c->d_dt, c->stream);
     }
     TRY(check_launch(c));
+    if (is_ztwd(c)) TRY(zt_check(c));
     std::vector<double> per(c->cap);
     int maxslot = 0;
     for (int s : c->all_slots) maxslot = std::max(maxslot, s + 1);

@@ -60,6 +60,12 @@ struct DevState {
     // null in the FP64 form
     float* fdphi;
     float* fdphi1;
+    // ZTWD state only (null otherwise): primitives [cap][nf][gnx^3] and the
+    // face-averaged normal velocities [cap][nx][nx][nx+1] per direction
+    double* W;
+    double* Vx;
+    double* Vy;
+    double* Vz;
 };
 
 // One coarse-fine flux (or force) correction task: coarse brick's face

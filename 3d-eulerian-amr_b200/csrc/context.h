@@ -9,6 +9,7 @@
 #include "amr_internal.h"
 #include "octree.h"
 #include "profiler.h"
+#include "ztwd.h"
 
 struct amr_ctx {
     amr_config cfg{};
@@ -86,6 +87,11 @@ struct amr_ctx {
     long long relax_calls = 0, relax_sweeps_total = 0;
     bool topo_dirty = true;
     long long topo_version = 0;  // bumped by every rebuild_topology
+    // ZTWD state: frame + EOS passed to its kernels, EOS-failure word
+    amr::ZtwdPar zpar{};
+    bool zt_eos = false;
+    int* d_zerr = nullptr;
+    int zt_first_solve = 1;  // BinaryDriver::solve's first_call (binary_driver.cpp:297-301)
     amr::Profiler prof;
     struct GraphState* gs = nullptr;  // captured step/solve graphs (graph_host.cpp)
 
@@ -93,6 +99,12 @@ struct amr_ctx {
 };
 
 namespace amr {
+inline bool is_ztwd(const amr_ctx* c) { return c->cfg.physics == AMR_PHYSICS_ZTWD; }
+inline bool has_gravity(const amr_ctx* c) {
+    return c->cfg.physics == AMR_PHYSICS_EULER_GRAVITY || c->cfg.physics == AMR_PHYSICS_ZTWD;
+}
+int zt_ready(amr_ctx* c);  // ZTWD context has its EOS (ztwd_host.cpp)
+int zt_check(amr_ctx* c);  // reads and clears the EOS-failure word
 int rebuild_topology(amr_ctx* c);
 int alloc_slot(amr_ctx* c);
 void graph_release(amr_ctx* c);

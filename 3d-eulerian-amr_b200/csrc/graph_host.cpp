@@ -330,8 +330,16 @@ int rec_solve(amr_ctx* c, cudaStream_t s, double tol, int depth) {
             },
             [&](cudaStream_t q, cudaGraphConditionalHandle h) { return rec_vcycle(c, q, depth + 1, h, tol); }));
     }
-    for (int l = c->tree.prm.max_level; l >= 0; l--)
-        launch_inject(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l], (int)c->parent_slots[l].size(), s);
+    if (is_ztwd(c)) {  // Binary's solve: pot_to_grid, then the ZTWD restriction
+        launch_zt_pot(c->geom, c->bt, c->st, c->zpar, all(c), nall(c), 0, s);
+        for (int l = c->tree.prm.max_level; l >= 0; l--)
+            launch_zt_inject(c->geom, c->bt, c->st, c->zpar, c->d_slots + c->off_parent[l],
+                             (int)c->parent_slots[l].size(), c->d_zerr, s);
+    } else {
+        for (int l = c->tree.prm.max_level; l >= 0; l--)
+            launch_inject(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l], (int)c->parent_slots[l].size(),
+                          s);
+    }
     return launched(c, __LINE__);
 }
 
@@ -454,8 +462,8 @@ void count_replay(amr_ctx* c, long long top_kernels) {
 int need(amr_ctx* c) {
     if (!c) return AMR_ERR_ARG;
     if (!c->has_device) return AMR_ERR_NODEVICE;
-    if (c->cfg.physics != AMR_PHYSICS_EULER_GRAVITY) {
-        c->err = "graph step needs AMR_PHYSICS_EULER_GRAVITY";
+    if (!has_gravity(c)) {
+        c->err = "graph solve needs a self-gravitating context";
         return AMR_ERR_ARG;
     }
     if (c->geom.nx != 8) {
@@ -557,6 +565,10 @@ int amr_graph_solve(amr_ctx* c, double tol, int max_cycles, double* l1_error, in
 // graph step) formed on the device.  step_index 0 starts the clamp afresh.
 int amr_graph_grav_step(amr_ctx* c, double tol, double dynamic_range, int step_index, double* dt_out) {
     TRY(need(c));
+    if (c->cfg.physics != AMR_PHYSICS_EULER_GRAVITY) {
+        c->err = "graph step needs AMR_PHYSICS_EULER_GRAVITY";
+        return AMR_ERR_ARG;
+    }
     GraphState* g = c->gs;
     const int max_cycles = 10000;
     if (step_index <= 0) {

@@ -314,3 +314,7 @@ int helm_ztwd_batch(helm_ctx* c, long long n, const double* zbar, const double* 
 }
 
 }  // extern "C"
+
+namespace amr {
+const HelmTable* helm_table_of(const helm_ctx* c) { return c ? &c->tab : nullptr; }
+}  // namespace amr

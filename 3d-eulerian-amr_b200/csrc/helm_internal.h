@@ -29,8 +29,10 @@ struct HelmPoint {
     int status;
 };
 
-__device__ void helm_point(const HelmTable& H, double rho_code, double T_code, double abar, double zbar,
-                           HelmPoint& o);
+// helm_point / helm_invert_point: helm_device.cuh
+
+// the device table of a context (helm_host.cpp)
+const HelmTable* helm_table_of(const helm_ctx* c);
 
 void launch_helm_eos(const HelmTable& H, long long n, const double* rho, const double* T, const double* abar,
                      const double* zbar, double* p, double* e, double* cs, double* cv, double* s, double* dsdt,

@@ -84,8 +84,8 @@ int amr_poisson_boundaries_noalloc(amr_ctx* c) {
         c->err = "context has no device pool";
         return AMR_ERR_NODEVICE;
     }
-    if (c->cfg.physics != AMR_PHYSICS_EULER_GRAVITY) {
-        c->err = "Poisson call on a context created without AMR_PHYSICS_EULER_GRAVITY";
+    if (!has_gravity(c)) {
+        c->err = "Poisson call on a context created without self-gravity";
         return AMR_ERR_ARG;
     }
     // the context's own Poisson buffers are allocated by the first ordinary

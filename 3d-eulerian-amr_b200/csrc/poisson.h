@@ -10,6 +10,13 @@
 struct amr_ctx;
 
 namespace amr {
+// checks the context has self-gravity and allocates the Poisson scratch
+// (domain-face tables zeroed, error words) on first use
+int poisson_need(amr_ctx* c);
+// phi ghosts of one level (faces, edges, vertices) and phi_from_children of
+// every level, as the V-cycle runs them (poisson_host.cpp)
+int poisson_phi_boundaries(amr_ctx* c, int l);
+int poisson_phi_from_children(amr_ctx* c);
 // New bricks: zero the Poisson arrays, then phi/phi0 piecewise constant from
 // the parent (Poisson::inject_from_parent, poisson.cpp:132-164).
 void launch_poisson_new_bricks(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,

@@ -49,8 +49,8 @@ int need_gravity(amr_ctx* c) {
         c->err = "context has no device pool";
         return AMR_ERR_NODEVICE;
     }
-    if (c->cfg.physics != AMR_PHYSICS_EULER_GRAVITY) {
-        c->err = "Poisson call on a context created without AMR_PHYSICS_EULER_GRAVITY";
+    if (!has_gravity(c)) {
+        c->err = "Poisson call on a context created without self-gravity";
         return AMR_ERR_ARG;
     }
     if (!c->d_bphi) {
@@ -240,6 +240,20 @@ int check_device_error(amr_ctx* c) {
 }  // namespace
 
 namespace amr {
+int poisson_need(amr_ctx* c) { return need_gravity(c); }
+int poisson_phi_boundaries(amr_ctx* c, int l) { return phi_boundaries(c, l); }
+
+// Poisson::phi_from_children (poisson.cpp:707-747), children first
+int poisson_phi_from_children(amr_ctx* c) {
+    const int maxlevel = max_level_present(c);
+    for (int l = maxlevel - 1; l >= 0; l--) {
+        ProfScope ps_(c->prof, KC_VDOWN, c->stream);
+        launch_phi_from_children(c->geom, c->bt, c->st, c->d_slots + c->off_parent[l],
+                                 (int)c->parent_slots[l].size(), c->stream);
+    }
+    return check_launch(c);
+}
+
 PhysWalk phys_walk(const amr_ctx* c) {
     return PhysWalk{c->d_pwalk, c->n_pseg, c->d_pwalk + 2 * c->n_pseg, c->n_ptop};
 }
@@ -384,6 +398,7 @@ int amr_poisson_solve(amr_ctx* c, double tol, int max_cycles, double* l1_error, 
     } while (e > tol);
     if (l1_error) *l1_error = e;
     if (cycles) *cycles = it;
+    if (is_ztwd(c)) TRY(amr_ztwd_pot(c, 0));  // Binary's solve: pot_to_grid (binary_driver.cpp:341)
     return amr_inject_from_children(c);
 }
 

@@ -42,6 +42,8 @@ extern "C" {
 
 #define AMR_PHYSICS_EULER 0         /* euler/state.cpp, no gravity */
 #define AMR_PHYSICS_EULER_GRAVITY 1 /* Euler state + Poisson self-gravity */
+#define AMR_PHYSICS_ZTWD 2          /* BINARY build, ZTWD state (binary/state_ztwd.cpp): 13 fields, Helmholtz
+                                       EOS, rotating frame, self-gravity; nf 13, PPM, bw >= 3 */
 
 #define AMR_RECON_MINMOD 0 /* Reconstruct::minmod (reconstruct.cpp:60-71), the EULER build */
 #define AMR_RECON_PPM 1    /* Reconstruct::ppm (reconstruct.cpp:22-58), PPM builds; needs bw >= 3 */
@@ -181,6 +183,42 @@ int amr_poisson_boundaries_noalloc(amr_ctx* ctx);
  * Euler state): per substep hydro + gravity sources, phi time level, solve;
  * regrid every 8 steps at state_max/dynamic_range. */
 int amr_grav_step(amr_ctx* ctx, double dt, double tol, double dynamic_range, int step_index);
+
+/* ---- ZTWD binary (AMR_PHYSICS_ZTWD) -----------------------------------------
+ * The BINARY build's hydro + gravity with the ZTWD state.  Every entry point
+ * above (boundaries, fluxes, add_difs, restriction, CFL step, regrid,
+ * Poisson solve) then runs the ZTWD kernels: State::to_prim/to_con,
+ * fluxes, eigenvalues, outflow and floor of binary/state_ztwd.cpp with p and
+ * c_s from the Helmholtz EOS, Binary::add_difs's gravity and -p div u
+ * sources (binary.cpp:205-254), and Binary::pot_to_grid after each solve.
+ * Set the EOS and the frame before the first hydro call.  Where the
+ * reference aborts inside the EOS (outside the table, Newton failure) the
+ * call returns AMR_ERR_RANGE. */
+#ifndef HELM_CTX_TYPEDEF
+#define HELM_CTX_TYPEDEF
+typedef struct helm_ctx helm_ctx;
+#endif
+/* EOS table and code units (helm_set_cgs_units) of `eos`, which must stay
+ * alive while the context uses it; the units are read at this call. */
+int amr_ztwd_set_eos(amr_ctx* ctx, helm_ctx* eos);
+/* Binary::Omega, Binary::Omega0 (binary.cpp:24-26) and the centre-of-mass
+ * correction force State::fR, State::ftheta (binary_driver.cpp:188-199). */
+int amr_ztwd_set_frame(amr_ctx* ctx, double omega, double omega0, double fR, double ftheta);
+/* binary.cpp:825-936 on every brick: mode 0 Binary::pot_to_grid, 1
+ * pot_from_grid (with the phi ghosts of every level), 2 add_pot_et,
+ * 3 sub_pot_et. */
+int amr_ztwd_pot(amr_ctx* ctx, int mode);
+/* BinaryDriver::step (binary_driver.cpp:346-459) without its diagnostics
+ * output: on step_index 0 pot_from_grid + the first solve (with
+ * phi_from_children) + store_phi; store; three substeps (boundaries, fluxes,
+ * Binary::add_difs, phi time level, solve + pot_to_grid + restriction); the
+ * MAXDTINC retry (restore and redo with dt / MAXDTINC while the new CFL step
+ * is below dt / MAXDTINC); every 8th step the regrid at
+ * state_max/dynamic_range between add_pot_et and sub_pot_et, with a solve at
+ * tol/10 after a change.  *dt_used gets the step taken.  With
+ * amr_config.persistent_solve > 0 (or the mixed precision) each solve runs as
+ * amr_graph_solve. */
+int amr_ztwd_step(amr_ctx* ctx, double dt, double tol, double dynamic_range, int step_index, double* dt_used);
 
 /* ---- graph-captured forms --------------------------------------------------
  * The same step and solve with every loop decided on the device: the V-cycle

@@ -27,7 +27,10 @@
 extern "C" {
 #endif
 
+#ifndef HELM_CTX_TYPEDEF
+#define HELM_CTX_TYPEDEF
 typedef struct helm_ctx helm_ctx;
+#endif
 
 #define HELM_IMAX 1081 /* densities (log10 ye*rho from -12 to 15), helmeos.cpp:7 */
 #define HELM_JMAX 401  /* temperatures (log10 T from 3 to 13), helmeos.cpp:8 */

@@ -22,6 +22,11 @@ Variants:
   ppm  g05 with PPM reconstruction (euler_defs.h:24 switched on) and BW 3,
        the ghost width PPM needs (reconstruct.cpp:22-58 reads cells i-3..i+2
        of face i)
+  ztwd BINARY physics with the ZTWD state as binary/binary_defs.h sets it
+       (PPM, BW 3, Z_REFLECT, GRID_DIM 1), except 8^3 interior cells per
+       brick instead of 12^3 (GNX 8+2*BW, the brick the CUDA path is written
+       for); driven by oracle/harness/ztwd_harness.cpp, with the reference's
+       own binary/initialize.cpp as the initial data
 
 Run:  python oracle/build_ref.py [--reference /root/reference]
 When the reference tree is absent (e.g. on a GPU box) this is a no-op and the
@@ -47,6 +52,20 @@ EULER_SOURCES = [
     "poisson/poisson_phys_bound.cpp", "binary/lane_emden.cpp",
 ]
 
+COMMON_SOURCES = [
+    "assert.cpp", "indexer_2d.cpp", "indexer_2d_by2.cpp", "reconstruct.cpp",
+    "grid/grid.cpp", "grid/grid_node.cpp", "grid/grid_amr_bound.cpp",
+    "grid/grid_phys_bound.cpp", "grid/grid_interface.cpp",
+    "oct_node/child_index.cpp", "oct_node/oct_face.cpp", "oct_node/oct_node.cpp",
+    "poisson/poisson.cpp", "poisson/poisson_amr_bound.cpp",
+    "poisson/poisson_phys_bound.cpp",
+]
+BINARY_SOURCES = COMMON_SOURCES + [
+    "binary/binary.cpp", "binary/binary_driver.cpp", "binary/state_ztwd.cpp",
+    "binary/state.cpp", "binary/lane_emden.cpp", "binary/initialize.cpp",
+    "helmholtz/helmeos.cpp",
+]
+
 CXXFLAGS = ["-O2", "-fopenmp", "-ffp-contract=off", "-DNDEBUG", "-w"]
 
 
@@ -66,6 +85,13 @@ def _patch(src, variant):
     _replace(os.path.join(src, "real.h"), "Real abs(Real);", "")
     _replace(os.path.join(src, "real.h"),
              "inline Real abs(Real a) {\n\treturn fabs(a);\n}", "")
+    # Silo is not installed; only the output path uses it.
+    shutil.copy(os.path.join(HERE, "stubs", "silo.h"), os.path.join(src, "silo.h"))
+    if variant == "ztwd":
+        # binary/binary_defs.h:31-35: 12^3 interior cells -> 8^3
+        bdefs = os.path.join(src, "binary", "binary_defs.h")
+        _replace(bdefs, "#define GNX \t\t\t\t(12+2*BW)", "#define GNX \t\t\t\t(8+2*BW)", count=2)
+        return
     # defs.h:4 hard-codes the BINARY driver; select the Euler state.
     _replace(os.path.join(src, "defs.h"), "#define BINARY", "#define EULER")
     defs = os.path.join(src, "euler", "euler_defs.h")
@@ -79,8 +105,6 @@ def _patch(src, variant):
     # harness defines initialize(GridNode*) instead.
     with open(os.path.join(src, "euler", "initialize.cpp"), "w") as f:
         f.write("// replaced by oracle/harness/amr_harness.cpp\n")
-    # Silo is not installed; only the output path uses it.
-    shutil.copy(os.path.join(HERE, "stubs", "silo.h"), os.path.join(src, "silo.h"))
 
 
 def _run(cmd, cwd=None):
@@ -100,8 +124,10 @@ def _stale(out, inputs):
 def build_variant(reference, variant, jobs=8):
     src = os.path.join(REF_OUT, "src_" + variant)
     exe = os.path.join(REF_OUT, variant + "_harness")
-    harness = os.path.join(HERE, "harness", "amr_harness.cpp")
-    inputs = [harness, os.path.abspath(__file__), os.path.join(HERE, "stubs", "silo.h")]
+    harness = os.path.join(HERE, "harness", "ztwd_harness.cpp" if variant == "ztwd" else "amr_harness.cpp")
+    sources = BINARY_SOURCES if variant == "ztwd" else EULER_SOURCES
+    inputs = [harness, os.path.abspath(__file__), os.path.join(HERE, "stubs", "silo.h"),
+              os.path.join(HERE, "harness", "dump.h")]
     if not _stale(exe, inputs):
         return exe
     if os.path.exists(src):
@@ -115,7 +141,7 @@ def build_variant(reference, variant, jobs=8):
     objdir = os.path.join(src, "_obj")
     os.makedirs(objdir, exist_ok=True)
     procs, objs = [], []
-    for s in EULER_SOURCES:
+    for s in sources:
         o = os.path.join(objdir, s.replace("/", "_") + ".o")
         objs.append(o)
         procs.append(subprocess.Popen(["g++"] + CXXFLAGS + ["-I", src, "-c", os.path.join(src, s), "-o", o],
@@ -130,7 +156,7 @@ def build_variant(reference, variant, jobs=8):
         if p.returncode:
             raise RuntimeError("compile failed:\n" + out + err)
     ho = os.path.join(objdir, "harness.o")
-    _run(["g++"] + CXXFLAGS + ["-I", src, "-c", harness, "-o", ho])
+    _run(["g++"] + CXXFLAGS + ["-I", src, "-I", os.path.join(HERE, "harness"), "-c", harness, "-o", ho])
     _run(["g++", "-fopenmp", "-o", exe] + objs + [ho])
     return exe
 
@@ -152,7 +178,7 @@ def build_helm(reference):
     return exe
 
 
-def build(reference="/root/reference", variants=("g05", "zr", "ppm")):
+def build(reference="/root/reference", variants=("g05", "zr", "ppm", "ztwd")):
     if not os.path.isdir(reference):
         print("[oracle] reference tree not present; using prebuilt oracle/_ref binaries")
         return []

@@ -41,4 +41,21 @@ static inline int DBPutUcdvar1(DBfile*, const char*, const char*, double*, int, 
                                DBoptlist*) { return 0; }
 static inline int DBClose(DBfile*) { return 0; }
 
+/* Read side, only named by Binary::input (binary/binary.cpp:1098-1169),
+ * which the oracle never calls. */
+typedef struct DBzonelist_s { int* nodelist; int nzones; int lnodelist; } DBzonelist;
+typedef struct DBucdmesh_s {
+    void* min_extents;
+    void* max_extents;
+    void* coords[3];
+    DBzonelist* zones;
+    int nnodes;
+    double time;
+} DBucdmesh;
+typedef struct DBucdvar_s { void** vals; } DBucdvar;
+static inline DBucdmesh* DBGetUcdmesh(DBfile*, const char*) { return 0; }
+static inline DBucdvar* DBGetUcdvar(DBfile*, const char*) { return 0; }
+static inline void DBFreeUcdmesh(DBucdmesh*) {}
+static inline void DBFreeUcdvar(DBucdvar*) {}
+
 #endif

@@ -48,6 +48,21 @@ def gpu(amr_mod):
     return amr_mod
 
 
+def _load_pkg_module(name, fname):
+    spec = importlib.util.spec_from_file_location(name, os.path.join(PKG, fname))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+@pytest.fixture(scope="session")
+def table_path(tmp_path_factory):
+    """The synthetic Helmholtz table (3d-eulerian-amr_b200/helm_table.py),
+    written once per session."""
+    helm_table = _load_pkg_module("helm_table", "helm_table.py")
+    return helm_table.ensure_table(str(tmp_path_factory.mktemp("helm")))
+
+
 def ref_binary(variant="g05"):
     p = os.path.join(REF_BIN, variant + "_harness")
     return p if os.path.exists(p) else None

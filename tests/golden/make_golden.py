@@ -34,13 +34,16 @@ CASES = {
     "poisson_poly_L3": ("g05", "poisson", ["polytrope", 3, 3]),
     "grav_poly_L2": ("g05", "grav", ["polytrope", 2, 3, 1e-6]),
     "grav_ppm_poly_L2": ("ppm", "grav", ["polytrope", 2, 3, 1e-6]),
+    # ZTWD binary (BINARY build): maxlevel, steps
+    "ztwd_L2": ("ztwd", "ztwd", [2, 3]),
+    "ztwd_L3": ("ztwd", "ztwd", [3, 9]),
 }
 # cases whose full state would make a large fixture keep only the tree and
 # per-brick, per-field sums and absolute sums of the interior cells
 SUMMARY_ONLY = {"hydro_blast_L2", "hydro_bump_L3", "poisson_poly_L3", "hydro_ppm_blast_L2"}
 # for these the final conserved state is kept as sums only (the potential in
 # full): the initial state is needed in full to start from the same data
-FINAL_SUMMARY = {"grav_poly_L2", "grav_ppm_poly_L2"}
+FINAL_SUMMARY = {"grav_poly_L2", "grav_ppm_poly_L2", "ztwd_L3"}
 
 
 def interior(d, U):
@@ -71,6 +74,11 @@ def run_case(name, workdir):
     exe = os.path.join(ROOT, "oracle", "_ref", variant + "_harness")
     out = os.path.join(workdir, name + ".bin")
     env = dict(os.environ, OMP_NUM_THREADS="1")
+    if mode == "ztwd":
+        # the BINARY build reads ./helmholtz.table at start-up (helmeos.cpp:73-130)
+        sys.path.insert(0, os.path.join(ROOT, "3d-eulerian-amr_b200"))
+        import helm_table
+        helm_table.ensure_table(workdir)
     r = subprocess.run([exe, mode] + [str(a) for a in args] + [out], cwd=workdir, env=env,
                        capture_output=True, text=True)
     if r.returncode != 0:

@@ -40,11 +40,6 @@ helm_oracle = _load("helm_oracle", os.path.join(ORACLE, "helm_oracle.py"))
 
 
 @pytest.fixture(scope="session")
-def table_path(tmp_path_factory):
-    return helm_table.ensure_table(str(tmp_path_factory.mktemp("helm")))
-
-
-@pytest.fixture(scope="session")
 def oracle_table(table_path):
     return helm_oracle.Table(table_path)
 

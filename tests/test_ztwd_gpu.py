@@ -1,0 +1,122 @@
+"""ZTWD binary (BINARY build of the reference) through the C ABI.
+
+ztwd_*: the reference's own two-polytrope initial data (binary/initialize.cpp)
+for a q = 0.7 binary in the co-rotating frame, then BinaryDriver::step
+(binary/binary_driver.cpp:346-459) with dt from GridNode::max_dt and the
+MAXDTINC clamp, run by oracle/harness/ztwd_harness.cpp on the reference's
+BINARY build (ZTWD state, PPM, BW 3, 8^3 bricks) reading the synthetic
+Helmholtz table.  The library replays the same steps (amr_ztwd_step); trees
+must match bit for bit, dt to 1e-12 and every field to 1e-12
+(max |a-b| / max |b| per field).  ztwd_L3 regrids at its step 8 (the tree
+changes), so its final state is compared through per-brick sums.
+"""
+
+import os
+
+import numpy as np
+import pytest
+
+from cases import FP64_FIELD_RTOL, field_rel_err, load_golden, same_tree
+from conftest import _load_pkg_module
+
+DT_RTOL = 1.0e-12
+ELL_TOLER = 1.0e-7     # binary/binary_defs.h:64
+DYNAMIC_RANGE = 1.0e6  # binary/binary_defs.h:14
+MIXED_RTOL = 1.0e-6    # mixed + persistent form against FP64, density / energy rel L1 after the run
+
+
+def ztwd_config(maxlevel, **kw):
+    """The BINARY build's compile-time constants (binary/binary_defs.h) with
+    8^3 interior cells per brick."""
+    cfg = dict(physics=2, nf=13, bw=3, nx=8, reconstruction=1, grid_dim=1.0, z_reflect=1, mirror_refine_y=1,
+               max_refine_level=maxlevel, rho_floor=1.0e-10, cfl=0.3, maxdtinc=1.25, max_bricks=1024)
+    cfg.update(kw)
+    return cfg
+
+
+def make(gpu, g, table_path, **kw):
+    helm = _load_pkg_module("helm_b200", "helm.py").Helm(table_path)
+    K1, Ucm, Ug, Us, omega, omega0 = [float(x) for x in g["extra"][:6]]
+    helm.set_cgs_units(Ucm, Ug, Us, 1.0)  # Binary::set_units (binary/binary.h:17-35)
+    a = gpu.AMR(**ztwd_config(int(g["init_level"].max()), **kw))
+    a.ztwd_set_eos(helm)
+    a.ztwd_set_frame(omega, omega0, 0.0, 0.0)
+    a.load_tree(g["init_level"], g["init_loc"], g["init_age"])
+    bw = a.bw
+    U = np.zeros((a.nbricks, a.nf, a.gnx, a.gnx, a.gnx))
+    U[:, :, bw:-bw, bw:-bw, bw:-bw] = g["init_U"]
+    a.upload_state(U)
+    a.enforce_boundaries()
+    return a
+
+
+def run(a, nsteps):
+    dts, last = [], 0.0
+    for s in range(nsteps):
+        dt = a.max_dt()
+        if s > 0:
+            dt = min(last * 1.25, dt)
+        dt = a.ztwd_step(dt, ELL_TOLER, DYNAMIC_RANGE, s)
+        last = dt
+        dts.append(dt)
+    return np.array(dts)
+
+
+def interior(a):
+    b = a.bw
+    return a.download_state()[:, :, b:-b, b:-b, b:-b]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["ztwd_L2", "ztwd_L3"])
+def test_ztwd_steps_match_reference(gpu, table_path, name):
+    g = load_golden(name)
+    nsteps = int(g["args"][1])
+    a = make(gpu, g, table_path)
+    dts = run(a, nsteps)
+    ex = g["extra"]
+    np.testing.assert_allclose(dts, ex[8:8 + nsteps], rtol=DT_RTOL)
+    t = a.get_tree()
+    assert same_tree(t, g, "final_")
+    assert np.array_equal(t["age"], g["final_age"])
+    U = interior(a)
+    if "final_U" in g:
+        err = field_rel_err(U, g["final_U"])
+        assert np.all(err <= FP64_FIELD_RTOL), err
+    else:
+        s = U.reshape(U.shape[0], U.shape[1], -1).sum(axis=2)
+        rel = np.abs(s - g["final_Usum"]) / np.maximum(g["final_Uabs"], 1e-300)
+        assert rel.max() <= 1e-11, rel.max()
+    fo = a.flow_off()
+    np.testing.assert_allclose(fo, g["final_FO"], rtol=1e-10, atol=1e-13 * max(1.0, np.abs(g["final_FO"]).max()))
+    a.close()
+
+
+@pytest.mark.gpu
+def test_ztwd_mixed_persistent_close_to_fp64(gpu, table_path):
+    """FP32 multigrid correction in the persistent solve, against the FP64
+    form after the same steps: same trees and steps, density and energy
+    within MIXED_RTOL (relative L1)."""
+    g = load_golden("ztwd_L2")
+    nsteps = int(g["args"][1])
+    a = make(gpu, g, table_path)
+    b = make(gpu, g, table_path, precision=gpu.PREC_MIXED, persistent_solve=2)
+    run(a, nsteps)
+    run(b, nsteps)
+    assert same_tree(b.get_tree(), {"final_" + k: v for k, v in a.get_tree().items()}, "final_")
+    ua, ub = interior(a), interior(b)
+    for f in (0, 7):
+        l1 = np.abs(ub[:, f] - ua[:, f]).sum() / np.abs(ua[:, f]).sum()
+        assert l1 <= MIXED_RTOL, (f, l1)
+    a.close()
+    b.close()
+
+
+@pytest.mark.gpu
+def test_ztwd_calls_need_the_eos(gpu):
+    a = gpu.AMR(**ztwd_config(1))
+    a.init()
+    with pytest.raises(gpu.AmrError) as e:
+        a.enforce_boundaries()
+    assert e.value.code == -6  # AMR_ERR_STATE
+    a.close()
