@@ -15,6 +15,12 @@ Initial conditions (cell centres, FP64, Euler state d sx sy sz et tau):
   random     seeded log-normal field: Gaussian random field with P(k)~k^-3,
              sigma 1, on a periodic 256^3 grid, trilinearly sampled;
              v ~ N(0, 0.1), p = rho^(5/3)
+  binary     (ZTWD state, 13 fields) the reference's two-polytrope binary of
+             binary/initialize.cpp:12-92 with q = 0.7, separation 0.5, donor
+             radius 0.17 (its Roche lobe radius at this q is 0.174),
+             M1 = 2.4e-3, n = 1.5, followed by State::floor (T at the table
+             floor, et = 0: a zero-temperature binary) and synchronous
+             rotation in the co-rotating frame (lz = rho Omega R^2)
 """
 
 import numpy as np
@@ -37,6 +43,97 @@ def cell_centres(tree, bw, nx, grid_dim, z_reflect, ghosts=False):
             f = (off[:, d:d + 1] + idx[None, :]) * h - bw * h0
         xs.append(f + 0.5 * h)
     return xs  # each (n, len(idx))
+
+
+# ZTWD binary parameters (Binary statics of binary/binary.cpp:8-26, set for
+# this configuration)
+BINARY = dict(q=0.7, a=0.5, R2=0.17, M1=2.4e-3, n=1.5, rho_floor=1.0e-10, T_floor=1.0e3)
+
+
+def binary_params():
+    """Derived constants of binary/initialize.cpp:13-19 and the code units of
+    Binary::set_units (binary/binary.h:17-35): K1, (cm, g, s) and Omega."""
+    q, a, R2, M1, n = (BINARY[k] for k in ("q", "a", "R2", "M1", "n"))
+    rho_c2 = q * M1 * (pow(3.65375 / R2, 3.0) / (2.71406 * 4.0 * np.pi))
+    rho_c1 = rho_c2 / pow(q, 2.0 * n / (3.0 - n))
+    K = pow(R2 / 3.65375, 2) * 4.0 * np.pi / (2.5) * pow(rho_c2, 1.0 / 3.0)
+    A, B, G = 6.0023e+22, 2.0 * 9.7393e+5, 6.6745e-8
+    g = pow(K, -1.5) * (pow(A / G, 1.5) / B / B)
+    cm = pow(K, -0.5) * (1.0 / B * np.sqrt(A / G))
+    s = 1.0 * (1.0 / np.sqrt(B * G))
+    omega = np.sqrt(M1 * (q + 1.0) / (a * a * a))
+    return dict(K1=K, rho_c1=rho_c1, rho_c2=rho_c2, cm=cm, g=g, s=s, omega=omega,
+                R1=R2 * pow(q, 1.0 / 3.0))
+
+
+def _minmod(a, b):  # real.h:63-65
+    sg = np.sign(a) + np.sign(b)
+    return 0.5 * sg * np.minimum(np.abs(a), np.abs(b))
+
+
+def _binary_state(tree, bw, nx, grid_dim, z_reflect, ghosts):
+    """binary/initialize.cpp:12-92 + State::floor + synchronous rotation."""
+    P = binary_params()
+    q, a, n, floor = BINARY["q"], BINARY["a"], BINARY["n"], BINARY["rho_floor"]
+    gnx = nx + 2 * bw
+    h0 = 2.0 * grid_dim / nx
+    idx = np.arange(gnx) if ghosts else np.arange(bw, gnx - bw)
+    off = tree["offset"].astype(np.float64)
+    h = tree["h"][:, None]
+    faces = []
+    for d in range(3):  # Grid::xf/yf/zf of cells idx and idx + 1
+        lo = (off[:, d:d + 1] + idx[None, :]) * h - bw * h0
+        hi = (off[:, d:d + 1] + idx[None, :] + 1) * h - bw * h0
+        if not (d == 2 and z_reflect):
+            lo, hi = lo - grid_dim, hi - grid_dim
+        faces.append((lo, hi))
+    nb, m = off.shape[0], len(idx)
+    rho_c1, rho_c2, K = P["rho_c1"], P["rho_c2"], P["K1"]
+    E1 = np.sqrt((4.0 * np.pi * pow(rho_c1, 1.0 - 1.0 / n)) / ((n + 1.0) * K))
+    E2 = np.sqrt((4.0 * np.pi * pow(rho_c2, 1.0 - 1.0 / n)) / ((n + 1.0) * K))
+    x1, x2 = a * q / (q + 1.0), -a / (q + 1.0)
+    (xl, xh), (yl, yh), (zl, zh) = faces
+    XL = np.broadcast_to(xl[:, None, None, :], (nb, m, m, m))
+    XH = np.broadcast_to(xh[:, None, None, :], (nb, m, m, m))
+    YL = np.broadcast_to(yl[:, None, :, None], (nb, m, m, m))
+    YH = np.broadcast_to(yh[:, None, :, None], (nb, m, m, m))
+    ZL = np.broadcast_to(zl[:, :, None, None], (nb, m, m, m))
+    ZH = np.broadcast_to(zh[:, :, None, None], (nb, m, m, m))
+    y = _minmod(YL, YH)
+    z = _minmod(ZL, ZH)
+    xa = _minmod(XL - x1, XH - x1)
+    xb = _minmod(XL - x2, XH - x2)
+    near = (np.sqrt(xa * xa + y * y + z * z) * E1 < 3.7) | (np.sqrt(xb * xb + y * y + z * z) * E2 < 3.7)
+    finest = tree["child_mask"] == 0
+    M0 = np.where(finest, (tree["h"] / P["R1"] + 2.0).astype(np.int64), 2)
+    rho1 = np.zeros((nb, m, m, m))
+    rho2 = np.zeros((nb, m, m, m))
+    hb = tree["h"][:, None, None, None]
+    for M in np.unique(M0):
+        sel = (M0 == M)[:, None, None, None] & near
+        for k0 in range(M):
+            zz = ZL + (k0 + 0.5) * hb / M
+            for j0 in range(M):
+                yy = YL + (j0 + 0.5) * hb / M
+                for i0 in range(M):
+                    xx = XL + (i0 + 0.5) * hb / M
+                    r1 = np.sqrt((xx - x1) * (xx - x1) + yy * yy + zz * zz) * E1
+                    r2 = np.sqrt((xx - x2) * (xx - x2) + yy * yy + zz * zz) * E2
+                    t1 = np.where(sel & (r1 < 3.7), lane_emden(np.where(r1 < 3.7, r1, 0.0)) ** n / M ** 3 * rho_c1, 0.0)
+                    t2 = np.where(sel & (r2 < 3.7), lane_emden(np.where(r2 < 3.7, r2, 0.0)) ** n / M ** 3 * rho_c2, 0.0)
+                    rho1 = rho1 + t1
+                    rho2 = rho2 + t2
+    rho1 = np.maximum(rho1, floor / 2.0)
+    rho2 = np.maximum(rho2, floor / 2.0)
+    rho = rho1 + rho2
+    U = np.zeros((nb, 13, m, m, m))
+    U[:, 0], U[:, 1], U[:, 2] = rho, rho1, rho2
+    U[:, 9] = BINARY["T_floor"]  # Newton from e = 0 stops at the table floor
+    U[:, 10] = rho               # all species zero -> species 0 (state_ztwd.cpp:520-526)
+    XC = XL + 0.5 * hb
+    YC = YL + 0.5 * hb
+    U[:, 4] = rho * P["omega"] * (XC * XC + YC * YC)
+    return U
 
 
 def _lane_emden_table(dr=0.05, rmax=3.7):
@@ -168,6 +265,8 @@ def evaluate(ic, tree, bw, nx, grid_dim, z_reflect, max_level, ghosts=True, seed
         ei = K * rho ** (1.0 + 1.0 / 1.5) / (GAMMA - 1.0)
         zero = np.zeros_like(X)
         return _state(rho, zero, zero, zero, ei)
+    if ic == "binary":
+        return _binary_state(tree, bw, nx, grid_dim, z_reflect, ghosts)
     if ic == "random":
         F = random_field(seed)
         nn = F.shape[0]

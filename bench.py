@@ -577,6 +577,116 @@ def run_batched_substep(amr, ini, torch, steps, warmup, levels=5):
     return out
 
 
+ZT_LEVELS = 5
+ZT_TOL = 1.0e-7  # ELL_TOLER of the BINARY build (binary/binary_defs.h:64)
+ZT_STEPS_TOTAL = 100
+
+
+def ztwd_context(amr, ini, helm_mod, table, levels, prec, persistent):
+    """A ZTWD binary context on the 5-level tree of the reference's two-polytrope
+    initial data (binary/initialize.cpp), EOS units of Binary::set_units."""
+    P = ini.binary_params()
+    h = helm_mod.Helm(table)
+    h.set_cgs_units(P["cm"], P["g"], P["s"], 1.0)
+    a = amr.AMR(physics=amr.PHYSICS_ZTWD, nf=13, bw=3, nx=8, reconstruction=amr.RECON_PPM, grid_dim=1.0,
+                z_reflect=1, mirror_refine_y=1, max_refine_level=levels, rho_floor=ini.BINARY["rho_floor"], cfl=0.3,
+                maxdtinc=1.25, max_bricks=4096, precision=prec, persistent_solve=persistent)
+    a.ztwd_set_eos(h)
+    a.ztwd_set_frame(P["omega"], P["omega"], 0.0, 0.0)
+    a.init()
+    U = ini.evaluate("binary", a.get_tree(), a.bw, a.nx, 1.0, 1, levels, ghosts=False)
+    thr = float(U[:, 0].max()) / DYNAMIC_RANGE  # min_refine_density from the root's first state
+    ini.build_tree(a, "binary", thr, 1.0, 1, levels, device=True, ghosts=False)
+    return a
+
+
+def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL):
+    """The 5-level ZTWD binary (q = 0.7, co-rotating frame, Helmholtz EOS):
+    BinaryDriver steps (hydro + multigrid gravity every substep, regrid every
+    8 steps) in the plain FP64 form, the persistent FP64 form and the mixed
+    persistent form; `total` steps each, steps [warmup, warmup + steps) timed;
+    the mixed form's potential, density and angular-momentum errors against
+    the FP64 form after `total` steps."""
+    helm_table = _load_module("helm_table", os.path.join(PKG, "helm_table.py"))
+    helm_mod = _load_module("helm_b200", os.path.join(PKG, "helm.py"))
+    tdir = tempfile.mkdtemp(prefix="ztwd_")
+    table = helm_table.ensure_table(tdir)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    forms = (("fp64", amr.PREC_FP64, 0), ("fp64_persistent", amr.PREC_FP64, 2), ("mixed", amr.PREC_MIXED, 2))
+    res = {"levels": ZT_LEVELS, "tol_l1": ZT_TOL, "steps_total": total, "timed_steps": steps,
+           "binary": dict(ini.BINARY), "regrid": "every 8 steps (binary_driver.cpp:426)"}
+    finals = {}
+    for name, prec, pers in forms:
+        a = ztwd_context(amr, ini, helm_mod, table, ZT_LEVELS, prec, pers)
+        stream = torch.cuda.ExternalStream(a.stream_handle())
+        times, cells, last = [], 0, 0.0
+        k0 = a.launch_count()
+        for s in range(total):
+            dt = a.max_dt()
+            if s > 0:
+                dt = min(1.25 * last, dt)
+            timed = warmup <= s < warmup + steps
+            if timed:
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+                n = a.get_zone_cnt()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+            last = a.ztwd_step(dt, ZT_TOL, DYNAMIC_RANGE, s)
+            if timed:
+                e1.record(stream)
+                e1.synchronize()
+                times.append(e0.elapsed_time(e1))
+                cells += n
+        t = a.get_tree()
+        finals[name] = {"U": a.download_state(), "phi": a.download_poisson()[0], "level": t["level"],
+                        "loc": t["loc"], "h": t["h"], "child_mask": t["child_mask"]}
+        ms = sum(times) / len(times)
+        res[name] = {"ms_per_step": ms, "value": cells / (sum(times) / 1000.0), "bricks": a.nbricks,
+                     "leaf_cells": int(a.get_zone_cnt()), "gpu_launches_total": a.launch_count() - k0}
+        a.close()
+    res["metric_unit"] = UNIT
+    res["speedup_mixed_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
+    f64, f32 = finals["fp64"], finals["mixed"]
+    if np.array_equal(f64["level"], f32["level"]) and np.array_equal(f64["loc"], f32["loc"]):
+        bw = 3
+        sl = (slice(None), slice(bw, -bw), slice(bw, -bw), slice(bw, -bw))
+        leaf = leaf_mask({"level": f64["level"], "child_mask": f64["child_mask"]}, 8)
+        vol = (f64["h"] ** 3)[:, None, None, None] * leaf
+        r64, r32 = f64["U"][:, 0][sl], f32["U"][:, 0][sl]
+        p64, p32 = f64["phi"][:, 1:-1, 1:-1, 1:-1], f32["phi"][:, 1:-1, 1:-1, 1:-1]
+        lz64, lz32 = (f64["U"][:, 4][sl] * vol).sum(), (f32["U"][:, 4][sl] * vol).sum()
+        res["errors_mixed_vs_fp64"] = {
+            "comparable": True, "steps": total,
+            "phi_rel_l2": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64)),
+            "rho_rel_l1": float(np.abs(r32 - r64).sum() / np.abs(r64).sum()),
+            "lz_total_rel": float(abs(lz32 - lz64) / abs(lz64)),
+            "against": "plain FP64 form (parity-tested against the reference's BINARY build)"}
+    else:
+        res["errors_mixed_vs_fp64"] = {"comparable": False, "why": "the forms regridded to different trees"}
+    if cpu_sample:
+        exe = os.path.join(ROOT, "oracle", "_ref", "ztwd_harness")
+        if os.path.exists(exe):
+            threads = os.cpu_count() or 1
+            env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+            try:
+                r = subprocess.run([exe, "time_ztwd", str(ZT_LEVELS), "2"], cwd=tdir, env=env, capture_output=True,
+                                   text=True, timeout=900)
+                row = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+                sec = row["seconds"][-1]
+                res["cpu_baseline"] = {
+                    "value": res["fp64"]["leaf_cells"] / sec, "unit": UNIT, "cores": row["threads"],
+                    "kind": "reference", "seconds_per_step": sec,
+                    "sample": "reference BINARY build (oracle/_ref/ztwd_harness, g++ -O2 -fopenmp): its second "
+                              "BinaryDriver step on the same 5-level binary (the first solves from the initial "
+                              "phi), leaf cells of our FP64 run per step"}
+            except (subprocess.TimeoutExpired, IndexError, ValueError, KeyError):
+                res["cpu_baseline"] = None
+    import shutil
+    shutil.rmtree(tdir, ignore_errors=True)
+    return res
+
+
 def run_case(case):
     """One small run of a single kernel family, for profiler captures:
     solve_L3      one Poisson solve (L1 tol 1e-6) of the 3-level star, mixed
@@ -681,6 +791,7 @@ def main():
     ap.add_argument("--json-out", default=None)
     ap.add_argument("--no-eos", action="store_true", help="skip the Helmholtz EOS throughput section")
     ap.add_argument("--no-batched", action="store_true", help="skip the random-field octree substep section")
+    ap.add_argument("--no-ztwd", action="store_true", help="skip the ZTWD binary section")
     ap.add_argument("--case", default=None, choices=["solve_L3", "substep_L4", "eos_1M"],
                     help="run one small case for a profiler capture and exit")
     args = ap.parse_args()
@@ -728,6 +839,9 @@ def main():
     batched = None
     if rank == 0 and not args.no_batched:
         batched = run_batched_substep(amr, ini, torch, max(args.steps, 3), max(args.warmup, 3))
+    ztwd = None
+    if rank == 0 and not args.no_ztwd:
+        ztwd = run_ztwd(amr, ini, torch, max(args.steps, 3), max(args.warmup, 3), not args.no_cpu_baseline)
     eos = None
     if rank == 0 and not args.no_eos:
         eos = run_eos(torch, max(args.steps, 3), max(args.warmup, 3), not args.no_cpu_baseline)
@@ -757,6 +871,7 @@ def main():
             "poisson_precision": pcheck,
             "helmholtz_eos": eos,
             "batched_substep": batched,
+            "ztwd_binary": ztwd,
         }
         line = json.dumps(out)
         print(line)

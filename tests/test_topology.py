@@ -74,3 +74,26 @@ def test_refine_from_flags_regrid_sequence():
     fl = initial.octant_flags(g["final_U"], 3.0)
     a.refine_from_flags(fl, True)
     assert same_tree(a.get_tree(), g, "final_")
+
+
+@pytest.mark.parametrize("name", ["ztwd_L2", "ztwd_L3"])
+def test_binary_initial_data_match_reference(name):
+    """initial.py's binary (binary/initialize.cpp + floor + synchronous
+    rotation) gives the reference harness's tree and refinement threshold,
+    and its leaf bricks' state to the last bits of pow/Lane-Emden."""
+    amr = load_amr()
+    g = load_golden(name)
+    L = int(g["init_level"].max())
+    a = amr.AMR(max_bricks=0, physics=2, nf=13, bw=3, nx=8, reconstruction=1, grid_dim=1.0, z_reflect=1,
+                max_refine_level=L, rho_floor=1e-10)
+    a.init()
+    U = initial.evaluate("binary", a.get_tree(), 3, 8, 1.0, 1, L, ghosts=False)
+    thr = U[:, 0].max() / 1e6
+    assert thr == g["extra"][6]
+    t, U = initial.build_tree(a, "binary", thr, 1.0, 1, L, device=False)
+    assert same_tree(t, g, "init_")
+    leaf = t["child_mask"] == 0
+    Ui, G = U[leaf][:, :, 3:-3, 3:-3, 3:-3], g["init_U"][leaf]
+    scale = np.abs(G).max(axis=(0, 2, 3, 4))
+    err = np.abs(Ui - G).max(axis=(0, 2, 3, 4)) / np.maximum(scale, 1e-300)
+    assert err.max() <= 1e-14, err
