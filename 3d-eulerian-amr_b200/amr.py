@@ -113,6 +113,8 @@ def load_library(path=LIB_PATH):
         if hasattr(lib, "amr_solve_phases"):
             lib.amr_solve_phases.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong), dp, I]
             lib.amr_solve_last_ms.argtypes = [P, ctypes.POINTER(ctypes.c_float)]
+            if hasattr(lib, "amr_solve_phase_waits"):
+                lib.amr_solve_phase_waits.argtypes = [P, dp, I, dp, ctypes.POINTER(ctypes.c_longlong)]
         _lib = lib
     return _lib
 
@@ -362,6 +364,18 @@ class AMR:
         by = (ctypes.c_double * n)()
         self._check(self.lib.amr_solve_phases(self.ctx, ms, cnt, by, n))
         return {k: {"ms": ms[i], "count": cnt[i], "bytes": by[i]} for i, k in enumerate(self.SOLVE_PHASES)}
+
+    def solve_phase_waits(self):
+        """Barrier share of each phase class (ms) and the relaxation level-sum time."""
+        n = len(self.SOLVE_PHASES)
+        w = np.zeros(n)
+        ls = ctypes.c_double()
+        cnt = ctypes.c_longlong()
+        self._check(self.lib.amr_solve_phase_waits(self.ctx, _dptr(w), n, ctypes.byref(ls), ctypes.byref(cnt)))
+        out = {k: w[i] for i, k in enumerate(self.SOLVE_PHASES)}
+        out["level_sum"] = ls.value
+        out["level_sum_count"] = cnt.value
+        return out
 
     def solve_last_ms(self):
         v = ctypes.c_float()

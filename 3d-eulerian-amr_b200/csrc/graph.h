@@ -49,6 +49,12 @@ struct Control {
     unsigned long long phase_ns[16];
     unsigned long long phase_n[16];
     double phase_bytes[16];  // algorithmic HBM bytes of those phases
+    // the part of each phase spent at its closing barrier (block 0: from its
+    // own arrival, after its share of the work, to the barrier's exit), and
+    // the time block 0 spends forming relaxation level sums after a barrier
+    unsigned long long phase_wait_ns[16];
+    unsigned long long level_sum_ns;
+    unsigned long long level_sum_n;
 };
 
 // phase classes of the persistent solve

@@ -519,6 +519,24 @@ int amr_solve_phases(amr_ctx* c, double* ms, long long* counts, double* bytes, i
     return AMR_OK;
 }
 
+// The barrier share of each phase class (wait_ms[PH_COUNT]) and the time of
+// the relaxation level sums formed after a barrier (*level_sum_ms, over
+// *level_sums of them), as block 0 of the persistent solve sees them.
+int amr_solve_phase_waits(amr_ctx* c, double* wait_ms, int n, double* level_sum_ms, long long* level_sums) {
+    if (!c || !wait_ms || !level_sum_ms || !level_sums || n < PH_COUNT) return AMR_ERR_ARG;
+    if (!c->gs) {
+        for (int p = 0; p < PH_COUNT; p++) wait_ms[p] = 0.0;
+        *level_sum_ms = 0.0;
+        *level_sums = 0;
+        return AMR_OK;
+    }
+    TRY(read_ctl(c));
+    for (int p = 0; p < PH_COUNT; p++) wait_ms[p] = c->gs->h_ctl->phase_wait_ns[p] * 1e-6;
+    *level_sum_ms = c->gs->h_ctl->level_sum_ns * 1e-6;
+    *level_sums = (long long)c->gs->h_ctl->level_sum_n;
+    return AMR_OK;
+}
+
 // Duration of the most recent persistent solve launch (CUDA events recorded
 // around it on the launching stream).
 int amr_solve_last_ms(amr_ctx* c, float* ms) {

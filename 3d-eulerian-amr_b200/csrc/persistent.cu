@@ -86,6 +86,7 @@ struct Solver {
     unsigned long long* ph_ns;
     unsigned* ph_n;
     double* ph_bytes;
+    unsigned long long* ph_wait;  // [PH_COUNT], then level-sum time and count
 
     __device__ static unsigned long long now() {
         unsigned long long t;
@@ -95,9 +96,11 @@ struct Solver {
 
     // barrier closing a phase of class ph
     __device__ bool sync(int ph, int units) {
+        const unsigned long long t_arrive = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
         const bool ok = grid_sync(a.bar, bar_target);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             const unsigned long long t = now();
+            ph_wait[ph] += t - t_arrive;
             ph_ns[ph] += t - t_last;
             ph_n[ph]++;
             ph_bytes[ph] += (double)units * phase_bytes(ph);
@@ -181,10 +184,22 @@ struct Solver {
     // Poisson::vcycle_relax sum over level l (poisson.cpp:107, nested as the
     // recursion adds it) from buffer `buf` of the per-brick sums
     __device__ double level_sum(int l, const double* buf) {
-        if (l == 0) return __ldcg(buf + a.L.slots[a.L.off[0]]);
-        __syncthreads();
-        if (a.L.max_cnt <= NEST_SMEM) return nested_sum_smem(a.L, buf, l, false, nbuf);
-        return nested_sum_block(a.L, a.bt.child, buf, nest, l, false);
+        const unsigned long long t0 = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
+        double r;
+        if (l == 0) {
+            r = __ldcg(buf + a.L.slots[a.L.off[0]]);
+        } else {
+            __syncthreads();
+            if (a.L.max_cnt <= NEST_SMEM)
+                r = nested_sum_smem(a.L, buf, l, false, nbuf);
+            else
+                r = nested_sum_block(a.L, a.bt.child, buf, nest, l, false);
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            ph_wait[PH_COUNT] += now() - t0;
+            ph_wait[PH_COUNT + 1]++;
+        }
+        return r;
     }
 
     // relax_until (poisson.cpp:66-70, 74-78): ghosts, one pass, then passes
@@ -320,9 +335,12 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
     __shared__ unsigned long long s_ph_ns[PH_COUNT];
     __shared__ unsigned s_ph_n[PH_COUNT];
     __shared__ double s_ph_bytes[PH_COUNT];
+    __shared__ unsigned long long s_ph_wait[PH_COUNT + 2];
     s.ph_ns = s_ph_ns;
     s.ph_n = s_ph_n;
     s.ph_bytes = s_ph_bytes;
+    s.ph_wait = s_ph_wait;
+    if (threadIdx.x < PH_COUNT + 2) s_ph_wait[threadIdx.x] = 0;
     s.t_last = Solver<CT>::now();
     if (threadIdx.x < PH_COUNT) {
         s_ph_ns[threadIdx.x] = 0;
@@ -361,7 +379,10 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
                 c->phase_ns[p] += s.ph_ns[p];
                 c->phase_n[p] += s.ph_n[p];
                 c->phase_bytes[p] += s.ph_bytes[p];
+                c->phase_wait_ns[p] += s.ph_wait[p];
             }
+            c->level_sum_ns += s.ph_wait[PH_COUNT];
+            c->level_sum_n += s.ph_wait[PH_COUNT + 1];
         }
     }
 }

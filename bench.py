@@ -218,6 +218,7 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
     st0 = a.stats()
     persistent = form in ("persistent", "mixed")
     ph0 = a.solve_phases() if persistent else None
+    w0 = a.solve_phase_waits() if persistent else None
     solve_ms = []
     k0 = a.launch_count()
     sampler = ClockSampler(local)
@@ -253,6 +254,10 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
                              "bytes_per_launch": sum(v["bytes"] for v in d.values()) / launches,
                              "phase_ms_per_step": {k: round(v["ms"] / args.steps, 4) for k, v in d.items()},
                              "phases_per_step": {k: v["count"] / args.steps for k, v in d.items()}}
+        w1 = a.solve_phase_waits()
+        res["persistent"]["barrier_ms_per_step"] = {k: round((w1[k] - w0[k]) / args.steps, 4) for k in ph1}
+        res["persistent"]["level_sum_ms_per_step"] = round((w1["level_sum"] - w0["level_sum"]) / args.steps, 4)
+        res["persistent"]["level_sums_per_step"] = (w1["level_sum_count"] - w0["level_sum_count"]) / args.steps
     # state after warm-up + timed steps, for the error of one form against another
     res["final"] = {"U": a.download_state(), "phi": a.download_poisson()[0], "level": a.get_tree()["level"],
                     "loc": a.get_tree()["loc"]}
@@ -626,6 +631,10 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL):
             if s > 0:
                 dt = min(1.25 * last, dt)
             timed = warmup <= s < warmup + steps
+            if s == warmup:
+                ph0 = a.solve_phases() if pers else None
+                w0 = a.solve_phase_waits() if pers else None
+                st0 = a.stats()
             if timed:
                 with torch.cuda.stream(stream):
                     flush.zero_()
@@ -638,12 +647,24 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL):
                 e1.synchronize()
                 times.append(e0.elapsed_time(e1))
                 cells += n
+            if s == warmup + steps - 1:
+                st1 = a.stats()
+                if pers:
+                    ph1, w1 = a.solve_phases(), a.solve_phase_waits()
+                    phase_split = {
+                        "phase_ms_per_step": {k: round((ph1[k]["ms"] - ph0[k]["ms"]) / steps, 3) for k in ph1},
+                        "phases_per_step": {k: (ph1[k]["count"] - ph0[k]["count"]) / steps for k in ph1},
+                        "barrier_ms_per_step": {k: round((w1[k] - w0[k]) / steps, 3) for k in ph1},
+                        "level_sum_ms_per_step": round((w1["level_sum"] - w0["level_sum"]) / steps, 3)}
         t = a.get_tree()
         finals[name] = {"U": a.download_state(), "phi": a.download_poisson()[0], "level": t["level"],
                         "loc": t["loc"], "h": t["h"], "child_mask": t["child_mask"]}
         ms = sum(times) / len(times)
         res[name] = {"ms_per_step": ms, "value": cells / (sum(times) / 1000.0), "bricks": a.nbricks,
-                     "leaf_cells": int(a.get_zone_cnt()), "gpu_launches_total": a.launch_count() - k0}
+                     "leaf_cells": int(a.get_zone_cnt()), "gpu_launches_total": a.launch_count() - k0,
+                     "relax_calls_per_step": (st1["relax_calls"] - st0["relax_calls"]) / steps}
+        if pers:
+            res[name]["persistent"] = phase_split
         a.close()
     res["metric_unit"] = UNIT
     res["speedup_mixed_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
@@ -753,6 +774,8 @@ def roofline_persistent(res):
             "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
             "algorithmic_bytes_per_launch": p["bytes_per_launch"], "ms_per_launch": p["ms_per_launch"],
             "phase_ms_per_step": p["phase_ms_per_step"], "phases_per_step": p["phases_per_step"],
+            "barrier_ms_per_step": p.get("barrier_ms_per_step"),
+            "level_sum_ms_per_step": p.get("level_sum_ms_per_step"),
             "note": "latency-bound: the reference's V-cycle is a chain of dependent per-level steps "
                     "(about 700 grid barriers per step here); the relaxation sweeps run in shared memory"}
 

@@ -251,6 +251,11 @@ int amr_solve_phases(amr_ctx* ctx, double* ms, long long* counts, double* bytes,
 /* Duration (CUDA events on the launching stream) of the most recent
  * persistent solve kernel. */
 int amr_solve_last_ms(amr_ctx* ctx, float* ms);
+/* Of those phase times, the part spent at each phase's closing grid barrier
+ * (block 0, from its arrival to the barrier's exit: the slowest block's extra
+ * work plus the barrier itself), and the time spent forming the relaxation
+ * loops' level sums after their barriers. */
+int amr_solve_phase_waits(amr_ctx* ctx, double* wait_ms, int n, double* level_sum_ms, long long* level_sums);
 int amr_profile_enable(amr_ctx* ctx, int on);
 int amr_profile_reset(amr_ctx* ctx);
 int amr_profile_get(amr_ctx* ctx, int cls, double* ms, long long* launches, const char** name);
