@@ -621,6 +621,7 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL):
     res = {"levels": ZT_LEVELS, "tol_l1": ZT_TOL, "steps_total": total, "timed_steps": steps,
            "binary": dict(ini.BINARY), "regrid": "every 8 steps (binary_driver.cpp:426)"}
     finals = {}
+    snaps = {}  # state after steps 1 and 10, for the growth of the mixed form's error
     for name, prec, pers in forms:
         a = ztwd_context(amr, ini, helm_mod, table, ZT_LEVELS, prec, pers)
         stream = torch.cuda.ExternalStream(a.stream_handle())
@@ -642,6 +643,10 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL):
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
             last = a.ztwd_step(dt, ZT_TOL, DYNAMIC_RANGE, s)
+            if s + 1 in (1, 10) and name in ("fp64", "mixed"):
+                t = a.get_tree()
+                snaps[(name, s + 1)] = {"U": a.download_state(), "phi": a.download_poisson()[0], "level": t["level"],
+                                        "loc": t["loc"], "h": t["h"], "child_mask": t["child_mask"]}
             if timed:
                 e1.record(stream)
                 e1.synchronize()
@@ -668,8 +673,9 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL):
         a.close()
     res["metric_unit"] = UNIT
     res["speedup_mixed_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
-    f64, f32 = finals["fp64"], finals["mixed"]
-    if np.array_equal(f64["level"], f32["level"]) and np.array_equal(f64["loc"], f32["loc"]):
+    def zt_errors(f64, f32, steps):
+        if not (np.array_equal(f64["level"], f32["level"]) and np.array_equal(f64["loc"], f32["loc"])):
+            return {"comparable": False, "steps": steps, "why": "the forms regridded to different trees"}
         bw = 3
         sl = (slice(None), slice(bw, -bw), slice(bw, -bw), slice(bw, -bw))
         leaf = leaf_mask({"level": f64["level"], "child_mask": f64["child_mask"]}, 8)
@@ -677,14 +683,14 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL):
         r64, r32 = f64["U"][:, 0][sl], f32["U"][:, 0][sl]
         p64, p32 = f64["phi"][:, 1:-1, 1:-1, 1:-1], f32["phi"][:, 1:-1, 1:-1, 1:-1]
         lz64, lz32 = (f64["U"][:, 4][sl] * vol).sum(), (f32["U"][:, 4][sl] * vol).sum()
-        res["errors_mixed_vs_fp64"] = {
-            "comparable": True, "steps": total,
-            "phi_rel_l2": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64)),
-            "rho_rel_l1": float(np.abs(r32 - r64).sum() / np.abs(r64).sum()),
-            "lz_total_rel": float(abs(lz32 - lz64) / abs(lz64)),
-            "against": "plain FP64 form (parity-tested against the reference's BINARY build)"}
-    else:
-        res["errors_mixed_vs_fp64"] = {"comparable": False, "why": "the forms regridded to different trees"}
+        return {"comparable": True, "steps": steps,
+                "phi_rel_l2": float(np.linalg.norm(p32 - p64) / np.linalg.norm(p64)),
+                "rho_rel_l1": float(np.abs(r32 - r64).sum() / np.abs(r64).sum()),
+                "lz_total_rel": float(abs(lz32 - lz64) / abs(lz64))}
+
+    res["errors_mixed_vs_fp64"] = zt_errors(finals["fp64"], finals["mixed"], total)
+    res["errors_mixed_vs_fp64"]["against"] = "plain FP64 form (parity-tested against the reference's BINARY build)"
+    res["errors_mixed_vs_fp64"]["growth"] = [zt_errors(snaps[("fp64", k)], snaps[("mixed", k)], k) for k in (1, 10)]
     if cpu_sample:
         exe = os.path.join(ROOT, "oracle", "_ref", "ztwd_harness")
         if os.path.exists(exe):
@@ -714,7 +720,9 @@ def run_case(case):
                   persistent form (k_solve_persistent)
     substep_L4    two fused substeps on the 5-level random-field octree
                   (k_substep_fused, FP64)
-    eos_1M        2^20 points, forward and inverse Helmholtz EOS"""
+    eos_1M        2^20 points, forward and inverse Helmholtz EOS
+    ztwd_L5       two BinaryDriver steps of the 5-level ZTWD binary, plain FP64
+                  (k_zt_flux, k_zt_add_difs, k_zt_max_dt, ... as separate launches)"""
     import torch
     amr, ini = load_amr()
     if case == "solve_L3":
@@ -755,6 +763,21 @@ def run_case(case):
         torch.cuda.synchronize()
         print(json.dumps({"case": case, "points": n, "bad": int((st != 0).sum())}))
         h.close()
+        import shutil
+        shutil.rmtree(tdir, ignore_errors=True)
+    elif case == "ztwd_L5":
+        helm_table = _load_module("helm_table", os.path.join(PKG, "helm_table.py"))
+        helm_mod = _load_module("helm_b200", os.path.join(PKG, "helm.py"))
+        tdir = tempfile.mkdtemp(prefix="ztwd_")
+        a = ztwd_context(amr, ini, helm_mod, helm_table.ensure_table(tdir), ZT_LEVELS, amr.PREC_FP64, 0)
+        last = 0.0
+        for s in range(2):
+            dt = a.max_dt()
+            dt = min(1.25 * last, dt) if s else dt
+            last = a.ztwd_step(dt, ZT_TOL, DYNAMIC_RANGE, s)
+        a.synchronize()
+        print(json.dumps({"case": case, "bricks": a.nbricks, "dt": last}))
+        a.close()
         import shutil
         shutil.rmtree(tdir, ignore_errors=True)
     else:
@@ -815,7 +838,7 @@ def main():
     ap.add_argument("--no-eos", action="store_true", help="skip the Helmholtz EOS throughput section")
     ap.add_argument("--no-batched", action="store_true", help="skip the random-field octree substep section")
     ap.add_argument("--no-ztwd", action="store_true", help="skip the ZTWD binary section")
-    ap.add_argument("--case", default=None, choices=["solve_L3", "substep_L4", "eos_1M"],
+    ap.add_argument("--case", default=None, choices=["solve_L3", "substep_L4", "eos_1M", "ztwd_L5"],
                     help="run one small case for a profiler capture and exit")
     args = ap.parse_args()
     if args.case:
