@@ -41,6 +41,13 @@ class AmrConfig(ctypes.Structure):
     ]
 
 
+class BinaryHeader(ctypes.Structure):
+    """Binary::write's root header (binary/binary.cpp:70-94)."""
+    _fields_ = [(k, ctypes.c_double) for k in ("l1x", "h", "M1", "fill_factor", "n", "R1", "q", "a", "K1", "K2",
+                                                "phi0_1", "phi0_2", "Omega", "phase", "Omega0")] + [
+        ("accretor_type", ctypes.c_int), ("donor_type", ctypes.c_int), ("dummy", ctypes.c_ubyte)]
+
+
 class AmrError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__("%s (%d): %s" % (ERRORS.get(code, "AMR_ERR"), code, msg))
@@ -110,6 +117,9 @@ def load_library(path=LIB_PATH):
             lib.amr_ztwd_set_frame.argtypes = [P, D, D, D, D]
             lib.amr_ztwd_pot.argtypes = [P, I]
             lib.amr_ztwd_step.argtypes = [P, D, D, D, I, dp]
+        if hasattr(lib, "amr_write_checkpoint"):
+            lib.amr_write_checkpoint.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(BinaryHeader), D]
+            lib.amr_read_checkpoint.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(BinaryHeader)]
         if hasattr(lib, "amr_solve_phases"):
             lib.amr_solve_phases.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong), dp, I]
             lib.amr_solve_last_ms.argtypes = [P, ctypes.POINTER(ctypes.c_float)]
@@ -411,4 +421,16 @@ class AMR:
         self._check(self.lib.amr_ztwd_step(self.ctx, float(dt), float(tol), float(dynamic_range), int(step_index),
                                            ctypes.byref(used)))
         return used.value
+
+    # ---- checkpoints (X.*.chk of the reference) --------------------------------
+    def write_checkpoint(self, path, header=None, refine_alpha=1.0):
+        """header: a BinaryHeader for BINARY-build files, None otherwise."""
+        hp = ctypes.byref(header) if header is not None else None
+        self._check(self.lib.amr_write_checkpoint(self.ctx, os.fsencode(path), hp, float(refine_alpha)))
+
+    def read_checkpoint(self, path, binary=False):
+        """Loads tree + state; returns the BinaryHeader when binary=True."""
+        h = BinaryHeader() if binary else None
+        self._check(self.lib.amr_read_checkpoint(self.ctx, os.fsencode(path), ctypes.byref(h) if binary else None))
+        return h
 

@@ -220,6 +220,26 @@ int amr_ztwd_pot(amr_ctx* ctx, int mode);
  * amr_graph_solve. */
 int amr_ztwd_step(amr_ctx* ctx, double dt, double tol, double dynamic_range, int step_index, double* dt_used);
 
+/* ---- checkpoints ------------------------------------------------------------
+ * Files in the reference's checkpoint format (X.*.chk): the BINARY build's
+ * root header (Binary::write / read, binary/binary.cpp:70-94, 175-203) when
+ * hdr is not NULL, then every brick in depth-first pre-order as
+ * GridNode::write / Grid::write give it (grid/grid_node.cpp:29-57,
+ * grid/grid.cpp:104-146): h, h0, time, offsets and origin, the flow-off
+ * vector, the GNX^3 x NF state (ghost cells included, x outermost), the child
+ * flags, refine_alpha and the age.  The reader rebuilds the tree, uploads the
+ * state and sets the time and the root's flow-off; it checks the offsets and
+ * the file length against the context's BW, GNX and NF (AMR_ERR_STATE).
+ * The potential is not part of the format (Binary::pot_from_grid rebuilds
+ * it from the pot field). */
+typedef struct amr_binary_header {
+    double l1x, h, M1, fill_factor, n, R1, q, a, K1, K2, phi0_1, phi0_2, Omega, phase, Omega0;
+    int accretor_type, donor_type;
+    unsigned char dummy;
+} amr_binary_header;
+int amr_write_checkpoint(amr_ctx* ctx, const char* path, const amr_binary_header* hdr, double refine_alpha);
+int amr_read_checkpoint(amr_ctx* ctx, const char* path, amr_binary_header* hdr);
+
 /* ---- graph-captured forms --------------------------------------------------
  * The same step and solve with every loop decided on the device: the V-cycle
  * loop and the relaxation loops are CUDA-graph WHILE nodes, the CFL step is

@@ -16,6 +16,11 @@
 //       (before the first step) and <out.bin> (after the last).
 //   time_ztwd <maxlevel> <nsteps>
 //       the same, printing wall time per step (JSON) instead of dumping.
+//   ztwd_chk <maxlevel> <nsteps> <out.bin> <out.chk>
+//       as ztwd, then also the reference's checkpoint of the final state
+//       (Binary::write, binary/binary.cpp:70-94).
+//   read_chk <in.chk> <out.bin>
+//       Binary::read of a checkpoint (binary/binary.cpp:175-203), then a dump.
 //
 // Binary parameters (a stand-in for the missing SCF model X.start.chk):
 // mass ratio q = 0.7, separation a = 0.5, donor radius R2 = 0.17 (its Roche
@@ -95,6 +100,21 @@ static Binary* build_tree(int maxlevel) {
 }
 
 int main(int argc, char* argv[]) {
+    if (argc == 4 && std::string(argv[1]) == "read_chk") {
+        set_binary_parameters();
+        Binary* root = new Binary;
+        root->init();
+        FILE* fp = fopen(argv[2], "rb");
+        if (!fp) {
+            perror(argv[2]);
+            return 3;
+        }
+        root->read(fp);
+        fclose(fp);
+        std::vector<double> extra = {Binary::K1, Binary::Omega, Binary::Omega0, Binary::q, Binary::M1};
+        dump(argv[3], root, root, root->get_time(), extra);
+        return 0;
+    }
     if (argc < 4) {
         fprintf(stderr, "usage: %s ztwd|time_ztwd maxlevel nsteps [out.bin]\n", argv[0]);
         return 2;
@@ -103,7 +123,8 @@ int main(int argc, char* argv[]) {
     const int maxlevel = atoi(argv[2]);
     const int nsteps = atoi(argv[3]);
     const bool timing = mode == "time_ztwd";
-    if (!timing && (mode != "ztwd" || argc < 5)) {
+    const bool chk = mode == "ztwd_chk";
+    if (!timing && !((mode == "ztwd" && argc >= 5) || (chk && argc >= 6))) {
         fprintf(stderr, "bad arguments\n");
         return 2;
     }
@@ -140,5 +161,14 @@ int main(int argc, char* argv[]) {
     extra.push_back(double(nsteps));
     for (double d : dts) extra.push_back(d);
     dump(argv[4], root, root, root->get_time(), extra);
+    if (chk) {
+        FILE* fp = fopen(argv[5], "wb");
+        if (!fp) {
+            perror(argv[5]);
+            return 3;
+        }
+        root->write(fp);
+        fclose(fp);
+    }
     return 0;
 }
