@@ -117,6 +117,10 @@ def load_library(path=LIB_PATH):
             lib.amr_ztwd_set_frame.argtypes = [P, D, D, D, D]
             lib.amr_ztwd_pot.argtypes = [P, I]
             lib.amr_ztwd_step.argtypes = [P, D, D, D, I, dp]
+        if hasattr(lib, "amr_state_sum"):
+            lib.amr_state_sum.argtypes = [P, I, dp]
+            lib.amr_mass_sum.argtypes = [P, I, dp]
+            lib.amr_sum_lz.argtypes = [P, dp]
         if hasattr(lib, "amr_write_checkpoint"):
             lib.amr_write_checkpoint.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(BinaryHeader), D]
             lib.amr_read_checkpoint.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(BinaryHeader)]
@@ -433,4 +437,22 @@ class AMR:
         h = BinaryHeader() if binary else None
         self._check(self.lib.amr_read_checkpoint(self.ctx, os.fsencode(path), ctypes.byref(h) if binary else None))
         return h
+
+    # ---- diagnostics ------------------------------------------------------------
+    def state_sum(self, field=0):
+        """GridNode::state_sum of one field: (sum u dV, its x, y, z moments)."""
+        out = np.zeros(4)
+        self._check(self.lib.amr_state_sum(self.ctx, int(field), _dptr(out)))
+        return out
+
+    def mass_sum(self, frac):
+        """Binary::mass_sum: (mass, centre of mass x, y, z) of the accretor (0) or donor (1)."""
+        out = np.zeros(4)
+        self._check(self.lib.amr_mass_sum(self.ctx, int(frac), _dptr(out)))
+        return out
+
+    def sum_lz(self):
+        out = np.zeros(1)
+        self._check(self.lib.amr_sum_lz(self.ctx, _dptr(out)))
+        return float(out[0])
 

@@ -220,6 +220,18 @@ int amr_ztwd_pot(amr_ctx* ctx, int mode);
  * amr_graph_solve. */
 int amr_ztwd_step(amr_ctx* ctx, double dt, double tol, double dynamic_range, int step_index, double* dt_used);
 
+/* ---- diagnostics (device reductions over the uncovered cells) -------------
+ * GridNode::state_sum for one field (grid/grid_node.cpp:1489-1527): out[4] =
+ * (sum u h^3, sum u h^3 x, sum u h^3 y, sum u h^3 z).  Binary::mass_sum
+ * (binary/binary.cpp:28-68, ZTWD; frac 0 the accretor's density, 1 the
+ * donor's): out[4] = (mass, centre of mass x, y, z; z = 0 with Z_REFLECT).
+ * Binary::sum_lz (binary.cpp:363-388, ZTWD): the total angular momentum.
+ * Per-brick sums in the reference's loop order, added over the tree in its
+ * recursion order (results equal the reference's one-thread run). */
+int amr_state_sum(amr_ctx* ctx, int field, double* out);
+int amr_mass_sum(amr_ctx* ctx, int frac, double* out);
+int amr_sum_lz(amr_ctx* ctx, double* out);
+
 /* ---- checkpoints ------------------------------------------------------------
  * Files in the reference's checkpoint format (X.*.chk): the BINARY build's
  * root header (Binary::write / read, binary/binary.cpp:70-94, 175-203) when

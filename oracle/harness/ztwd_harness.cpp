@@ -160,6 +160,15 @@ int main(int argc, char* argv[]) {
     }
     extra.push_back(double(nsteps));
     for (double d : dts) extra.push_back(d);
+    // diagnostics of the final state: Binary::mass_sum of both stars,
+    // Binary::sum_lz, GridNode::state_sum of the density
+    for (int frac = 0; frac < 2; frac++) {
+        const Vector<Real, 4> m = root->mass_sum(frac);
+        for (int q = 0; q < 4; q++) extra.push_back(m[q]);
+    }
+    extra.push_back(root->sum_lz());
+    const Vector<State, 4> ss = root->state_sum();
+    for (int q = 0; q < 4; q++) extra.push_back(ss[q][0]);
     dump(argv[4], root, root, root->get_time(), extra);
     if (chk) {
         FILE* fp = fopen(argv[5], "wb");

@@ -120,3 +120,24 @@ def test_ztwd_calls_need_the_eos(gpu):
         a.enforce_boundaries()
     assert e.value.code == -6  # AMR_ERR_STATE
     a.close()
+
+
+@pytest.mark.gpu
+def test_ztwd_diagnostics_match_reference(gpu, table_path):
+    """Binary::mass_sum of both stars, Binary::sum_lz and GridNode::state_sum
+    of the density, on the reference's own final state of ztwd_L2: equal to
+    the reference's one-thread values bit for bit (same data, same order)."""
+    g = load_golden("ztwd_L2")
+    nsteps = int(g["args"][1])
+    diag = g["extra"][8 + nsteps:]
+    a = gpu.AMR(**ztwd_config(int(g["final_level"].max())))
+    a.load_tree(g["final_level"], g["final_loc"], g["final_age"])
+    bw = a.bw
+    U = np.zeros((a.nbricks, a.nf, a.gnx, a.gnx, a.gnx))
+    U[:, :, bw:-bw, bw:-bw, bw:-bw] = g["final_U"]
+    a.upload_state(U)
+    assert np.array_equal(a.mass_sum(0), diag[0:4])
+    assert np.array_equal(a.mass_sum(1), diag[4:8])
+    assert a.sum_lz() == diag[8]
+    assert np.array_equal(a.state_sum(0), diag[9:13])
+    a.close()
