@@ -124,6 +124,7 @@ def load_library(path=LIB_PATH):
         if hasattr(lib, "amr_write_checkpoint"):
             lib.amr_write_checkpoint.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(BinaryHeader), D]
             lib.amr_read_checkpoint.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(BinaryHeader)]
+            lib.amr_write_output.argtypes = [P, ctypes.c_char_p]
         if hasattr(lib, "amr_solve_phases"):
             lib.amr_solve_phases.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong), dp, I]
             lib.amr_solve_last_ms.argtypes = [P, ctypes.POINTER(ctypes.c_float)]
@@ -144,6 +145,44 @@ def default_config(**kw):
         else:
             setattr(cfg, k, v)
     return cfg
+
+
+def read_output(path):
+    """Parse a file of amr_write_output: dict with time, per-brick level, loc,
+    offset, age, child_mask, h, U [n, nf, nx, nx, nx] and phi [n, nx, nx, nx]
+    (None without self-gravity)."""
+    with open(path, "rb") as f:
+        data = f.read()
+    if data[:8] != b"AMRB200O":
+        raise ValueError("not an amr_write_output file")
+    nf, nx, bw, n, has_phi = np.frombuffer(data, np.int32, 5, 8)
+    pos = 8 + 32
+    time = float(np.frombuffer(data, np.float64, 1, pos)[0])
+    pos += 8
+    cells = nx * nx * nx
+    out = {k: [] for k in ("level", "loc", "offset", "age", "child_mask", "h", "U", "phi")}
+    for _ in range(n):
+        rec = np.frombuffer(data, np.int32, 9, pos)
+        pos += 36
+        out["level"].append(rec[0])
+        out["loc"].append(rec[1:4])
+        out["offset"].append(rec[4:7])
+        out["age"].append(rec[7])
+        out["child_mask"].append(rec[8])
+        out["h"].append(np.frombuffer(data, np.float64, 1, pos)[0])
+        pos += 8
+        out["U"].append(np.frombuffer(data, np.float64, nf * cells, pos).reshape(nf, nx, nx, nx))
+        pos += 8 * nf * cells
+        if has_phi:
+            out["phi"].append(np.frombuffer(data, np.float64, cells, pos).reshape(nx, nx, nx))
+            pos += 8 * cells
+    if pos != len(data):
+        raise ValueError("trailing bytes in %s" % path)
+    res = {k: np.array(v) for k, v in out.items() if k != "phi"}
+    res["phi"] = np.array(out["phi"]) if has_phi else None
+    res["time"] = time
+    res["bw"] = int(bw)
+    return res
 
 
 def _dptr(a):
@@ -431,6 +470,10 @@ class AMR:
         """header: a BinaryHeader for BINARY-build files, None otherwise."""
         hp = ctypes.byref(header) if header is not None else None
         self._check(self.lib.amr_write_checkpoint(self.ctx, os.fsencode(path), hp, float(refine_alpha)))
+
+    def write_output(self, path):
+        """Headless output (amr_write_output); read it back with read_output."""
+        self._check(self.lib.amr_write_output(self.ctx, os.fsencode(path)))
 
     def read_checkpoint(self, path, binary=False):
         """Loads tree + state; returns the BinaryHeader when binary=True."""

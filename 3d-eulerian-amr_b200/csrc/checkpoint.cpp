@@ -218,4 +218,65 @@ int amr_read_checkpoint(amr_ctx* c, const char* path, amr_binary_header* hdr) {
     return amr_set_time(c, recs[0].time);
 }
 
+// Headless output (the per-brick data GridNode::output writes to Silo,
+// grid/grid_node.cpp:1422-1487, without the Silo library): "AMRB200O",
+// int32 {nf, nx, bw, nbricks, has_phi, 0, 0, 0}, double time, then per brick
+// in depth-first pre-order int32 {level, loc[3], offset[3], age,
+// child_mask}, double h, the interior state [nf][nx][nx][nx] and, with
+// self-gravity, the interior potential [nx][nx][nx].
+int amr_write_output(amr_ctx* c, const char* path) {
+    if (!c || !path) return AMR_ERR_ARG;
+    if (!c->has_device) {
+        c->err = "context has no device pool";
+        return AMR_ERR_NODEVICE;
+    }
+    const Geom& g = c->geom;
+    const int n = (int)c->order.size();
+    std::vector<double> U((size_t)n * g.ucount);
+    TRY(amr_download_state(c, U.data()));
+    const bool phi = has_gravity(c) && c->d_bphi != nullptr;
+    std::vector<double> P;
+    if (phi) {
+        P.resize((size_t)8 * n * g.pnx3);
+        TRY(amr_download_poisson(c, P.data()));
+    }
+    File f;
+    f.fp = fopen(path, "wb");
+    if (!f.fp) {
+        c->err = std::string("cannot open ") + path;
+        return AMR_ERR_ARG;
+    }
+    const int hdr[8] = {g.nf, g.nx, g.bw, n, phi ? 1 : 0, 0, 0, 0};
+    bool ok = fwrite("AMRB200O", 1, 8, f.fp) == 8 && fwrite(hdr, sizeof(int), 8, f.fp) == 8 && put(f.fp, c->time);
+    std::vector<double> buf((size_t)g.nf * g.nx * g.nx * g.nx);
+    for (int e = 0; e < n && ok; e++) {
+        const Node* nd = c->order[e];
+        int cm = 0;
+        for (int q = 0; q < 8; q++) cm |= nd->child[q] ? 1 << q : 0;
+        const int rec[9] = {nd->level, nd->loc[0], nd->loc[1], nd->loc[2], nd->off[0], nd->off[1], nd->off[2],
+                            nd->age, cm};
+        ok = fwrite(rec, sizeof(int), 9, f.fp) == 9 && put(f.fp, nd->h);
+        const double* Ub = U.data() + (size_t)e * g.ucount;
+        size_t m = 0;
+        for (int l = 0; l < g.nf; l++)
+            for (int k = g.bw; k < g.bw + g.nx; k++)
+                for (int j = g.bw; j < g.bw + g.nx; j++)
+                    for (int i = g.bw; i < g.bw + g.nx; i++) buf[m++] = Ub[(size_t)l * g.gnx3 + (k * g.gnx + j) * g.gnx + i];
+        ok = ok && fwrite(buf.data(), sizeof(double), m, f.fp) == m;
+        if (phi && ok) {
+            const double* pb = P.data() + (size_t)e * g.pnx3;  // phi is the first of the 8 arrays
+            m = 0;
+            for (int k = 1; k <= g.nx; k++)
+                for (int j = 1; j <= g.nx; j++)
+                    for (int i = 1; i <= g.nx; i++) buf[m++] = pb[(k * g.pnx + j) * g.pnx + i];
+            ok = fwrite(buf.data(), sizeof(double), m, f.fp) == m;
+        }
+    }
+    if (!ok) {
+        c->err = std::string("write failed: ") + path;
+        return AMR_ERR_STATE;
+    }
+    return AMR_OK;
+}
+
 }  // extern "C"

@@ -251,6 +251,13 @@ typedef struct amr_binary_header {
 } amr_binary_header;
 int amr_write_checkpoint(amr_ctx* ctx, const char* path, const amr_binary_header* hdr, double refine_alpha);
 int amr_read_checkpoint(amr_ctx* ctx, const char* path, amr_binary_header* hdr);
+/* Headless output in place of the reference's Silo files (GridNode::output,
+ * grid/grid_node.cpp:1422-1487): "AMRB200O", int32 {nf, nx, bw, nbricks,
+ * has_phi, 0, 0, 0}, double time, then per brick in depth-first pre-order
+ * int32 {level, loc[3], offset[3], age, child_mask}, double h, the interior
+ * state [nf][nx][nx][nx] and, with self-gravity, the interior potential
+ * [nx][nx][nx] (little-endian, no padding).  amr.read_output parses it. */
+int amr_write_output(amr_ctx* ctx, const char* path);
 
 /* ---- graph-captured forms --------------------------------------------------
  * The same step and solve with every loop decided on the device: the V-cycle

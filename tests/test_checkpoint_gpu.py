@@ -95,3 +95,28 @@ def test_euler_checkpoint_roundtrip(gpu, tmp_path):
     assert e.value.code == -6
     for x in (a, b, c):
         x.close()
+
+
+@pytest.mark.gpu
+def test_headless_output(gpu, tmp_path):
+    """amr_write_output of a self-gravitating run: tree, interiors and the
+    interior potential as the device holds them."""
+    import importlib.util
+    from conftest import PKG
+    spec = importlib.util.spec_from_file_location("amr_initial", os.path.join(PKG, "initial.py"))
+    initial = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(initial)
+    a = gpu.AMR(physics=gpu.PHYSICS_EULER_GRAVITY, max_refine_level=2, grid_dim=0.5, z_reflect=0, max_bricks=512)
+    initial.build_tree(a, "polytrope", 1e-6, 0.5, 0, 2, device=True)
+    a.grav_step(a.max_dt(), 1e-6, 1e6, 0)
+    path = str(tmp_path / "out.bin")
+    a.write_output(path)
+    o = gpu.read_output(path)
+    t = a.get_tree()
+    for k in ("level", "loc", "offset", "age", "child_mask", "h"):
+        assert np.array_equal(o[k], t[k]), k
+    bw = a.bw
+    assert np.array_equal(o["U"], a.download_state()[:, :, bw:-bw, bw:-bw, bw:-bw])
+    assert np.array_equal(o["phi"], a.download_poisson()[0][:, 1:-1, 1:-1, 1:-1])
+    assert o["time"] == a.get_time()
+    a.close()
