@@ -12,20 +12,17 @@
 
 namespace amr {
 
-// The sums of squares that decide the sweep loop are formed in CT: FP64 in
-// the plain form, FP32 in the mixed form (whose correction is FP32 anyway;
-// its loop may then stop a sweep earlier or later than the FP64 form's).
 template <int NX, typename CT = double>
 struct RelaxSmem {
     static constexpr int P = NX + 2, P3 = P * P * P, NT = NX * NX * NX, NW = NT / 32;
     CT buf[2][P3];
-    CT red[2][NW];
+    double red[2][NW];
 };
 
 // Stages the brick (slot base) into both buffers; returns the last sweep's
 // sum and leaves the relaxed interior value of this thread's cell in *out.
 // CT is the correction's storage and arithmetic type (FP64, or FP32 in the
-// mixed form), the sums of squares included.
+// mixed form); the sums of squares are formed in FP64 either way.
 template <int NX, typename CT = double>
 __device__ __forceinline__ double relax_brick(RelaxSmem<NX, CT>& sm, const CT* __restrict__ dphi,
                                               const CT* __restrict__ dphi1, CT* out) {
@@ -41,20 +38,20 @@ __device__ __forceinline__ double relax_brick(RelaxSmem<NX, CT>& sm, const CT* _
     const int c = (k * P + j) * P + i;
     const CT d1 = dphi1[c];
     __syncthreads();
-    CT resid0 = 0, resid = 0;
+    double resid0 = 0.0, resid = 0.0;
     int iters = 0, cur = 0;
     do {
         const CT* d = sm.buf[cur];
         const CT div = (d[c + 1] + d[c - 1] + d[c + P] + d[c - P] + d[c + P * P] + d[c - P * P]) - (d[c] * CT(6.0));
         const CT tmp0 = d1 + div * (CT(1.0) / CT(6.0));
         sm.buf[cur ^ 1][c] = d[c] + tmp0;
-        CT sq = tmp0 * tmp0;
+        double sq = double(tmp0) * double(tmp0);
         for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
         if ((t & 31) == 0) sm.red[cur][t >> 5] = sq;
         __syncthreads();
         // pairwise sum of the warp partials (fixed tree, identical in every
         // thread): log2(NW) dependent additions instead of NW
-        CT r[NW];
+        double r[NW];
 #pragma unroll
         for (int w = 0; w < NW; w++) r[w] = sm.red[cur][w];
 #pragma unroll
@@ -65,9 +62,9 @@ __device__ __forceinline__ double relax_brick(RelaxSmem<NX, CT>& sm, const CT* _
         if (iters == 0) resid0 = resid;
         iters++;
         cur ^= 1;
-    } while (resid / resid0 > CT(0.5) && iters < 16);
+    } while (resid / resid0 > 0.5 && iters < 16);
     *out = sm.buf[cur][c];
-    return double(resid);
+    return resid;
 }
 
 // Barrier over `n` threads with id `id` (1..15; 0 is __syncthreads).
@@ -99,7 +96,7 @@ __device__ __forceinline__ double relax_brick_half(RelaxSmem<NX, CT>& sm, const 
         d1[h] = dphi1[c[h]];
     }
     named_sync(bar, HT);
-    CT resid0 = 0, resid = 0;
+    double resid0 = 0.0, resid = 0.0;
     int iters = 0, cur = 0;
     do {
         const CT* d = sm.buf[cur];
@@ -110,12 +107,12 @@ __device__ __forceinline__ double relax_brick_half(RelaxSmem<NX, CT>& sm, const 
                 (d[cc + 1] + d[cc - 1] + d[cc + P] + d[cc - P] + d[cc + P * P] + d[cc - P * P]) - (d[cc] * CT(6.0));
             const CT tmp0 = d1[h] + div * (CT(1.0) / CT(6.0));
             sm.buf[cur ^ 1][cc] = d[cc] + tmp0;
-            CT sq = tmp0 * tmp0;
+            double sq = double(tmp0) * double(tmp0);
             for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
             if ((lt & 31) == 0) sm.red[cur][h * (HT >> 5) + (lt >> 5)] = sq;
         }
         named_sync(bar, HT);
-        CT r[NW];
+        double r[NW];
 #pragma unroll
         for (int w = 0; w < NW; w++) r[w] = sm.red[cur][w];
 #pragma unroll
@@ -126,10 +123,10 @@ __device__ __forceinline__ double relax_brick_half(RelaxSmem<NX, CT>& sm, const 
         if (iters == 0) resid0 = resid;
         iters++;
         cur ^= 1;
-    } while (resid / resid0 > CT(0.5) && iters < 16);
+    } while (resid / resid0 > 0.5 && iters < 16);
     out[0] = sm.buf[cur][c[0]];
     out[1] = sm.buf[cur][c[1]];
-    return double(resid);
+    return resid;
 }
 
 }  // namespace amr

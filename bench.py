@@ -722,7 +722,9 @@ def run_case(case):
                   (k_substep_fused, FP64)
     eos_1M        2^20 points, forward and inverse Helmholtz EOS
     ztwd_L5       two BinaryDriver steps of the 5-level ZTWD binary, plain FP64
-                  (k_zt_flux, k_zt_add_difs, k_zt_max_dt, ... as separate launches)"""
+                  (k_zt_flux, k_zt_add_difs, k_zt_max_dt, ... as separate launches)
+    ztwd_mixed_L5 four steps of the same binary in the mixed persistent form,
+                  the last two inside the NVTX range timed_step"""
     import torch
     amr, ini = load_amr()
     if case == "solve_L3":
@@ -765,16 +767,24 @@ def run_case(case):
         h.close()
         import shutil
         shutil.rmtree(tdir, ignore_errors=True)
-    elif case == "ztwd_L5":
+    elif case in ("ztwd_L5", "ztwd_mixed_L5"):
         helm_table = _load_module("helm_table", os.path.join(PKG, "helm_table.py"))
         helm_mod = _load_module("helm_b200", os.path.join(PKG, "helm.py"))
         tdir = tempfile.mkdtemp(prefix="ztwd_")
-        a = ztwd_context(amr, ini, helm_mod, helm_table.ensure_table(tdir), ZT_LEVELS, amr.PREC_FP64, 0)
+        mixed = case == "ztwd_mixed_L5"
+        a = ztwd_context(amr, ini, helm_mod, helm_table.ensure_table(tdir), ZT_LEVELS,
+                         amr.PREC_MIXED if mixed else amr.PREC_FP64, 2 if mixed else 0)
         last = 0.0
-        for s in range(2):
+        nsteps = 4 if mixed else 2
+        for s in range(nsteps):
             dt = a.max_dt()
             dt = min(1.25 * last, dt) if s else dt
+            if mixed and s >= 2:
+                torch.cuda.nvtx.range_push("timed_step")
             last = a.ztwd_step(dt, ZT_TOL, DYNAMIC_RANGE, s)
+            if mixed and s >= 2:
+                a.synchronize()
+                torch.cuda.nvtx.range_pop()
         a.synchronize()
         print(json.dumps({"case": case, "bricks": a.nbricks, "dt": last}))
         a.close()
@@ -838,7 +848,8 @@ def main():
     ap.add_argument("--no-eos", action="store_true", help="skip the Helmholtz EOS throughput section")
     ap.add_argument("--no-batched", action="store_true", help="skip the random-field octree substep section")
     ap.add_argument("--no-ztwd", action="store_true", help="skip the ZTWD binary section")
-    ap.add_argument("--case", default=None, choices=["solve_L3", "substep_L4", "eos_1M", "ztwd_L5"],
+    ap.add_argument("--case", default=None,
+                    choices=["solve_L3", "substep_L4", "eos_1M", "ztwd_L5", "ztwd_mixed_L5"],
                     help="run one small case for a profiler capture and exit")
     args = ap.parse_args()
     if args.case:
