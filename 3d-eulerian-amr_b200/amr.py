@@ -128,6 +128,8 @@ def load_library(path=LIB_PATH):
         if hasattr(lib, "amr_solve_phases"):
             lib.amr_solve_phases.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong), dp, I]
             lib.amr_solve_last_ms.argtypes = [P, ctypes.POINTER(ctypes.c_float)]
+            if hasattr(lib, "amr_solve_totals"):
+                lib.amr_solve_totals.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong)]
             if hasattr(lib, "amr_solve_phase_waits"):
                 lib.amr_solve_phase_waits.argtypes = [P, dp, I, dp, ctypes.POINTER(ctypes.c_longlong)]
         _lib = lib
@@ -429,6 +431,13 @@ class AMR:
         out["level_sum"] = ls.value
         out["level_sum_count"] = cnt.value
         return out
+
+    def solve_totals(self):
+        """(device ms, count) of the persistent solve launches of graph_solve."""
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        self._check(self.lib.amr_solve_totals(self.ctx, ctypes.byref(ms), ctypes.byref(n)))
+        return ms.value, n.value
 
     def solve_last_ms(self):
         v = ctypes.c_float()

@@ -69,6 +69,8 @@ struct GraphState {
     double* d_pnest = nullptr;
     GridBarrier* d_bar = nullptr;
     cudaEvent_t ev_ps[2] = {nullptr, nullptr};  // around the last persistent launch
+    double ps_ms_total = 0.0;                   // persistent launches of amr_graph_solve: device time, count
+    long long ps_count = 0;
     long long rec_in_bodies = 0;  // kernels recorded inside outermost WHILE bodies
     long long rec_nested = 0;     // kernels recorded inside the bodies of the body being recorded
     int while_depth = 0;
@@ -537,6 +539,15 @@ int amr_solve_phase_waits(amr_ctx* c, double* wait_ms, int n, double* level_sum_
     return AMR_OK;
 }
 
+// Device time and number of the persistent solve launches made by
+// amr_graph_solve (CUDA events around each launch on its stream).
+int amr_solve_totals(amr_ctx* c, double* ms, long long* count) {
+    if (!c || !ms || !count) return AMR_ERR_ARG;
+    *ms = c->gs ? c->gs->ps_ms_total : 0.0;
+    *count = c->gs ? c->gs->ps_count : 0;
+    return AMR_OK;
+}
+
 // Duration of the most recent persistent solve launch (CUDA events recorded
 // around it on the launching stream).
 int amr_solve_last_ms(amr_ctx* c, float* ms) {
@@ -565,6 +576,12 @@ int amr_graph_solve(amr_ctx* c, double tol, int max_cycles, double* l1_error, in
     CUDA_TRY(cudaGraphLaunch(g->solve_exec, c->stream));
     TRY(read_ctl(c));
     count_replay(c, g->k_solve);
+    if (c->cfg.persistent_solve > 0) {
+        float ms = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&ms, g->ev_ps[0], g->ev_ps[1]));
+        g->ps_ms_total += ms;
+        g->ps_count++;
+    }
     if (l1_error) *l1_error = g->h_ctl->err;
     if (cycles) *cycles = g->h_ctl->cycles;
     if (g->h_ctl->status == 3) {

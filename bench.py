@@ -1,14 +1,23 @@
 #!/usr/bin/env python
 """Benchmark: cell-updates/s of the self-gravitating hydro step on one B200.
 
-Workload (the reference's single-star configuration): n=1.5 Lane-Emden
-polytrope, central density 1, radius 0.25, unit cube [-0.5,0.5]^3, ambient
-floor 1e-10, at rest; 4 refinement levels (8^3-cell bricks, BW=2,
-minmod-theta 1.3, CFL 0.4, gamma 5/3); regrid every 8 steps at
-rho_max/1e6; one RK3 step = 3 substeps, each hydro (KT fluxes, coarse-fine
-correction, RK combine, gravity sources) followed by a multigrid Poisson
-solve to an L1 error <= 1e-6 (the reference's single-star ELL_TOLER).
-A step's work is the leaf cells it advances (GridNode::get_zone_cnt).
+Headline workload (the configuration the target is quoted on): the 5-level
+ZTWD binary of the reference's BINARY build -- two zero-temperature white
+dwarfs (the reference's two-polytrope initial data, binary/initialize.cpp),
+mass ratio q = 0.7, separation 0.5, donor near its Roche lobe, co-rotating
+frame, Helmholtz EOS (synthetic table in the reference's format), PPM with
+BW 3 on 8^3-cell bricks, CFL 0.3; one step = BinaryDriver::step: three RK3
+substeps, each hydro followed by a multigrid Poisson solve to L1 error
+1e-7 (ELL_TOLER), regrid every 8 steps.  `value` is the mixed-precision
+persistent form (FP32 multigrid correction inside FP64 defect correction,
+each solve one persistent kernel); the plain FP64 form, the FP64 persistent
+form and the mixed form's errors after 100 steps are reported beside it,
+with the reference's own BINARY build timed on the host cores.  A step's
+work is the leaf cells it advances (GridNode::get_zone_cnt).
+
+Secondary sections: the single star (n=1.5 polytrope, 4 levels, Euler
+state, minmod, the graph and persistent forms), the batched uneven-brick
+substep on a random-field octree, the Helmholtz EOS at 2^24 points.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -34,10 +43,15 @@ PKG = os.path.join(ROOT, "3d-eulerian-amr_b200")
 
 LEVELS = 4
 TOL = 1.0e-6
+ZT_LEVELS = 5
+ZT_TOL = 1.0e-7  # ELL_TOLER of the BINARY build (binary/binary_defs.h:64)
+ZT_STEPS_TOTAL = 100
 DYNAMIC_RANGE = 1.0e6
 METRIC = "cell-updates/s (hydro+gravity step), 1 B200: mixed+batched vs FP64 at set error"
 UNIT = "cell-updates/s"
 WORKLOAD = "single star: n=1.5 polytrope, 4 levels, RK3 hydro + multigrid gravity (L1 tol 1e-6)"
+ZT_WORKLOAD = ("ZTWD binary: q=0.7, 5 levels, 8^3 bricks, PPM, Helmholtz EOS, BinaryDriver steps "
+               "(RK3 hydro + multigrid gravity every substep, L1 tol 1e-7, regrid every 8 steps)")
 
 # Bytes each kernel class must move per brick per launch (FP64, nx=8, BW=2,
 # NF=6, PNX=10); the denominator-free "algorithmic" traffic of one launch.
@@ -53,6 +67,14 @@ BYTES_PER_BRICK = {
     "ghost_fill": 8 * NF * 2 * 6 * BW * NX * NX,
     "dphi_boundaries": 8 * 2 * 6 * NX * NX,
 }
+
+# DRAM bytes (read + write) per launch of the persistent solve on the 5-level
+# ZTWD binary: the mean over the six solve launches of two BinaryDriver steps
+# of `bench.py --case ztwd_mixed_L5`, one ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum, caches flushed before each launch); those launches
+# carry 2.72 GB of algorithmic bytes each.  The solve's arrays stay in L2
+# across its V-cycles, so DRAM sees the cold fill and the dirty write-back.
+ZT_SOLVE_DRAM_BYTES_PER_LAUNCH = 17.97e6
 
 
 def load_amr():
@@ -147,7 +169,61 @@ def run_reference_steps(levels, threads, warm, steps, timeout=3000):
             "bricks": summ["bricks"], "threads": summ["threads"]}
 
 
+def run_reference_ztwd(threads, warm, steps, timeout=1500):
+    """The reference's BINARY build (oracle/_ref/ztwd_harness, g++ -O2 -fopenmp)
+    on the headline workload: `warm` untimed BinaryDriver steps (the first
+    solves from the initial potential), then `steps` timed ones."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ztwd_harness")
+    if not os.path.exists(exe):
+        return None
+    helm_table = _load_module("helm_table", os.path.join(PKG, "helm_table.py"))
+    tdir = tempfile.mkdtemp(prefix="ztwd_ref_")
+    helm_table.ensure_table(tdir)
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    try:
+        r = subprocess.run([exe, "time_ztwd", str(ZT_LEVELS), str(warm + steps)], cwd=tdir, env=env,
+                           capture_output=True, text=True, timeout=timeout)
+        row = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
+    except (subprocess.TimeoutExpired, IndexError, ValueError):
+        return None
+    finally:
+        import shutil
+        shutil.rmtree(tdir, ignore_errors=True)
+    return {"seconds": row["seconds"][warm:], "leaf_cells": row["leaf_cells"][warm:], "bricks": row["bricks"],
+            "threads": row["threads"]}
+
+
 def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    # a bounded sample: one untimed step (the initial solve) and at most two
+    # timed steps (~20 s each on 16 host threads)
+    s = run_reference_ztwd(threads, 1, min(args.steps, 2))
+    if s is None or not s["seconds"]:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref/ztwd_harness missing, failed or timed out"}))
+        return 0
+    t = sum(s["seconds"])
+    value = sum(s["leaf_cells"]) / t
+    sample = ("reference BINARY build (oracle/_ref/ztwd_harness, g++ -O2 -fopenmp, %d threads): %d BinaryDriver "
+              "steps of the 5-level binary after 1 untimed step, %d bricks" % (s["threads"], len(s["seconds"]),
+                                                                                s["bricks"]))
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": len(s["seconds"]), "warmup": 1, "ms_per_step": 1000.0 * t / len(s["seconds"]),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": ZT_WORKLOAD, "levels": ZT_LEVELS, "bricks": s["bricks"]},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": s["threads"], "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def reference_arm_single_star(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -582,11 +658,6 @@ def run_batched_substep(amr, ini, torch, steps, warmup, levels=5):
     return out
 
 
-ZT_LEVELS = 5
-ZT_TOL = 1.0e-7  # ELL_TOLER of the BINARY build (binary/binary_defs.h:64)
-ZT_STEPS_TOTAL = 100
-
-
 def ztwd_context(amr, ini, helm_mod, table, levels, prec, persistent):
     """A ZTWD binary context on the 5-level tree of the reference's two-polytrope
     initial data (binary/initialize.cpp), EOS units of Binary::set_units."""
@@ -702,13 +773,134 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL):
                 row = json.loads([x for x in r.stdout.splitlines() if x.startswith("{")][-1])
                 sec = row["seconds"][-1]
                 res["cpu_baseline"] = {
-                    "value": res["fp64"]["leaf_cells"] / sec, "unit": UNIT, "cores": row["threads"],
+                    "value": row["leaf_cells"][-1] / sec, "unit": UNIT, "cores": row["threads"],
                     "kind": "reference", "seconds_per_step": sec,
                     "sample": "reference BINARY build (oracle/_ref/ztwd_harness, g++ -O2 -fopenmp): its second "
                               "BinaryDriver step on the same 5-level binary (the first solves from the initial "
-                              "phi), leaf cells of our FP64 run per step"}
+                              "phi), %d leaf cells" % row["leaf_cells"][-1]}
             except (subprocess.TimeoutExpired, IndexError, ValueError, KeyError):
                 res["cpu_baseline"] = None
+    import shutil
+    shutil.rmtree(tdir, ignore_errors=True)
+    return res
+
+
+def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
+    """The headline: W untimed then K timed BinaryDriver steps of the 5-level
+    ZTWD binary in the mixed persistent form (L2 flushed between timed steps,
+    outside the timed interval); then, on a second context that replays the
+    same W warm-up steps, the same K steps end to end through the C ABI with
+    the state copied from and to pinned host memory every step."""
+    helm_table = _load_module("helm_table", os.path.join(PKG, "helm_table.py"))
+    helm_mod = _load_module("helm_b200", os.path.join(PKG, "helm.py"))
+    tdir = tempfile.mkdtemp(prefix="ztwd_head_")
+    table = helm_table.ensure_table(tdir)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def warmed():
+        """A fresh context of the workload after the W warm-up steps, and its
+        step function (dt from max_dt with the MAXDTINC clamp)."""
+        a = ztwd_context(amr, ini, helm_mod, table, ZT_LEVELS, amr.PREC_MIXED, 2)
+        state = {"step": 0, "last": 0.0}
+
+        def one_step():
+            s = state["step"]
+            dt = a.max_dt()
+            if s > 0:
+                dt = min(1.25 * state["last"], dt)
+            state["last"] = a.ztwd_step(dt, ZT_TOL, DYNAMIC_RANGE, s)
+            state["step"] = s + 1
+
+        for _ in range(args.warmup):
+            one_step()
+        return a, one_step
+
+    a, one_step = warmed()
+    stream = torch.cuda.ExternalStream(a.stream_handle())
+    ph0, w0, tot0 = a.solve_phases(), a.solve_phase_waits(), a.solve_totals()
+    k0 = a.launch_count()
+    sampler = ClockSampler(local)
+    barrier()
+    sampler.start()
+    times, cells = [], 0
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        n = a.get_zone_cnt()
+        torch.cuda.nvtx.range_push("timed_step")
+        ev0.record(stream)
+        one_step()
+        ev1.record(stream)
+        torch.cuda.nvtx.range_pop()
+        ev1.synchronize()
+        times.append(ev0.elapsed_time(ev1))
+        cells += n
+    barrier()
+    res = {"clocks": sampler.stop(), "gpu_launches": a.launch_count() - k0, "bricks": a.nbricks,
+           "ms_steps": [round(x, 3) for x in times]}
+    ph1, w1, tot1 = a.solve_phases(), a.solve_phase_waits(), a.solve_totals()
+    launches = max(tot1[1] - tot0[1], 1)
+    d = {k: {"ms": ph1[k]["ms"] - ph0[k]["ms"], "count": ph1[k]["count"] - ph0[k]["count"],
+             "bytes": ph1[k]["bytes"] - ph0[k]["bytes"]} for k in ph1}
+    res["persistent"] = {
+        "ms_per_launch": (tot1[0] - tot0[0]) / launches, "launches": launches,
+        "bytes_per_launch": sum(v["bytes"] for v in d.values()) / launches,
+        "phase_ms_per_step": {k: round(v["ms"] / args.steps, 4) for k, v in d.items()},
+        "phases_per_step": {k: v["count"] / args.steps for k, v in d.items()},
+        "barrier_ms_per_step": {k: round((w1[k] - w0[k]) / args.steps, 4) for k in ph1},
+        "level_sum_ms_per_step": round((w1["level_sum"] - w0["level_sum"]) / args.steps, 4)}
+    a.close()
+    t = torch.tensor([sum(times), float(cells)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
+    res["ms_total"], res["cells"] = float(t[0]), float(t[1])
+    res["value"] = res["cells"] / (res["ms_total"] / 1000.0)
+    res["ms_per_step"] = res["ms_total"] / args.steps
+    res["leaf_cells_per_step"] = cells / args.steps
+    # end to end through the public API, host buffers, the same K steps
+    a, one_step = warmed()
+    stream = torch.cuda.ExternalStream(a.stream_handle())
+    cap = 3 * a.nbricks * a.nf * a.gnx ** 3  # room for the tree to grow during the K steps
+    hbuf = torch.empty(cap, dtype=torch.float64, pin_memory=True)
+    U = a.download_state()
+    hbuf[:U.size].copy_(torch.from_numpy(U.reshape(-1)))
+    ptr = ctypes.cast(hbuf.data_ptr(), ctypes.POINTER(ctypes.c_double))
+    barrier()
+    e_times, e_cells, h2d, d2h = [], 0, 0, 0
+    for _ in range(args.steps):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        n_in = a.nbricks * a.nf * a.gnx ** 3
+        e_cells += a.get_zone_cnt()
+        ev0.record(stream)
+        a._check(a.lib.amr_upload_state(a.ctx, ptr))
+        one_step()
+        n_out = a.nbricks * a.nf * a.gnx ** 3
+        if n_out > cap:
+            raise RuntimeError("e2e host buffer too small for the regridded tree")
+        a._check(a.lib.amr_download_state(a.ctx, ptr))
+        ev1.record(stream)
+        ev1.synchronize()
+        e_times.append(ev0.elapsed_time(ev1))
+        h2d += 8 * n_in
+        d2h += 8 * n_out
+    barrier()
+    a.close()
+    et = torch.tensor([sum(e_times), float(e_cells)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(et[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(et[1:2], op=dist.ReduceOp.SUM)
+    res["e2e"] = {"value": float(et[1]) / (float(et[0]) / 1000.0), "unit": UNIT,
+                  "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
+                  "ms_per_step": float(et[0]) / args.steps, "ms_steps": [round(x, 3) for x in e_times]}
     import shutil
     shutil.rmtree(tdir, ignore_errors=True)
     return res
@@ -724,7 +916,10 @@ def run_case(case):
     ztwd_L5       two BinaryDriver steps of the 5-level ZTWD binary, plain FP64
                   (k_zt_flux, k_zt_add_difs, k_zt_max_dt, ... as separate launches)
     ztwd_mixed_L5 four steps of the same binary in the mixed persistent form,
-                  the last two inside the NVTX range timed_step"""
+                  the last two inside the NVTX range timed_step
+    single_fp64_L4, single_mixed_L4
+                  the 4-level single star, plain FP64 / mixed persistent form:
+                  3 warm-up steps, then 2 steps inside timed_step"""
     import torch
     amr, ini = load_amr()
     if case == "solve_L3":
@@ -767,6 +962,13 @@ def run_case(case):
         h.close()
         import shutil
         shutil.rmtree(tdir, ignore_errors=True)
+    elif case in ("single_fp64_L4", "single_mixed_L4"):
+        # the single star's timed steps (NVTX range timed_step), 3 warm-up
+        import types
+        form = "mixed" if case == "single_mixed_L4" else "fp64"
+        r = run_form(amr, ini, form, types.SimpleNamespace(steps=2, warmup=3), 1, 0, torch, None)
+        print(json.dumps({"case": case, "bricks": r["bricks"], "ms_per_step": r["ms_per_step"],
+                          "gpu_launches": r["gpu_launches"]}))
     elif case in ("ztwd_L5", "ztwd_mixed_L5"):
         helm_table = _load_module("helm_table", os.path.join(PKG, "helm_table.py"))
         helm_mod = _load_module("helm_b200", os.path.join(PKG, "helm.py"))
@@ -776,9 +978,12 @@ def run_case(case):
                          amr.PREC_MIXED if mixed else amr.PREC_FP64, 2 if mixed else 0)
         last = 0.0
         nsteps = 4 if mixed else 2
+        solve = {}
         for s in range(nsteps):
             dt = a.max_dt()
             dt = min(1.25 * last, dt) if s else dt
+            if mixed and s == 2:
+                tot0, ph0 = a.solve_totals(), a.solve_phases()
             if mixed and s >= 2:
                 torch.cuda.nvtx.range_push("timed_step")
             last = a.ztwd_step(dt, ZT_TOL, DYNAMIC_RANGE, s)
@@ -786,7 +991,15 @@ def run_case(case):
                 a.synchronize()
                 torch.cuda.nvtx.range_pop()
         a.synchronize()
-        print(json.dumps({"case": case, "bricks": a.nbricks, "dt": last}))
+        if mixed:
+            # the persistent solve launches inside the timed_step ranges:
+            # algorithmic bytes per launch, to set beside a profiler's DRAM bytes
+            tot1, ph1 = a.solve_totals(), a.solve_phases()
+            n = max(tot1[1] - tot0[1], 1)
+            solve = {"solve_launches": tot1[1] - tot0[1], "solve_ms_per_launch": (tot1[0] - tot0[0]) / n,
+                     "solve_algorithmic_bytes_per_launch":
+                         sum(ph1[k]["bytes"] - ph0[k]["bytes"] for k in ph1) / n}
+        print(json.dumps({"case": case, "bricks": a.nbricks, "dt": last, **solve}))
         a.close()
         import shutil
         shutil.rmtree(tdir, ignore_errors=True)
@@ -795,22 +1008,24 @@ def run_case(case):
     return 0
 
 
-def roofline_persistent(res):
+def roofline_persistent(res, traffic=None):
     """Roofline of the persistent solve kernel, the step's dominant kernel:
     algorithmic bytes per launch (the arrays each phase must read and write
     once, summed by the kernel over its phases) over the launch's duration
-    from CUDA events on the launching stream."""
+    from CUDA events on the launching stream; `traffic` the measured DRAM
+    bytes per launch where a capture of this workload exists."""
     p = res["persistent"]
     peak, peak_kind = peaks()
     achieved = p["bytes_per_launch"] / (p["ms_per_launch"] * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": "k_solve_persistent", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
             "algorithmic_bytes_per_launch": p["bytes_per_launch"], "ms_per_launch": p["ms_per_launch"],
             "phase_ms_per_step": p["phase_ms_per_step"], "phases_per_step": p["phases_per_step"],
             "barrier_ms_per_step": p.get("barrier_ms_per_step"),
             "level_sum_ms_per_step": p.get("level_sum_ms_per_step"),
             "note": "latency-bound: the reference's V-cycle is a chain of dependent per-level steps "
-                    "(about 700 grid barriers per step here); the relaxation sweeps run in shared memory"}
+                    "(%d grid barriers per step here); the relaxation sweeps run in shared memory"
+                    % round(sum(p["phases_per_step"].values()))}
 
 
 def roofline_of(prof):
@@ -822,17 +1037,42 @@ def roofline_of(prof):
     bytes_per_launch = BYTES_PER_BRICK[name] * pr["units"] / pr["launches"]
     ms_per_launch = pr["ms"] / pr["launches"]
     achieved = bytes_per_launch / (ms_per_launch * 1e-3) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
-        with open(tpath) as f:
-            traffic = json.load(f).get(name)
     total = sum(x["ms"] for x in prof.values())
     return {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
             "algorithmic_bytes_per_launch": bytes_per_launch, "ms_per_launch": ms_per_launch,
             "dominant_class": dom,
             "class_share": {k: round(v["ms"] / max(total, 1e-9), 4) for k, v in prof.items() if v["ms"] > 0}}
+
+
+def run_single_star(amr, ini, args, world, local, torch, dist):
+    """The single star (4 levels, Euler state): mixed persistent form with its
+    e2e and kernel-class profile, the plain / graph / persistent FP64 forms,
+    the mixed form's errors, a tight Poisson solve, the reference CPU code."""
+    head = run_form(amr, ini, "mixed", args, 1, local, torch, dist, e2e=True, profile=True)
+    plain = run_form(amr, ini, "fp64", args, 1, local, torch, dist)
+    graph64 = run_form(amr, ini, "graph", args, 1, local, torch, dist)
+    pers64 = run_form(amr, ini, "persistent", args, 1, local, torch, dist)
+    errors = state_errors(head["final"], plain["final"], 2)
+    errors["steps"] = args.warmup + args.steps
+    errors["against"] = "plain FP64 form (parity-tested against the reference CPU code)"
+    cpu = None
+    if not args.no_cpu_baseline:
+        s = run_reference_steps(LEVELS, os.cpu_count() or 1, 1, 1, timeout=1200)
+        if s is not None and s["seconds"]:
+            cpu = {"value": sum(s["leaf_cells"]) / sum(s["seconds"]), "unit": UNIT, "cores": s["threads"],
+                   "kind": "reference",
+                   "sample": "reference CPU code (oracle/_ref): one full RK3 step of this workload after one "
+                             "untimed step (which solves from phi = 0), %d bricks, %d V-cycles" %
+                             (s["bricks"], s["vcycles"][0])}
+    form = lambda r: {"value": r["value"], "ms_per_step": r["ms_per_step"], "gpu_launches": r["gpu_launches"]}
+    return {"workload": WORKLOAD, "levels": LEVELS, "bricks": head["bricks"],
+            "mixed_persistent": dict(form(head), e2e=head["e2e"], clocks=head["clocks"],
+                                     relax_calls_per_step=head["relax_calls_per_step"]),
+            "roofline": roofline_persistent(head), "class_roofline": roofline_of(head["profile"]),
+            "fp64_plain": form(plain), "fp64_graph": form(graph64), "fp64_persistent": form(pers64),
+            "speedup_vs_fp64_plain": plain["ms_per_step"] / head["ms_per_step"],
+            "errors_vs_fp64": errors, "poisson_precision": poisson_precision_check(amr, ini), "cpu_baseline": cpu}
 
 
 def main():
@@ -841,15 +1081,16 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--form", default="mixed", choices=["fp64", "graph", "persistent", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-compare", action="store_true", help="skip the plain FP64 comparison run")
+    ap.add_argument("--no-compare", action="store_true",
+                    help="skip the FP64 forms and the 100-step error comparison of the binary")
     ap.add_argument("--json-out", default=None)
     ap.add_argument("--no-eos", action="store_true", help="skip the Helmholtz EOS throughput section")
     ap.add_argument("--no-batched", action="store_true", help="skip the random-field octree substep section")
-    ap.add_argument("--no-ztwd", action="store_true", help="skip the ZTWD binary section")
+    ap.add_argument("--no-single", action="store_true", help="skip the single-star section")
     ap.add_argument("--case", default=None,
-                    choices=["solve_L3", "substep_L4", "eos_1M", "ztwd_L5", "ztwd_mixed_L5"],
+                    choices=["solve_L3", "substep_L4", "eos_1M", "ztwd_L5", "ztwd_mixed_L5", "single_fp64_L4",
+                             "single_mixed_L4"],
                     help="run one small case for a profiler capture and exit")
     args = ap.parse_args()
     if args.case:
@@ -869,66 +1110,44 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
     amr, ini = load_amr()
-    head = run_form(amr, ini, args.form, args, world, local, torch, dist, e2e=True, profile=True)
-    plain = graph64 = pers64 = None
-    errors = None
-    pcheck = None
-    if not args.no_compare and args.form != "fp64":
-        plain = run_form(amr, ini, "fp64", args, world, local, torch, dist)
-        if args.form == "mixed":
-            graph64 = run_form(amr, ini, "graph", args, world, local, torch, dist)
-            pers64 = run_form(amr, ini, "persistent", args, world, local, torch, dist)
-            errors = state_errors(head["final"], plain["final"], 2)
-            errors["steps"] = args.warmup + args.steps
-            errors["against"] = "plain FP64 form (parity-tested against the reference CPU code)"
-            if rank == 0:
-                pcheck = poisson_precision_check(amr, ini)
-    cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        s = run_reference_steps(LEVELS, threads, 1, 1, timeout=1200)
-        if s is not None and s["seconds"]:
-            cpu = {"value": sum(s["leaf_cells"]) / sum(s["seconds"]), "unit": UNIT, "cores": s["threads"],
-                   "kind": "reference",
-                   "sample": "reference CPU code (oracle/_ref): one full RK3 step of this workload after one "
-                             "untimed step (which solves from phi = 0), %d bricks, %d V-cycles" %
-                             (s["bricks"], s["vcycles"][0])}
+    head = run_ztwd_headline(amr, ini, args, world, local, torch, dist)
+    ztwd = None
+    if rank == 0 and not args.no_compare:
+        ztwd = run_ztwd(amr, ini, torch, args.steps, max(args.warmup, 3), not args.no_cpu_baseline)
+    single = None
+    if rank == 0 and not args.no_single:
+        single = run_single_star(amr, ini, args, world, local, torch, dist)
     batched = None
     if rank == 0 and not args.no_batched:
         batched = run_batched_substep(amr, ini, torch, max(args.steps, 3), max(args.warmup, 3))
-    ztwd = None
-    if rank == 0 and not args.no_ztwd:
-        ztwd = run_ztwd(amr, ini, torch, max(args.steps, 3), max(args.warmup, 3), not args.no_cpu_baseline)
     eos = None
     if rank == 0 and not args.no_eos:
         eos = run_eos(torch, max(args.steps, 3), max(args.warmup, 3), not args.no_cpu_baseline)
     if rank == 0:
+        cpu = ztwd.get("cpu_baseline") if ztwd else None
         out = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.form != "mixed" else "f64+f32",
+            "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "ms_steps": head["ms_steps"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64+f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "form": args.form, "levels": LEVELS, "bricks": head["bricks"],
-                       "leaf_cells_per_step": head["cells"] / args.steps / world, "tol_l1": TOL,
+            "config": {"workload": ZT_WORKLOAD, "form": "mixed persistent", "levels": ZT_LEVELS,
+                       "bricks": head["bricks"], "leaf_cells_per_step": head["leaf_cells_per_step"],
+                       "tol_l1": ZT_TOL, "binary": dict(ini.BINARY),
                        "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"},
-            "roofline": roofline_persistent(head) if "persistent" in head else roofline_of(head["profile"]),
-            "class_roofline": roofline_of(head["profile"]), "cpu_baseline": cpu, "e2e": head.get("e2e"),
+            "roofline": dict(roofline_persistent(head, ZT_SOLVE_DRAM_BYTES_PER_LAUNCH),
+                             traffic_note="ncu DRAM read+write per solve launch on this workload (L2-resident "
+                                          "arrays: far below the algorithmic bytes)"),
+            "cpu_baseline": cpu, "e2e": head["e2e"],
             "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
-            "relax_calls_per_step": head["relax_calls_per_step"],
-            "fp64_plain": None if plain is None else {"value": plain["value"], "ms_per_step": plain["ms_per_step"],
-                                                       "gpu_launches": plain["gpu_launches"]},
-            "fp64_graph": None if graph64 is None else {"value": graph64["value"],
-                                                         "ms_per_step": graph64["ms_per_step"],
-                                                         "gpu_launches": graph64["gpu_launches"]},
-            "fp64_persistent": None if pers64 is None else {"value": pers64["value"],
-                                                             "ms_per_step": pers64["ms_per_step"],
-                                                             "gpu_launches": pers64["gpu_launches"]},
-            "errors_vs_fp64": errors,
-            "poisson_precision": pcheck,
+            "fp64_plain": None if ztwd is None else {k: ztwd["fp64"][k] for k in ("value", "ms_per_step")},
+            "fp64_persistent": None if ztwd is None else {k: ztwd["fp64_persistent"][k]
+                                                          for k in ("value", "ms_per_step")},
+            "speedup_vs_fp64_plain": None if ztwd is None else ztwd["fp64"]["ms_per_step"] / head["ms_per_step"],
+            "errors_vs_fp64": None if ztwd is None else ztwd["errors_mixed_vs_fp64"],
+            "ztwd_binary": ztwd,
+            "single_star": single,
             "helmholtz_eos": eos,
             "batched_substep": batched,
-            "ztwd_binary": ztwd,
         }
         line = json.dumps(out)
         print(line)

@@ -290,6 +290,9 @@ int amr_solve_phases(amr_ctx* ctx, double* ms, long long* counts, double* bytes,
 /* Duration (CUDA events on the launching stream) of the most recent
  * persistent solve kernel. */
 int amr_solve_last_ms(amr_ctx* ctx, float* ms);
+/* Total device time (CUDA events around each launch) and number of the
+ * persistent solve launches made by amr_graph_solve so far. */
+int amr_solve_totals(amr_ctx* ctx, double* ms, long long* count);
 /* Of those phase times, the part spent at each phase's closing grid barrier
  * (block 0, from its arrival to the barrier's exit: the slowest block's extra
  * work plus the barrier itself), and the time spent forming the relaxation

@@ -143,9 +143,11 @@ int main(int argc, char* argv[]) {
     BinaryDriver driver(root);
     double last = 0.0;
     std::vector<double> dts, secs;
+    std::vector<long> zones;
     for (int s = 0; s < nsteps; s++) {
         double dt = root->max_dt();
         if (s > 0) dt = min(last * MAXDTINC, dt);
+        zones.push_back((long)root->get_zone_cnt());  // leaf cells the step advances
         const double t0 = omp_get_wtime();
         dt = driver.step(dt);
         secs.push_back(omp_get_wtime() - t0);
@@ -155,6 +157,8 @@ int main(int argc, char* argv[]) {
     if (timing) {
         printf("{\"steps\": %d, \"bricks\": %d, \"seconds\": [", nsteps, root->get_node_cnt());
         for (size_t i = 0; i < secs.size(); i++) printf("%s%.6f", i ? ", " : "", secs[i]);
+        printf("], \"leaf_cells\": [");
+        for (size_t i = 0; i < zones.size(); i++) printf("%s%ld", i ? ", " : "", zones[i]);
         printf("], \"threads\": %d}\n", omp_get_max_threads());
         return 0;
     }
