@@ -132,6 +132,8 @@ def load_library(path=LIB_PATH):
                 lib.amr_solve_totals.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong)]
             if hasattr(lib, "amr_solve_phase_waits"):
                 lib.amr_solve_phase_waits.argtypes = [P, dp, I, dp, ctypes.POINTER(ctypes.c_longlong)]
+            if hasattr(lib, "amr_relax_passes"):
+                lib.amr_relax_passes.argtypes = [P, ctypes.POINTER(ctypes.c_longlong), I]
         _lib = lib
     return _lib
 
@@ -438,6 +440,12 @@ class AMR:
         n = ctypes.c_longlong()
         self._check(self.lib.amr_solve_totals(self.ctx, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+    def relax_passes(self, n=16):
+        """Relaxation passes per level since the context started (every form)."""
+        out = (ctypes.c_longlong * n)()
+        self._check(self.lib.amr_relax_passes(self.ctx, out, n))
+        return np.array(out[:], dtype=np.int64)
 
     def solve_last_ms(self):
         v = ctypes.c_float()

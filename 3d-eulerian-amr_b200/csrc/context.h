@@ -85,6 +85,7 @@ struct amr_ctx {
     std::vector<int> off_vrange;
     int vcycle_max_outer = 1000;
     long long relax_calls = 0, relax_sweeps_total = 0;
+    long long relax_level[16] = {};  // relaxation passes per level
     bool topo_dirty = true;
     long long topo_version = 0;  // bumped by every rebuild_topology
     // ZTWD state: frame + EOS passed to its kernels, EOS-failure word

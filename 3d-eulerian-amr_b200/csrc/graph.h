@@ -55,6 +55,7 @@ struct Control {
     unsigned long long phase_wait_ns[16];
     unsigned long long level_sum_ns;
     unsigned long long level_sum_n;
+    long long relax_level[MAX_LEVELS];  // relaxation passes per level
 };
 
 // phase classes of the persistent solve

@@ -76,6 +76,7 @@ struct GraphState {
     int while_depth = 0;
     int nlevels_captured = 0;
     long long last_cycles = 0, last_relax = 0;  // device counters at the last read
+    long long last_relax_level[MAX_LEVELS] = {};
 };
 
 namespace {
@@ -457,6 +458,10 @@ void count_replay(amr_ctx* c, long long top_kernels) {
     const long long loops = dr - dc * 2LL * g->nlevels_captured;
     c->prof.kernels += top_kernels + dc * g->k_vbody + loops * g->k_rbody;
     c->relax_calls += dr;
+    for (int l = 0; l < MAX_LEVELS; l++) {
+        c->relax_level[l] += g->h_ctl->relax_level[l] - g->last_relax_level[l];
+        g->last_relax_level[l] = g->h_ctl->relax_level[l];
+    }
     g->last_cycles = g->h_ctl->cycles_total;
     g->last_relax = g->h_ctl->relax_calls;
 }
@@ -545,6 +550,15 @@ int amr_solve_totals(amr_ctx* c, double* ms, long long* count) {
     if (!c || !ms || !count) return AMR_ERR_ARG;
     *ms = c->gs ? c->gs->ps_ms_total : 0.0;
     *count = c->gs ? c->gs->ps_count : 0;
+    return AMR_OK;
+}
+
+// Relaxation passes per level since the context started (every form:
+// host-driven, captured graph, persistent solve).
+static_assert(MAX_LEVELS == 16, "amr_ctx::relax_level holds 16 levels");
+int amr_relax_passes(amr_ctx* c, long long* per_level, int n) {
+    if (!c || !per_level || n < 0) return AMR_ERR_ARG;
+    for (int l = 0; l < n; l++) per_level[l] = l < MAX_LEVELS ? c->relax_level[l] : 0;
     return AMR_OK;
 }
 

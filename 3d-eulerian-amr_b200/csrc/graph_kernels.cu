@@ -44,6 +44,7 @@ __global__ void __launch_bounds__(NX* NX* NX)
     if (t == 0) {
         *counter = 0u;
         ctl->relax_calls++;
+        ctl->relax_level[level]++;
         ctl->snap_par[level] = mode == 0 ? 0 : par ^ 1;  // the buffer just written
         if (mode == 0) {
             ctl->r0[level] = r;

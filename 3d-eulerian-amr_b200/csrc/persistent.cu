@@ -87,6 +87,7 @@ struct Solver {
     unsigned* ph_n;
     double* ph_bytes;
     unsigned long long* ph_wait;  // [PH_COUNT], then level-sum time and count
+    unsigned* lvl_n;              // relaxation passes per level
 
     __device__ static unsigned long long now() {
         unsigned long long t;
@@ -221,6 +222,7 @@ struct Solver {
         const double r0 = level_sum(l, pres);
         relax_par ^= 1;
         relax_calls++;
+        if (blockIdx.x == 0 && threadIdx.x == 0) lvl_n[l]++;
         int outer = 0;
         for (;;) {
             pres = a.pres + (size_t)relax_par * a.L.cap;
@@ -232,6 +234,7 @@ struct Solver {
             const double r = level_sum(l, pres);
             relax_par ^= 1;
             relax_calls++;
+            if (blockIdx.x == 0 && threadIdx.x == 0) lvl_n[l]++;
             ++outer;
             bool again = r / r0 > ratio;
             if (again && outer > max_outer) {
@@ -336,6 +339,9 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
     __shared__ unsigned s_ph_n[PH_COUNT];
     __shared__ double s_ph_bytes[PH_COUNT];
     __shared__ unsigned long long s_ph_wait[PH_COUNT + 2];
+    __shared__ unsigned s_lvl_n[MAX_LEVELS];
+    s.lvl_n = s_lvl_n;
+    if (threadIdx.x < MAX_LEVELS) s_lvl_n[threadIdx.x] = 0;
     s.ph_ns = s_ph_ns;
     s.ph_n = s_ph_n;
     s.ph_bytes = s_ph_bytes;
@@ -383,6 +389,7 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
             }
             c->level_sum_ns += s.ph_wait[PH_COUNT];
             c->level_sum_n += s.ph_wait[PH_COUNT + 1];
+            for (int l = 0; l < MAX_LEVELS; l++) c->relax_level[l] += s.lvl_n[l];
         }
     }
 }

@@ -128,6 +128,7 @@ int relax(amr_ctx* c, int l, double* resid) {
     TRY(fetch_per_slot(c, per));
     *resid = nested_level_sum(c->tree.root(), l, per);
     c->relax_calls++;
+    if (l < 16) c->relax_level[l]++;
     return AMR_OK;
 }
 

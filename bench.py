@@ -823,6 +823,7 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
     a, one_step = warmed()
     stream = torch.cuda.ExternalStream(a.stream_handle())
     ph0, w0, tot0 = a.solve_phases(), a.solve_phase_waits(), a.solve_totals()
+    rp0 = a.relax_passes()
     k0 = a.launch_count()
     sampler = ClockSampler(local)
     barrier()
@@ -856,6 +857,11 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
         "phases_per_step": {k: v["count"] / args.steps for k, v in d.items()},
         "barrier_ms_per_step": {k: round((w1[k] - w0[k]) / args.steps, 4) for k in ph1},
         "level_sum_ms_per_step": round((w1["level_sum"] - w0["level_sum"]) / args.steps, 4)}
+    lv = a.get_tree()["level"]
+    nl = int(lv.max()) + 1
+    res["persistent"]["bricks_by_level"] = [int((lv == l).sum()) for l in range(nl)]
+    res["persistent"]["relax_passes_per_step_by_level"] = [
+        round(float(x) / args.steps, 1) for x in (a.relax_passes() - rp0)[:nl]]
     a.close()
     t = torch.tensor([sum(times), float(cells)], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -1023,6 +1029,8 @@ def roofline_persistent(res, traffic=None):
             "phase_ms_per_step": p["phase_ms_per_step"], "phases_per_step": p["phases_per_step"],
             "barrier_ms_per_step": p.get("barrier_ms_per_step"),
             "level_sum_ms_per_step": p.get("level_sum_ms_per_step"),
+            "bricks_by_level": p.get("bricks_by_level"),
+            "relax_passes_per_step_by_level": p.get("relax_passes_per_step_by_level"),
             "note": "latency-bound: the reference's V-cycle is a chain of dependent per-level steps "
                     "(%d grid barriers per step here); the relaxation sweeps run in shared memory"
                     % round(sum(p["phases_per_step"].values()))}

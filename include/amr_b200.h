@@ -293,6 +293,10 @@ int amr_solve_last_ms(amr_ctx* ctx, float* ms);
 /* Total device time (CUDA events around each launch) and number of the
  * persistent solve launches made by amr_graph_solve so far. */
 int amr_solve_totals(amr_ctx* ctx, double* ms, long long* count);
+/* Relaxation passes (one vcycle_relax call over a level, poisson.cpp:88-130)
+ * per level since the context started, in every form of the solve;
+ * per_level[0 .. n-1]. */
+int amr_relax_passes(amr_ctx* ctx, long long* per_level, int n);
 /* Of those phase times, the part spent at each phase's closing grid barrier
  * (block 0, from its arrival to the barrier's exit: the slowest block's extra
  * work plus the barrier itself), and the time spent forming the relaxation
