@@ -144,6 +144,93 @@ __device__ __forceinline__ void op_relax_pass(const Geom& g, const BrickTable& b
     if (t == 0) pres[b] = resid;
 }
 
+// op_relax_pass in mode 1 split in two, so that a pass can be computed
+// before the loop has decided whether it runs.  op_relax_spec computes it
+// from the current dphi and the snapshot snap_rd with nothing written to
+// global memory (the ghost faces go to the staged brick only, where the
+// sweeps leave them); op_relax_commit then writes what op_relax_pass
+// writes: the ghost faces and the relaxed interior to dphi, the first
+// interior layers to snap_wr, the sum to pres[b].  Same values as
+// op_relax_pass; called by every thread, with the brick's shared memory
+// untouched in between.
+template <typename CT>
+struct RelaxSpec {
+    CT v;          // this thread's relaxed interior cell
+    double resid;  // the brick's last sweep sum
+};
+
+// ghost-face cell t (< 6 NX^2) of the (NX+2)^3 brick, and its face coordinates
+template <int NX>
+__device__ __forceinline__ int relax_ghost_cell(int t, int& face, int& t1, int& t2) {
+    constexpr int P = NX + 2, F = NX * NX;
+    face = t / F;
+    const int qq = t % F;
+    t1 = qq % NX + 1;
+    t2 = qq / NX + 1;
+    const int ax = face >> 1;
+    int d[3];
+    d[ax] = (face & 1) ? P - 1 : 0;
+    d[ax == 0 ? 1 : 0] = t1;
+    d[ax == 2 ? 1 : 2] = t2;
+    return (d[2] * P + d[1]) * P + d[0];
+}
+
+template <int NX, typename CT>
+__device__ __forceinline__ RelaxSpec<CT> op_relax_spec(const Geom& g, const BrickTable& bt, const DevState& st,
+                                                       int b, const CT* snap_rd, size_t stride,
+                                                       RelaxSmem<NX, CT>& sm) {
+    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX, NT = NX * NX * NX;
+    const CT* D = Corr<CT>::dphi(st) + (size_t)b * P3;
+    const int t = threadIdx.x;
+    CT gv = CT(0);
+    int gi = -1;
+    if (t < 6 * F) {
+        int face, t1, t2;
+        gi = relax_ghost_cell<NX>(t, face, t1, t2);
+        gv = ghost_dphi<NX, CT>(g, bt, st, snap_rd, stride, b, face, t1, t2);
+    }
+    for (int q = t; q < P3; q += NT) {
+        const CT v = D[q];
+        sm.buf[0][q] = v;
+        sm.buf[1][q] = v;
+    }
+    const int c = relax_cell<NX>(t);
+    const CT d1 = (Corr<CT>::dphi1(st) + (size_t)b * P3)[c];
+    __syncthreads();
+    if (gi >= 0) {
+        sm.buf[0][gi] = gv;
+        sm.buf[1][gi] = gv;
+    }
+    __syncthreads();
+    RelaxSpec<CT> r;
+    r.resid = relax_sweeps<NX, CT>(sm, c, d1, &r.v);
+    return r;
+}
+
+template <int NX, typename CT>
+__device__ __forceinline__ void op_relax_commit(const DevState& st, int b, const RelaxSpec<CT>& r,
+                                                const RelaxSmem<NX, CT>& sm, CT* snap_wr, size_t stride,
+                                                double* pres) {
+    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX;
+    CT* D = Corr<CT>::dphi(st) + (size_t)b * P3;
+    const int t = threadIdx.x;
+    const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
+    if (t < 6 * F) {
+        int face, t1, t2;
+        const int gi = relax_ghost_cell<NX>(t, face, t1, t2);
+        D[gi] = sm.buf[0][gi];
+    }
+    D[relax_cell<NX>(t)] = r.v;
+    CT* sw = snap_wr + (size_t)b * stride;
+    if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = r.v;
+    if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = r.v;
+    if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = r.v;
+    if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = r.v;
+    if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = r.v;
+    if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = r.v;
+    if (t == 0) pres[b] = r.resid;
+}
+
 // op_relax_pass for half a block (NX^3/2 threads, local index lt, barrier
 // `bar`): the same pass with two cells per thread (relax_brick_half), so
 // that one block relaxes two bricks at once.

@@ -69,6 +69,46 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned& target) {
     return ok != 0;
 }
 
+// Level-sum mailbox.  The publishing block's thread 0 stores sum g, then
+// releases lsum_gen = g; readers acquire lsum_gen until it reaches g (the
+// generations of a launch are 1, 2, ...; a reader waiting for g never sees
+// g + 1, which is published only after a grid barrier the reader has not
+// reached yet).  lsum_wait is called by every thread of a block and returns
+// the sum in all of them; false when the solve aborted.
+__device__ __forceinline__ void lsum_publish(GridBarrier* bar, unsigned g, double r) {
+    __stcg(&bar->lsum_val[g & 1], r);
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&bar->lsum_gen), "r"(g) : "memory");
+}
+
+__device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& r) {
+    __shared__ double s_r;
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        int good = 1;
+        unsigned long long spins = 0;
+        for (;;) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(&bar->lsum_gen) : "memory");
+            if ((int)(v - g) >= 0) break;
+            if ((spins & 63) == 63 && ld_volatile(&bar->abort)) {
+                good = 0;
+                break;
+            }
+            if (++spins > BARRIER_SPINS) {
+                atomicExch(&bar->abort, 1);
+                good = 0;
+                break;
+            }
+            if (spins > 32) __nanosleep(20);
+        }
+        s_r = good ? __ldcg(&bar->lsum_val[g & 1]) : 0.0;
+        s_ok = good;
+    }
+    __syncthreads();
+    r = s_r;
+    return s_ok != 0;
+}
+
 template <typename CT>
 struct Solver {
     const SolveArgs& a;
@@ -81,6 +121,7 @@ struct Solver {
     long long relax_calls;
     int max_outer;
     unsigned bar_target = 0;    // thread 0: arrivals that complete the next barrier
+    unsigned lsum_gen = 0;      // level sums published so far in this launch
     unsigned long long t_last;  // block 0: global time at the last barrier exit
     // block 0's phase accounting, in shared memory
     unsigned long long* ph_ns;
@@ -203,6 +244,23 @@ struct Solver {
         return r;
     }
 
+    __device__ void count_pass(int l) {
+        relax_calls++;
+        if (blockIdx.x == 0 && threadIdx.x == 0) lvl_n[l]++;
+    }
+
+    // the level sum published as generation lsum_gen (block 0 records the
+    // time it waits for it)
+    __device__ bool wait_sum(double& r) {
+        const unsigned long long t0 = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
+        const bool ok = lsum_wait(a.bar, lsum_gen, r);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            ph_wait[PH_COUNT] += now() - t0;
+            ph_wait[PH_COUNT + 1]++;
+        }
+        return ok;
+    }
+
     // relax_until (poisson.cpp:66-70, 74-78): ghosts, one pass, then passes
     // with ghosts from the previous pass's snapshot until the level sum has
     // fallen to `ratio` of the first
@@ -215,6 +273,7 @@ struct Solver {
             if (t < 384) op_dphi_faces<CT>(a.g, a.bt, a.st, a.aux, sl[q], t / 64, t % 64, 64);
         });
         if (!sync(PH_DPHI_FACES, n)) return false;
+        if (n < (int)gridDim.x) return relax_loop_overlapped(l, ratio, sl, n, snap);
         int par = 0;
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
         relax_pass(sl, n, 0, snap, snap, pres);
@@ -246,6 +305,69 @@ struct Solver {
         return true;
     }
 
+    // The relaxation loop of a level with fewer bricks than blocks (one
+    // brick per block, the last block without one), with the level sums off
+    // the critical path: after each pass's barrier the last block forms the
+    // pass's nested sum and publishes it, while every brick computes the
+    // next pass without writing anything (op_relax_spec).  The pass is
+    // written (op_relax_commit) once the sum says the loop goes on, and
+    // dropped when it ends.  Passes written, their values, the sums and the
+    // loop decisions are those of the loop in relax_until.
+    __device__ bool relax_loop_overlapped(int l, double ratio, const int* sl, int n, CT* snap) {
+        const bool mine = (int)blockIdx.x < n;
+        const bool server = blockIdx.x == gridDim.x - 1;
+        const int b = mine ? sl[blockIdx.x] : -1;
+        double* pres = a.pres + (size_t)relax_par * a.L.cap;
+        if (mine) op_relax_pass<8, CT>(a.g, a.bt, a.st, b, 0, snap, snap, a.stride, pres, sm[0]);
+        if (!sync(PH_RELAX_FIRST, n)) return false;
+        count_pass(l);
+        // pass 1 runs whatever the first sum; that sum is formed meanwhile
+        double r0;
+        {
+            const double* done = pres;
+            relax_par ^= 1;
+            pres = a.pres + (size_t)relax_par * a.L.cap;
+            ++lsum_gen;
+            if (server) {
+                const double r = level_sum(l, done);
+                if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
+            }
+            if (mine) op_relax_pass<8, CT>(a.g, a.bt, a.st, b, 1, snap, snap + a.snap_half, a.stride, pres, sm[0]);
+            if (!wait_sum(r0)) return false;
+            if (!sync(PH_RELAX, n)) return false;
+            count_pass(l);
+        }
+        int par = 1;  // snapshot buffer written by the last pass
+        int outer = 1;
+        for (;;) {
+            const double* done = pres;
+            relax_par ^= 1;
+            pres = a.pres + (size_t)relax_par * a.L.cap;
+            ++lsum_gen;
+            if (server) {
+                const double r = level_sum(l, done);
+                if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
+            }
+            RelaxSpec<CT> sp;
+            if (mine) sp = op_relax_spec<8, CT>(a.g, a.bt, a.st, b, snap + (size_t)par * a.snap_half, a.stride, sm[0]);
+            double r;
+            if (!wait_sum(r)) return false;
+            bool again = r / r0 > ratio;
+            if (again && outer > max_outer) {
+                again = false;
+                status = 1;
+            }
+            if (!again) break;
+            if (mine)
+                op_relax_commit<8, CT>(a.st, b, sp, sm[0], snap + (size_t)(par ^ 1) * a.snap_half, a.stride, pres);
+            if (!sync(PH_RELAX, n)) return false;
+            par ^= 1;
+            count_pass(l);
+            ++outer;
+        }
+        return true;
+    }
+
     // Poisson::vcycle (poisson.cpp:1069-1074) = vcycle0 (poisson.cpp:53-84)
     // without the two dphi ghost fills that nothing reads (see vcycle0 in
     // poisson_host.cpp)
@@ -263,25 +385,28 @@ struct Solver {
             if (!phi_boundaries(l)) return false;
         each(a.L.nall, [&](int q) { op_init_vcycle<CT>(a.g, a.st, a.L.all[q], t, blockDim.x); });
         if (!sync(PH_INIT, a.L.nall)) return false;
-        for (int l = maxl; l >= 0; l--) {
+        // down sweep (levels maxl .. 0), then up sweep (0 .. maxl), as one
+        // loop so that the relaxation loop is expanded once
+        for (int step = 0; step < 2 * (maxl + 1); step++) {
+            const bool down = step <= maxl;
+            const int l = down ? maxl - step : step - (maxl + 1);
             const int* sl = level(l);
-            each(a.L.cnt[l], [&](int q) {
-                op_vdown<CT>(a.g, a.bt, a.st, sl[q], a.vitems, a.vranges + 4 * (a.voff[l] + q));
-                __syncthreads();
-            });
-            if (!sync(PH_VDOWN, a.L.cnt[l])) return false;
-            if (!relax_until(l, 1.0)) return false;
-        }
-        for (int l = 0; l <= maxl; l++) {
-            const int* sl = level(l);
-            if (l > 0) {
+            if (down) {
+                each(a.L.cnt[l], [&](int q) {
+                    op_vdown<CT>(a.g, a.bt, a.st, sl[q], a.vitems, a.vranges + 4 * (a.voff[l] + q));
+                    __syncthreads();
+                });
+                if (!sync(PH_VDOWN, a.L.cnt[l])) return false;
+            } else if (l > 0) {
                 each(a.L.cnt[l], [&](int q) { op_coarse_correction<CT>(a.g, a.bt, a.st, sl[q], t); });
                 if (!sync(PH_CORRECT, a.L.cnt[l])) return false;
             }
-            if (!relax_until(l, 0.05)) return false;
-            each(a.L.cnt[l], [&](int q) { op_retire<CT>(a.g, a.st, sl[q], t, blockDim.x); });
-            if (!sync(PH_RETIRE, a.L.cnt[l])) return false;
-            if (!phi_boundaries(l)) return false;
+            if (!relax_until(l, down ? 1.0 : 0.05)) return false;
+            if (!down) {
+                each(a.L.cnt[l], [&](int q) { op_retire<CT>(a.g, a.st, sl[q], t, blockDim.x); });
+                if (!sync(PH_RETIRE, a.L.cnt[l])) return false;
+                if (!phi_boundaries(l)) return false;
+            }
         }
         return true;
     }

@@ -15,6 +15,11 @@ struct GridBarrier {
     unsigned int pad0;
     int abort;
     int pad;
+    // relaxation level sums published by one block: sum g of the launch in
+    // lsum_val[g & 1], then lsum_gen = g
+    unsigned int lsum_gen;
+    unsigned int pad1;
+    double lsum_val[2];
 };
 
 struct SolveArgs {

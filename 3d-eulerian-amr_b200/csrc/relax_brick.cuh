@@ -19,25 +19,13 @@ struct RelaxSmem {
     double red[2][NW];
 };
 
-// Stages the brick (slot base) into both buffers; returns the last sweep's
-// sum and leaves the relaxed interior value of this thread's cell in *out.
-// CT is the correction's storage and arithmetic type (FP64, or FP32 in the
-// mixed form); the sums of squares are formed in FP64 either way.
+// The sweeps on a brick staged in both buffers (every cell, ghosts
+// included): thread t owns interior cell c with dphi1 value d1.  Returns the
+// last sweep's sum and leaves the relaxed value of cell c in *out.
 template <int NX, typename CT = double>
-__device__ __forceinline__ double relax_brick(RelaxSmem<NX, CT>& sm, const CT* __restrict__ dphi,
-                                              const CT* __restrict__ dphi1, CT* out) {
-    constexpr int P = RelaxSmem<NX, CT>::P, P3 = RelaxSmem<NX, CT>::P3, NT = RelaxSmem<NX, CT>::NT,
-                  NW = RelaxSmem<NX, CT>::NW;
+__device__ __forceinline__ double relax_sweeps(RelaxSmem<NX, CT>& sm, int c, CT d1, CT* out) {
+    constexpr int P = RelaxSmem<NX, CT>::P, NW = RelaxSmem<NX, CT>::NW;
     const int t = threadIdx.x;
-    for (int q = t; q < P3; q += NT) {
-        const CT v = dphi[q];
-        sm.buf[0][q] = v;
-        sm.buf[1][q] = v;
-    }
-    const int i = t % NX + 1, j = (t / NX) % NX + 1, k = t / (NX * NX) + 1;
-    const int c = (k * P + j) * P + i;
-    const CT d1 = dphi1[c];
-    __syncthreads();
     double resid0 = 0.0, resid = 0.0;
     int iters = 0, cur = 0;
     do {
@@ -65,6 +53,34 @@ __device__ __forceinline__ double relax_brick(RelaxSmem<NX, CT>& sm, const CT* _
     } while (resid / resid0 > 0.5 && iters < 16);
     *out = sm.buf[cur][c];
     return resid;
+}
+
+// Interior cell of thread t in the (NX+2)^3 brick.
+template <int NX>
+__device__ __forceinline__ int relax_cell(int t) {
+    constexpr int P = NX + 2;
+    return ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
+}
+
+// Stages the brick (slot base) into both buffers;
+// returns the last sweep's sum and leaves the relaxed interior value of this
+// thread's cell in *out.  CT is the correction's storage and arithmetic type
+// (FP64, or FP32 in the mixed form); the sums of squares are formed in FP64
+// either way.
+template <int NX, typename CT = double>
+__device__ __forceinline__ double relax_brick(RelaxSmem<NX, CT>& sm, const CT* __restrict__ dphi,
+                                              const CT* __restrict__ dphi1, CT* out) {
+    constexpr int P3 = RelaxSmem<NX, CT>::P3, NT = RelaxSmem<NX, CT>::NT;
+    const int t = threadIdx.x;
+    for (int q = t; q < P3; q += NT) {
+        const CT v = dphi[q];
+        sm.buf[0][q] = v;
+        sm.buf[1][q] = v;
+    }
+    const int c = relax_cell<NX>(t);
+    const CT d1 = dphi1[c];
+    __syncthreads();
+    return relax_sweeps<NX, CT>(sm, c, d1, out);
 }
 
 // Barrier over `n` threads with id `id` (1..15; 0 is __syncthreads).

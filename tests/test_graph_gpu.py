@@ -48,6 +48,34 @@ def test_graph_solve_is_bitwise_plain(gpu, persistent):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("persistent", [1, 2])
+def test_persistent_solve_bitwise_plain_on_large_levels(gpu, persistent):
+    """The 4-level single star has levels of 1, 8, 64, 160 and 408 bricks.
+    With 148 or 296 cooperative blocks some levels have fewer bricks than
+    blocks (the relaxation loop that forms each level sum in one block while
+    the bricks compute the next pass) and some have more (two bricks per
+    block, level sums in every block); the solve must reproduce the plain
+    form bit for bit, pass for pass."""
+    import importlib.util
+    import os
+    from conftest import PKG
+    spec = importlib.util.spec_from_file_location("amr_initial", os.path.join(PKG, "initial.py"))
+    initial = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(initial)
+    a, b = make(gpu, 4), make(gpu, 4, persistent)
+    for x in (a, b):
+        initial.build_tree(x, "polytrope", 1.0e-6, 0.5, 0, 4, device=True)
+    assert [int((a.get_tree()["level"] == l).sum()) for l in range(5)] == [1, 8, 64, 160, 408]
+    ea, na = a.poisson_solve(1.0e-6)
+    eb, nb = b.graph_solve(1.0e-6)
+    assert na == nb and ea == eb
+    assert np.array_equal(a.relax_passes(), b.relax_passes())
+    assert np.array_equal(a.download_poisson(), b.download_poisson())
+    a.close()
+    b.close()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("persistent", [0, 1])
 def test_graph_grav_steps_are_bitwise_plain(gpu, persistent):
     g = load_golden("grav_poly_L2")
