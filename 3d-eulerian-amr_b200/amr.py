@@ -121,6 +121,7 @@ def load_library(path=LIB_PATH):
             lib.amr_state_sum.argtypes = [P, I, dp]
             lib.amr_mass_sum.argtypes = [P, I, dp]
             lib.amr_sum_lz.argtypes = [P, dp]
+            lib.amr_m1m2data.argtypes = [P, dp, dp]
         if hasattr(lib, "amr_write_checkpoint"):
             lib.amr_write_checkpoint.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(BinaryHeader), D]
             lib.amr_read_checkpoint.argtypes = [P, ctypes.c_char_p, ctypes.POINTER(BinaryHeader)]
@@ -515,4 +516,20 @@ class AMR:
         out = np.zeros(1)
         self._check(self.lib.amr_sum_lz(self.ctx, _dptr(out)))
         return float(out[0])
+
+    M1M2_FIELDS = ("m1", "m2", "mc", "js1", "js2", "jorb", "jc", "a", "q", "total_energy", "kinetic", "I1", "I2",
+                   "Ic", "V1", "V2")
+
+    def m1m2data(self):
+        """Binary::M1M2data: (dict of the 16 scalars plus x1, xdot1, x2,
+        xdot2 as 3-vectors, the L1 point as (phi_eff, x, y, z)), and the raw
+        28-value array in the C ABI's order."""
+        out = np.zeros(28)
+        l1 = np.zeros(4)
+        self._check(self.lib.amr_m1m2data(self.ctx, _dptr(out), _dptr(l1)))
+        d = {k: float(out[i]) for i, k in enumerate(self.M1M2_FIELDS)}
+        for i, k in enumerate(("x1", "xdot1", "x2", "xdot2")):
+            d[k] = out[16 + 3 * i:19 + 3 * i].copy()
+        d["l1"] = l1
+        return d, out
 

@@ -231,6 +231,15 @@ int amr_ztwd_step(amr_ctx* ctx, double dt, double tol, double dynamic_range, int
 int amr_state_sum(amr_ctx* ctx, int field, double* out);
 int amr_mass_sum(amr_ctx* ctx, int frac, double* out);
 int amr_sum_lz(amr_ctx* ctx, double* out);
+/* Binary::M1M2data (binary/binary.cpp:718-823, ZTWD) on the current state,
+ * potential (with ghosts) and face forces: the L1 point (find_l1
+ * :390-447), the lobe of every cell (mark_lobes :449-492 with the lobe
+ * centres of find_phimin :642-690), then out[28] = m1, m2, mc, js1, js2,
+ * jorb, jc, a, q, total_energy, kinetic, I1, I2, Ic, V1, V2, x1[3],
+ * xdot1[3], x2[3], xdot2[3]; l1[4] (may be NULL) = the L1 point's
+ * effective potential, x, y, z.  Searches and sums in the reference's
+ * orders. */
+int amr_m1m2data(amr_ctx* ctx, double* out, double* l1);
 
 /* ---- checkpoints ------------------------------------------------------------
  * Files in the reference's checkpoint format (X.*.chk): the BINARY build's

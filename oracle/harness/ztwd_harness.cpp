@@ -165,7 +165,7 @@ int main(int argc, char* argv[]) {
     extra.push_back(double(nsteps));
     for (double d : dts) extra.push_back(d);
     // diagnostics of the final state: Binary::mass_sum of both stars,
-    // Binary::sum_lz, GridNode::state_sum of the density
+    // Binary::sum_lz, GridNode::state_sum of the density, Binary::M1M2data
     for (int frac = 0; frac < 2; frac++) {
         const Vector<Real, 4> m = root->mass_sum(frac);
         for (int q = 0; q < 4; q++) extra.push_back(m[q]);
@@ -173,6 +173,16 @@ int main(int argc, char* argv[]) {
     extra.push_back(root->sum_lz());
     const Vector<State, 4> ss = root->state_sum();
     for (int q = 0; q < 4; q++) extra.push_back(ss[q][0]);
+    // Binary::M1M2data (binary/binary.cpp:718-823): L1 point, lobe marking,
+    // the per-star and total integrals
+    Binary::binary_integrals_t bi;
+    root->M1M2data(&bi);
+    const double sc[16] = {bi.m1, bi.m2, bi.mc, bi.js1, bi.js2, bi.jorb, bi.jc, bi.a,
+                           bi.q,  bi.total_energy, bi.kinetic, bi.I1, bi.I2, bi.Ic, bi.V1, bi.V2};
+    for (double v : sc) extra.push_back(v);
+    const _3Vec* vec[4] = {&bi.x1, &bi.xdot1, &bi.x2, &bi.xdot2};
+    for (const _3Vec* v : vec)
+        for (int q = 0; q < 3; q++) extra.push_back((*v)[q]);
     dump(argv[4], root, root, root->get_time(), extra);
     if (chk) {
         FILE* fp = fopen(argv[5], "wb");

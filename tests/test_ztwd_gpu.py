@@ -141,3 +141,31 @@ def test_ztwd_diagnostics_match_reference(gpu, table_path):
     assert a.sum_lz() == diag[8]
     assert np.array_equal(a.state_sum(0), diag[9:13])
     a.close()
+
+
+@pytest.mark.gpu
+def test_ztwd_m1m2data_matches_reference(gpu, table_path):
+    """Binary::M1M2data (the L1 point, the lobes, the per-star and total
+    integrals) on the reference's own final state and potential of ztwd_L2,
+    with the face forces formed from that potential: the reference's values
+    bit for bit."""
+    g = load_golden("ztwd_L2")
+    nsteps = int(g["args"][1])
+    ref = g["extra"][8 + nsteps + 13:]
+    assert ref.size == 28
+    a = gpu.AMR(**ztwd_config(int(g["final_level"].max())))
+    a.ztwd_set_frame(float(g["extra"][4]), float(g["extra"][5]), 0.0, 0.0)
+    a.load_tree(g["final_level"], g["final_loc"], g["final_age"])
+    bw = a.bw
+    U = np.zeros((a.nbricks, a.nf, a.gnx, a.gnx, a.gnx))
+    U[:, :, bw:-bw, bw:-bw, bw:-bw] = g["final_U"]
+    a.upload_state(U)
+    P = np.zeros((8, a.nbricks, a.pnx, a.pnx, a.pnx))
+    P[0] = g["final_phi"]
+    a.upload_poisson(P)
+    a.compute_forces()
+    d, out = a.m1m2data()
+    bad = [(i, out[i], ref[i]) for i in range(28) if out[i] != ref[i]]
+    assert not bad, bad
+    assert d["m1"] > 0 and d["m2"] > 0 and 0.0 < d["q"] < 2.0
+    a.close()
