@@ -251,6 +251,17 @@ def reference_arm_single_star(args):
     return 0
 
 
+def aggregate(ms_total, cells, world, dist, device="cuda"):
+    """Whole-job figures over the replicas: the slowest rank's device time
+    (max) and the cells of all ranks (sum); every rank gets both."""
+    import torch
+    t = torch.tensor([float(ms_total), float(cells)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
+    return float(t[0]), float(t[1])
+
+
 def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile=False):
     """Build the workload and time K steps of one form of our path.
 
@@ -337,11 +348,8 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
     # state after warm-up + timed steps, for the error of one form against another
     res["final"] = {"U": a.download_state(), "phi": a.download_poisson()[0], "level": a.get_tree()["level"],
                     "loc": a.get_tree()["loc"]}
-    t = torch.tensor([sum(times), float(cells)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
-    res["ms_total"], res["cells"] = float(t[0]), float(t[1])
+    t = aggregate(sum(times), cells, world, dist)
+    res["ms_total"], res["cells"] = t
     res["value"] = res["cells"] / (res["ms_total"] / 1000.0)
     res["ms_per_step"] = res["ms_total"] / args.steps
     res["bricks"] = a.nbricks
@@ -373,11 +381,8 @@ def run_form(amr, ini, form, args, world, local, torch, dist, e2e=False, profile
             h2d += 8 * n_in
             d2h += 8 * n_out
         barrier()
-        et = torch.tensor([sum(e_times), float(e_cells)], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(et[0:1], op=dist.ReduceOp.MAX)
-            dist.all_reduce(et[1:2], op=dist.ReduceOp.SUM)
-        res["e2e"] = {"value": float(et[1]) / (float(et[0]) / 1000.0), "unit": UNIT,
+        et = aggregate(sum(e_times), e_cells, world, dist)
+        res["e2e"] = {"value": et[1] / (et[0] / 1000.0), "unit": UNIT,
                       "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
 
     if profile:
@@ -863,11 +868,8 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
     res["persistent"]["relax_passes_per_step_by_level"] = [
         round(float(x) / args.steps, 1) for x in (a.relax_passes() - rp0)[:nl]]
     a.close()
-    t = torch.tensor([sum(times), float(cells)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
-    res["ms_total"], res["cells"] = float(t[0]), float(t[1])
+    t = aggregate(sum(times), cells, world, dist)
+    res["ms_total"], res["cells"] = t
     res["value"] = res["cells"] / (res["ms_total"] / 1000.0)
     res["ms_per_step"] = res["ms_total"] / args.steps
     res["leaf_cells_per_step"] = cells / args.steps
@@ -900,13 +902,10 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
         d2h += 8 * n_out
     barrier()
     a.close()
-    et = torch.tensor([sum(e_times), float(e_cells)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(et[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(et[1:2], op=dist.ReduceOp.SUM)
-    res["e2e"] = {"value": float(et[1]) / (float(et[0]) / 1000.0), "unit": UNIT,
+    et = aggregate(sum(e_times), e_cells, world, dist)
+    res["e2e"] = {"value": et[1] / (et[0] / 1000.0), "unit": UNIT,
                   "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps,
-                  "ms_per_step": float(et[0]) / args.steps, "ms_steps": [round(x, 3) for x in e_times]}
+                  "ms_per_step": et[0] / args.steps, "ms_steps": [round(x, 3) for x in e_times]}
     import shutil
     shutil.rmtree(tdir, ignore_errors=True)
     return res
