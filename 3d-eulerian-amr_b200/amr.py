@@ -135,6 +135,8 @@ def load_library(path=LIB_PATH):
                 lib.amr_solve_phase_waits.argtypes = [P, dp, I, dp, ctypes.POINTER(ctypes.c_longlong)]
             if hasattr(lib, "amr_relax_passes"):
                 lib.amr_relax_passes.argtypes = [P, ctypes.POINTER(ctypes.c_longlong), I]
+            if hasattr(lib, "amr_set_wait_limit"):
+                lib.amr_set_wait_limit.argtypes = [P, I]
         _lib = lib
     return _lib
 
@@ -441,6 +443,10 @@ class AMR:
         n = ctypes.c_longlong()
         self._check(self.lib.amr_solve_totals(self.ctx, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+    def set_wait_limit(self, polls):
+        """Polls per bounded wait of the persistent solve (0: the default)."""
+        self._check(self.lib.amr_set_wait_limit(self.ctx, int(polls)))
 
     def relax_passes(self, n=16):
         """Relaxation passes per level since the context started (every form)."""

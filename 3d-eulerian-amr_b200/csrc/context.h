@@ -86,6 +86,7 @@ struct amr_ctx {
     int vcycle_max_outer = 1000;
     long long relax_calls = 0, relax_sweeps_total = 0;
     long long relax_level[16] = {};  // relaxation passes per level
+    int wait_limit = 1 << 22;        // polls per bounded wait of the persistent solve
     bool topo_dirty = true;
     long long topo_version = 0;  // bumped by every rebuild_topology
     // ZTWD state: frame + EOS passed to its kernels, EOS-failure word

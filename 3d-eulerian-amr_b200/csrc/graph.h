@@ -56,6 +56,8 @@ struct Control {
     unsigned long long level_sum_ns;
     unsigned long long level_sum_n;
     long long relax_level[MAX_LEVELS];  // relaxation passes per level
+    int wait_limit;                     // persistent solve: polls per bounded wait (<= 0: default)
+    int pad2;
 };
 
 // phase classes of the persistent solve

@@ -88,7 +88,7 @@ int ensure_state(amr_ctx* c) {
     CUDA_TRY(cudaMalloc(&g->d_ctl, sizeof(Control)));
     CUDA_TRY(cudaMemsetAsync(g->d_ctl, 0, sizeof(Control), c->stream));
     CUDA_TRY(cudaMallocHost(&g->h_ctl, sizeof(Control)));
-    CUDA_TRY(cudaMallocHost(&g->h_steps, sizeof(int) * 4));
+    CUDA_TRY(cudaMallocHost(&g->h_steps, sizeof(int) * 5));
     CUDA_TRY(cudaMalloc(&g->d_nest, sizeof(double) * c->cap));
     CUDA_TRY(cudaMalloc(&g->d_snap, sizeof(double) * 2 * SNAP_STRIDE * (size_t)c->cap));
     CUDA_TRY(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
@@ -436,6 +436,8 @@ int set_limits(amr_ctx* c, int max_cycles, int steps) {
     CUDA_TRY(cudaMemcpyAsync(&g->d_ctl->max_cycles, &hs[0], sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemcpyAsync(&g->d_ctl->max_outer, &hs[1], sizeof(int), cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemcpyAsync(&g->d_ctl->status, &hs[2], sizeof(int), cudaMemcpyHostToDevice, c->stream));
+    hs[4] = c->wait_limit;
+    CUDA_TRY(cudaMemcpyAsync(&g->d_ctl->wait_limit, &hs[4], sizeof(int), cudaMemcpyHostToDevice, c->stream));
     if (steps >= 0)
         CUDA_TRY(cudaMemcpyAsync(&g->d_ctl->steps, &hs[3], sizeof(int), cudaMemcpyHostToDevice, c->stream));
     return AMR_OK;
@@ -550,6 +552,14 @@ int amr_solve_totals(amr_ctx* c, double* ms, long long* count) {
     if (!c || !ms || !count) return AMR_ERR_ARG;
     *ms = c->gs ? c->gs->ps_ms_total : 0.0;
     *count = c->gs ? c->gs->ps_count : 0;
+    return AMR_OK;
+}
+
+// Polls per bounded wait of the persistent solve before it aborts with
+// AMR_ERR_TIMEOUT; 0 restores the default (2^22).
+int amr_set_wait_limit(amr_ctx* c, int polls) {
+    if (!c || polls < 0) return AMR_ERR_ARG;
+    c->wait_limit = polls > 0 ? polls : (1 << 22);
     return AMR_OK;
 }
 

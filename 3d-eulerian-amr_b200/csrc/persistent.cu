@@ -16,9 +16,10 @@
 // decision without another barrier.  Per-brick values are double-buffered
 // by pass so a block still summing one pass cannot see the next pass's.
 //
-// The grid barrier spins with a bound: a block that waits longer than
-// BARRIER_SPINS polls sets the abort word, every block leaves at its next
-// barrier, and the host reports AMR_ERR_TIMEOUT.
+// The grid barrier spins with a bound: a block that waits longer than the
+// control block's wait limit (BARRIER_SPINS polls by default) sets the
+// abort word, every block leaves at its next barrier, and the host reports
+// AMR_ERR_TIMEOUT.
 #include <cuda_runtime.h>
 
 #include "graph_ops.cuh"
@@ -39,7 +40,7 @@ __device__ __forceinline__ unsigned ld_volatile(const unsigned* p) { return *(co
 // The arrival counter only grows: barrier k of the launch completes when it
 // reaches k * gridDim.x (target, kept by thread 0), so an arrival is one
 // fire-and-forget release add and the wait one acquire load per poll.
-__device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned& target) {
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned& target, unsigned long long limit) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -56,7 +57,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned& target) {
                 good = 0;
                 break;
             }
-            if (++spins > BARRIER_SPINS) {
+            if (++spins > limit) {
                 atomicExch(&bar->abort, 1);
                 good = 0;
                 break;
@@ -80,7 +81,7 @@ __device__ __forceinline__ void lsum_publish(GridBarrier* bar, unsigned g, doubl
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&bar->lsum_gen), "r"(g) : "memory");
 }
 
-__device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& r) {
+__device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& r, unsigned long long limit) {
     __shared__ double s_r;
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
@@ -94,7 +95,7 @@ __device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& 
                 good = 0;
                 break;
             }
-            if (++spins > BARRIER_SPINS) {
+            if (++spins > limit) {
                 atomicExch(&bar->abort, 1);
                 good = 0;
                 break;
@@ -122,6 +123,7 @@ struct Solver {
     int max_outer;
     unsigned bar_target = 0;    // thread 0: arrivals that complete the next barrier
     unsigned lsum_gen = 0;      // level sums published so far in this launch
+    unsigned long long spin_limit = BARRIER_SPINS;  // polls per bounded wait
     unsigned long long t_last;  // block 0: global time at the last barrier exit
     // block 0's phase accounting, in shared memory
     unsigned long long* ph_ns;
@@ -139,7 +141,7 @@ struct Solver {
     // barrier closing a phase of class ph
     __device__ bool sync(int ph, int units) {
         const unsigned long long t_arrive = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
-        const bool ok = grid_sync(a.bar, bar_target);
+        const bool ok = grid_sync(a.bar, bar_target, spin_limit);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             const unsigned long long t = now();
             ph_wait[ph] += t - t_arrive;
@@ -253,7 +255,7 @@ struct Solver {
     // time it waits for it)
     __device__ bool wait_sum(double& r) {
         const unsigned long long t0 = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
-        const bool ok = lsum_wait(a.bar, lsum_gen, r);
+        const bool ok = lsum_wait(a.bar, lsum_gen, r, spin_limit);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             ph_wait[PH_COUNT] += now() - t0;
             ph_wait[PH_COUNT + 1]++;
@@ -464,6 +466,10 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
     __shared__ unsigned s_ph_n[PH_COUNT];
     __shared__ double s_ph_bytes[PH_COUNT];
     __shared__ unsigned long long s_ph_wait[PH_COUNT + 2];
+    {
+        const int wl = *(volatile int*)&a.ctl->wait_limit;
+        if (wl > 0) s.spin_limit = (unsigned long long)wl;
+    }
     __shared__ unsigned s_lvl_n[MAX_LEVELS];
     s.lvl_n = s_lvl_n;
     if (threadIdx.x < MAX_LEVELS) s_lvl_n[threadIdx.x] = 0;

@@ -306,6 +306,13 @@ int amr_solve_totals(amr_ctx* ctx, double* ms, long long* count);
  * per level since the context started, in every form of the solve;
  * per_level[0 .. n-1]. */
 int amr_relax_passes(amr_ctx* ctx, long long* per_level, int n);
+/* Polls each bounded wait of the persistent solve (grid barriers, published
+ * level sums) makes before the solve gives up: the waiting block sets the
+ * abort word, every block leaves at its next wait, and amr_graph_solve (or
+ * the step that called it) returns AMR_ERR_TIMEOUT with the context still
+ * usable.  Replaces the reference's unbounded loops; 0 restores the default
+ * 2^22 polls (seconds). */
+int amr_set_wait_limit(amr_ctx* ctx, int polls);
 /* Of those phase times, the part spent at each phase's closing grid barrier
  * (block 0, from its arrival to the barrier's exit: the slowest block's extra
  * work plus the barrier itself), and the time spent forming the relaxation

@@ -115,3 +115,28 @@ def test_graph_steps_match_reference(gpu, name):
     s = U.reshape(U.shape[0], U.shape[1], -1).sum(axis=2)
     rel = np.abs(s - g["final_Usum"]) / np.maximum(g["final_Uabs"], 1e-300)
     assert rel.max() <= 1e-11
+
+
+@pytest.mark.gpu
+def test_persistent_wait_limit_times_out_and_context_recovers(gpu):
+    """A wait limit of one poll makes some grid barrier or level-sum wait of
+    the persistent solve run out (no block is made to fault or hang): the
+    solve returns AMR_ERR_TIMEOUT, and with the default limit back the same
+    context solves again, bit for bit like the plain form."""
+    g = load_golden("poisson_poly_L2")
+    a, b = make(gpu, 2), make(gpu, 2, 2)
+    load_state(a, g)
+    load_state(b, g)
+    b.set_wait_limit(1)
+    with pytest.raises(gpu.AmrError) as e:
+        b.graph_solve(1.0e-7)
+    assert e.value.code == -5  # AMR_ERR_TIMEOUT
+    b.set_wait_limit(0)
+    load_state(b, g)
+    b.upload_poisson(np.zeros_like(b.download_poisson()))
+    ea, na = a.poisson_solve(1.0e-7)
+    eb, nb = b.graph_solve(1.0e-7)
+    assert na == nb and ea == eb
+    assert np.array_equal(a.download_poisson()[0], b.download_poisson()[0])
+    a.close()
+    b.close()
