@@ -46,7 +46,8 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned& target, un
     if (threadIdx.x == 0) {
         int good = 1;
         target += gridDim.x;
-        __threadfence();
+        // the release orders the whole block's writes (made before the block
+        // barrier above) before the arrival, at GPU scope
         asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&bar->count), "r"(1u) : "memory");
         unsigned long long spins = 0;
         for (;;) {
