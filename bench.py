@@ -74,7 +74,7 @@ BYTES_PER_BRICK = {
 # dram__bytes_write.sum, caches flushed before each launch); those launches
 # carry 2.72 GB of algorithmic bytes each.  The solve's arrays stay in L2
 # across its V-cycles, so DRAM sees the cold fill and the dirty write-back.
-ZT_SOLVE_DRAM_BYTES_PER_LAUNCH = 16.35e6
+ZT_SOLVE_DRAM_BYTES_PER_LAUNCH = 16.69e6
 
 
 def load_amr():
