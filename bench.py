@@ -1085,7 +1085,8 @@ def run_single_star(amr, ini, args, world, local, torch, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=8,
+                    help="timed steps (the default 8 covers one regrid cadence of the binary)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1140,7 +1141,10 @@ def main():
             "config": {"workload": ZT_WORKLOAD, "form": "mixed persistent", "levels": ZT_LEVELS,
                        "bricks": head["bricks"], "leaf_cells_per_step": head["leaf_cells_per_step"],
                        "tol_l1": ZT_TOL, "binary": dict(ini.BINARY),
-                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"},
+                       "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas",
+                       "timed_steps": [args.warmup, args.warmup + args.steps - 1],
+                       "regrids_in_timed_steps": sum(1 for q in range(args.warmup, args.warmup + args.steps)
+                                                     if q % 8 == 0)},
             "roofline": dict(roofline_persistent(head, ZT_SOLVE_DRAM_BYTES_PER_LAUNCH),
                              traffic_note="ncu DRAM read+write per solve launch on this workload (L2-resident "
                                           "arrays: far below the algorithmic bytes)"),
