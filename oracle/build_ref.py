@@ -22,15 +22,18 @@ Variants:
   ppm  g05 with PPM reconstruction (euler_defs.h:24 switched on) and BW 3,
        the ghost width PPM needs (reconstruct.cpp:22-58 reads cells i-3..i+2
        of face i)
-  ztwd BINARY physics with the ZTWD state as binary/binary_defs.h sets it
-       (PPM, BW 3, Z_REFLECT, GRID_DIM 1), except 8^3 interior cells per
-       brick instead of 12^3 (GNX 8+2*BW, the brick the CUDA path is written
-       for); driven by oracle/harness/ztwd_harness.cpp, with the reference's
-       own binary/initialize.cpp as the initial data
+  ztwd12 BINARY physics with the ZTWD state exactly as binary/binary_defs.h
+       sets it (PPM, BW 3, Z_REFLECT, GRID_DIM 1, 12^3 interior cells per
+       brick); driven by oracle/harness/ztwd_harness.cpp, with the
+       reference's own binary/initialize.cpp as the initial data
+  ztwd the same with 8^3 interior cells per brick (GNX 8+2*BW), a second
+       brick size the CUDA path also runs
 
-Run:  python oracle/build_ref.py [--reference /root/reference]
-When the reference tree is absent (e.g. on a GPU box) this is a no-op and the
-previously built binaries are used as they are.
+Run:  python oracle/build_ref.py [--reference DIR]
+The reference tree is DIR, else $AMR_REFERENCE, else a directory named
+`reference` beside this repository's directory.  When it is absent (e.g. on
+a GPU box) this is a no-op and the previously built binaries are used as
+they are.
 """
 
 import argparse
@@ -87,6 +90,8 @@ def _patch(src, variant):
              "inline Real abs(Real a) {\n\treturn fabs(a);\n}", "")
     # Silo is not installed; only the output path uses it.
     shutil.copy(os.path.join(HERE, "stubs", "silo.h"), os.path.join(src, "silo.h"))
+    if variant == "ztwd12":
+        return
     if variant == "ztwd":
         # binary/binary_defs.h:31-35: 12^3 interior cells -> 8^3
         bdefs = os.path.join(src, "binary", "binary_defs.h")
@@ -124,8 +129,9 @@ def _stale(out, inputs):
 def build_variant(reference, variant, jobs=8):
     src = os.path.join(REF_OUT, "src_" + variant)
     exe = os.path.join(REF_OUT, variant + "_harness")
-    harness = os.path.join(HERE, "harness", "ztwd_harness.cpp" if variant == "ztwd" else "amr_harness.cpp")
-    sources = BINARY_SOURCES if variant == "ztwd" else EULER_SOURCES
+    binary = variant in ("ztwd", "ztwd12")
+    harness = os.path.join(HERE, "harness", "ztwd_harness.cpp" if binary else "amr_harness.cpp")
+    sources = BINARY_SOURCES if binary else EULER_SOURCES
     inputs = [harness, os.path.abspath(__file__), os.path.join(HERE, "stubs", "silo.h"),
               os.path.join(HERE, "harness", "dump.h")]
     if not _stale(exe, inputs):
@@ -178,7 +184,16 @@ def build_helm(reference):
     return exe
 
 
-def build(reference="/root/reference", variants=("g05", "zr", "ppm", "ztwd")):
+def default_reference():
+    """$AMR_REFERENCE, else `reference` beside the repository's directory."""
+    env = os.environ.get("AMR_REFERENCE")
+    if env:
+        return env
+    return os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+
+
+def build(reference=None, variants=("g05", "zr", "ppm", "ztwd", "ztwd12")):
+    reference = reference or default_reference()
     if not os.path.isdir(reference):
         print("[oracle] reference tree not present; using prebuilt oracle/_ref binaries")
         return []
@@ -192,7 +207,7 @@ def build(reference="/root/reference", variants=("g05", "zr", "ppm", "ztwd")):
 
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", default=None)
     a = ap.parse_args()
     for e in build(a.reference):
         print(e)

@@ -37,13 +37,31 @@ CASES = {
     # ZTWD binary (BINARY build): maxlevel, steps
     "ztwd_L2": ("ztwd", "ztwd", [2, 3]),
     "ztwd_L3": ("ztwd", "ztwd", [3, 9]),
+    # the same on the BINARY build's own 12^3-cell bricks
+    "ztwd12_L2": ("ztwd12", "ztwd", [2, 3]),
+    "ztwd12_L3": ("ztwd12", "ztwd", [3, 9]),
+    # the configured sizes: the 4-level single star (9 coupled steps, regrids
+    # at steps 0 and 8) and the 5-level binary on 12^3 bricks (10
+    # BinaryDriver steps, regrids at steps 0 and 8)
+    "grav_poly_L4": ("g05", "grav", ["polytrope", 4, 9, 1e-6]),
+    "ztwd12_L5": ("ztwd12", "ztwd", [5, 10]),
 }
 # cases whose full state would make a large fixture keep only the tree and
 # per-brick, per-field sums and absolute sums of the interior cells
-SUMMARY_ONLY = {"hydro_blast_L2", "hydro_bump_L3", "poisson_poly_L3", "hydro_ppm_blast_L2"}
-# for these the final conserved state is kept as sums only (the potential in
-# full): the initial state is needed in full to start from the same data
-FINAL_SUMMARY = {"grav_poly_L2", "grav_ppm_poly_L2", "ztwd_L3"}
+SUMMARY_ONLY = {"hydro_bump_L3"}
+# Poisson cases whose state is rebuilt by the test from the host initializer:
+# sums of the state, every cell of the potential after each V-cycle
+PHI_ONLY = {"poisson_poly_L3"}
+# cases too large for every cell: the initial state as sums only (a test
+# regenerates it with a zero-step run of the same harness and checks the
+# sums), the final state as sums plus every cell of a fixed sample of bricks
+# (evenly spaced in depth-first order) and the per-field maxima
+SAMPLED = {"grav_poly_L4": 24, "ztwd12_L5": 24}
+
+
+def sample_bricks(n, k):
+    """Indices of k bricks evenly spaced over n (all of them when n <= k)."""
+    return np.unique(np.linspace(0, n - 1, min(n, k)).round().astype(np.int64))
 
 
 def interior(d, U):
@@ -51,7 +69,7 @@ def interior(d, U):
     return U[:, :, b:-b, b:-b, b:-b].copy()
 
 
-def pack(prefix, d, summary):
+def pack(prefix, d, summary, sample=0, phi=False):
     U = interior(d, d.U)
     out = {
         prefix + "level": d.level, prefix + "loc": d.loc, prefix + "age": d.age,
@@ -62,18 +80,26 @@ def pack(prefix, d, summary):
     }
     if not summary:
         out[prefix + "U"] = U
-    if d.P is not None and not summary:
+    if d.P is not None and (phi or not summary):
         out[prefix + "phi"] = d.P["phi"]
     if d.P is not None:
         out[prefix + "phisum"] = d.P["phi"][:, 1:-1, 1:-1, 1:-1].reshape(d.nnodes, -1).sum(axis=1)
+    if sample:
+        idx = sample_bricks(U.shape[0], sample)
+        out[prefix + "sample"] = idx
+        out[prefix + "sample_U"] = U[idx]
+        out[prefix + "Umax"] = np.abs(U).max(axis=(0, 2, 3, 4))
+        if d.P is not None:
+            out[prefix + "sample_phi"] = d.P["phi"][idx]
+            out[prefix + "phimax"] = np.float64(np.abs(d.P["phi"][:, 1:-1, 1:-1, 1:-1]).max())
     return out
 
 
-def run_case(name, workdir):
+def run_case(name, workdir, threads=1):
     variant, mode, args = CASES[name]
     exe = os.path.join(ROOT, "oracle", "_ref", variant + "_harness")
     out = os.path.join(workdir, name + ".bin")
-    env = dict(os.environ, OMP_NUM_THREADS="1")
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     if mode == "ztwd":
         # the BINARY build reads ./helmholtz.table at start-up (helmeos.cpp:73-130)
         sys.path.insert(0, os.path.join(ROOT, "3d-eulerian-amr_b200"))
@@ -84,7 +110,7 @@ def run_case(name, workdir):
     if r.returncode != 0:
         raise RuntimeError(r.stdout + r.stderr)
     d0 = read_dump(out + ".init")
-    summ = name in SUMMARY_ONLY
+    summ = name in SUMMARY_ONLY or name in SAMPLED or name in PHI_ONLY
     res = {"variant": np.array(variant), "mode": np.array(mode), "args": np.array([str(a) for a in args]),
            "bw": np.int32(d0.bw), "nx": np.int32(d0.gnx - 2 * d0.bw)}
     res.update(pack("init_", d0, summ))
@@ -92,14 +118,12 @@ def run_case(name, workdir):
         ncyc = int(args[2])
         for c in range(ncyc):
             dc = read_dump(out + ".%d" % c)
-            res.update(pack("cycle%d_" % c, dc, summ))
+            res.update(pack("cycle%d_" % c, dc, summ, phi=name in PHI_ONLY))
             res["extra"] = dc.extra
     else:
         d1 = read_dump(out)
         res["extra"] = d1.extra
-        res.update(pack("final_", d1, summ or name in FINAL_SUMMARY))
-        if name in FINAL_SUMMARY:
-            res["final_phi"] = d1.P["phi"]
+        res.update(pack("final_", d1, summ, SAMPLED.get(name, 0)))
     return res
 
 
