@@ -476,7 +476,7 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
     const int min_bw = cfg->reconstruction == AMR_RECON_PPM ? 3 : 2;
     const bool ztwd = cfg->physics == AMR_PHYSICS_ZTWD;
     if (cfg->physics < AMR_PHYSICS_EULER || cfg->physics > AMR_PHYSICS_ZTWD ||
-        (ztwd && (cfg->reconstruction != AMR_RECON_PPM || cfg->nx != 8)))
+        (ztwd && (cfg->reconstruction != AMR_RECON_PPM || (cfg->nx != 8 && cfg->nx != 12))))
         return AMR_ERR_ARG;
     if (cfg->nf != (ztwd ? (int)ZTWD_NF : 6) || cfg->bw < min_bw || cfg->bw > 4 || cfg->nx < 4 || (cfg->nx % 4) != 0 ||
         cfg->max_refine_level < 0 || cfg->max_refine_level > 12 || cfg->max_bricks < 0 ||
@@ -1024,6 +1024,7 @@ int amr_fused_sub_step(amr_ctx* c, double dt, double beta, int blocks_per_sm) {
     a.Fy = c->st.Fy;
     a.Fz = c->st.Fz;
     a.err = reinterpret_cast<int*>(c->d_fctl + 1);
+    a.wait_limit = (unsigned long long)c->fused_wait_limit;
     cudaError_t e;
     {
         ProfScope ps_(c->prof, KC_FUSED, c->stream, (long long)c->nfwork);

@@ -118,6 +118,7 @@ int read_node(amr_ctx* c, FILE* fp, int level, const int* loc, const int* exp_of
         c->err = "checkpoint: truncated node trailer";
         return AMR_ERR_STATE;
     }
+    c->chk_refine_alpha = alpha;  // GridNode::refine_alpha is one static: every node writes the same
     out.push_back(std::move(r));
     for (int q = 0; q < 8; q++) {
         if (!child[q]) continue;
@@ -152,6 +153,7 @@ int amr_write_checkpoint(amr_ctx* c, const char* path, const amr_binary_header* 
         c->err = std::string("cannot open ") + path;
         return AMR_ERR_ARG;
     }
+    if (refine_alpha < 0.0) refine_alpha = c->chk_refine_alpha;
     bool ok = !hdr || put_header(f.fp, hdr);
     std::vector<double> cells((size_t)g.gnx3 * g.nf);
     for (int e = 0; e < n && ok; e++) {

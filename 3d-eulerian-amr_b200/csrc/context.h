@@ -87,6 +87,8 @@ struct amr_ctx {
     long long relax_calls = 0, relax_sweeps_total = 0;
     long long relax_level[16] = {};  // relaxation passes per level
     int wait_limit = 1 << 22;        // polls per bounded wait of the persistent solve
+    int fused_wait_limit = 1 << 24;  // polls per wait of the fused substep for a child's faces
+    double chk_refine_alpha = 1.0;   // GridNode::refine_alpha of the last checkpoint read
     bool topo_dirty = true;
     long long topo_version = 0;  // bumped by every rebuild_topology
     // ZTWD state: frame + EOS passed to its kernels, EOS-failure word

@@ -70,6 +70,9 @@ enum SolvePhase {
 void launch_relax_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int level,
                       int mode, double ratio, cudaGraphConditionalHandle cond, Control* ctl, double* pres,
                       double* nest, unsigned int* counter, double* snap, size_t snap_stride, cudaStream_t s);
+// raises the dynamic shared-memory limit of the relaxation kernels (call
+// outside stream capture)
+int relax_dev_attributes();
 void launch_error_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int nlevels,
                       double tol, cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest,
                       unsigned int* counter, cudaStream_t s);

@@ -39,14 +39,14 @@ using namespace amr;
         if (rc__) return rc__; \
     } while (0)
 
-// doubles per brick in one face-snapshot buffer: 6 faces of nx*nx (nx = 8)
-constexpr size_t SNAP_STRIDE = 6 * 8 * 8;
+// entries per brick in one face-snapshot buffer: 6 faces of nx*nx
+inline size_t snap_stride(const amr_ctx* c) { return 6 * (size_t)c->geom.nx * c->geom.nx; }
 
 struct GraphState {
     Control* d_ctl = nullptr;
     Control* h_ctl = nullptr;  // pinned mirror
     double* d_nest = nullptr;
-    double* d_snap = nullptr;  // [2][cap][6][8][8] first-interior dphi layers
+    double* d_snap = nullptr;  // [2][cap][6][nx][nx] first-interior dphi layers
     unsigned int* d_counter = nullptr;
     int* h_steps = nullptr;     // pinned scalar staging
     cudaGraphExec_t step_exec = nullptr;
@@ -90,11 +90,15 @@ int ensure_state(amr_ctx* c) {
     CUDA_TRY(cudaMallocHost(&g->h_ctl, sizeof(Control)));
     CUDA_TRY(cudaMallocHost(&g->h_steps, sizeof(int) * 5));
     CUDA_TRY(cudaMalloc(&g->d_nest, sizeof(double) * c->cap));
-    CUDA_TRY(cudaMalloc(&g->d_snap, sizeof(double) * 2 * SNAP_STRIDE * (size_t)c->cap));
+    CUDA_TRY(cudaMalloc(&g->d_snap, sizeof(double) * 2 * snap_stride(c) * (size_t)c->cap));
+    if (relax_dev_attributes() != 0 || solve_persistent_attributes() != 0) {
+        c->err = "shared-memory attributes of the relaxation kernels";
+        return AMR_ERR_CUDA;
+    }
     CUDA_TRY(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CUDA_TRY(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned int) * 4, c->stream));
     if (c->cfg.persistent_solve) {
-        g->pblocks = solve_persistent_blocks(c->cfg.precision, c->cfg.persistent_solve);
+        g->pblocks = solve_persistent_blocks(c->geom.nx, c->cfg.precision, c->cfg.persistent_solve);
         if (g->pblocks <= 0) {
             c->err = "no cooperative launch configuration for the persistent solve";
             return AMR_ERR_CUDA;
@@ -215,13 +219,13 @@ int rec_relax_until(amr_ctx* c, cudaStream_t s, int l, double ratio, int depth) 
         c, s, depth,
         [&](cudaStream_t q, cudaGraphConditionalHandle h) {
             launch_relax_dev(c->geom, c->bt, c->st, g->L, l, 0, ratio, h, g->d_ctl, c->d_pres, g->d_nest,
-                             g->d_counter, g->d_snap, SNAP_STRIDE, q);
+                             g->d_counter, g->d_snap, snap_stride(c), q);
             return launched(c, __LINE__);
         },
         [&](cudaStream_t q, cudaGraphConditionalHandle h) {
             // ghost fill folded into the pass (face snapshot of the previous pass)
             launch_relax_dev(c->geom, c->bt, c->st, g->L, l, 1, ratio, h, g->d_ctl, c->d_pres, g->d_nest,
-                             g->d_counter, g->d_snap, SNAP_STRIDE, q);
+                             g->d_counter, g->d_snap, snap_stride(c), q);
             return launched(c, __LINE__);
         });
 }
@@ -297,8 +301,8 @@ int rec_persistent(amr_ctx* c, cudaStream_t s, double tol) {
     a.pres = g->d_pres3;
     a.nest = g->d_pnest;
     a.snap = g->d_snap;
-    a.stride = SNAP_STRIDE;
-    a.snap_half = SNAP_STRIDE * (size_t)c->cap;
+    a.stride = snap_stride(c);
+    a.snap_half = snap_stride(c) * (size_t)c->cap;
     a.bar = g->d_bar;
     CUDA_TRY(cudaMemsetAsync(g->d_bar, 0, sizeof(GridBarrier), s));
     // event nodes bracketing the launch: the elapsed time of the latest
@@ -475,8 +479,8 @@ int need(amr_ctx* c) {
         c->err = "graph solve needs a self-gravitating context";
         return AMR_ERR_ARG;
     }
-    if (c->geom.nx != 8) {
-        c->err = "graph step built for nx == 8";
+    if (c->geom.nx != 8 && c->geom.nx != 12) {
+        c->err = "graph step built for nx == 8 or 12";
         return AMR_ERR_ARG;
     }
     TRY(amr_poisson_set_source(c));  // allocates the Poisson scratch on first use
@@ -555,11 +559,13 @@ int amr_solve_totals(amr_ctx* c, double* ms, long long* count) {
     return AMR_OK;
 }
 
-// Polls per bounded wait of the persistent solve before it aborts with
-// AMR_ERR_TIMEOUT; 0 restores the default (2^22).
+// Polls per bounded wait of the persistent solve and of the fused substep
+// before they give up with AMR_ERR_TIMEOUT; 0 restores the defaults (2^22
+// and 2^24).
 int amr_set_wait_limit(amr_ctx* c, int polls) {
     if (!c || polls < 0) return AMR_ERR_ARG;
     c->wait_limit = polls > 0 ? polls : (1 << 22);
+    c->fused_wait_limit = polls > 0 ? polls : (1 << 24);
     return AMR_OK;
 }
 

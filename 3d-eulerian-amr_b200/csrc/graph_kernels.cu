@@ -12,17 +12,29 @@
 
 namespace amr {
 
+// Byte offset of the level-sum buffers in k_relax_dev's dynamic shared
+// memory, and the whole size.
+template <int NX, typename CT>
+__host__ __device__ constexpr size_t relax_dev_nbuf_offset() {
+    return (sizeof(RelaxSmem<NX, CT>) + 15) / 16 * 16;
+}
+template <int NX, typename CT>
+__host__ __device__ constexpr size_t relax_dev_smem() {
+    return relax_dev_nbuf_offset<NX, CT>() + 2 * NEST_SMEM * sizeof(double);
+}
+
 // Relaxation pass of one level whose last block reduces the per-brick sums
 // as the recursion does and decides the relaxation loop of vcycle0
 // (poisson.cpp:66-70, 74-78): mode 0 records resid0 and opens the loop,
 // mode 1 continues it while resid / resid0 > ratio.
 template <int NX, typename CT>
-__global__ void __launch_bounds__(NX* NX* NX)
+__global__ void __launch_bounds__(RelaxThreads<NX>::value)
     k_relax_dev(Geom g, BrickTable bt, DevState st, LevelLists L, int level, int mode, double ratio,
                 cudaGraphConditionalHandle cond, Control* ctl, double* pres, double* nest, unsigned int* counter,
                 CT* snap, size_t stride, size_t snap_half) {
-    __shared__ RelaxSmem<NX, CT> sm;
-    __shared__ double nbuf[2 * NEST_SMEM];
+    // dynamic shared memory: the staged brick, then the level-sum buffers
+    RelaxSmem<NX, CT>& sm = *reinterpret_cast<RelaxSmem<NX, CT>*>(dyn_smem());
+    double* nbuf = reinterpret_cast<double*>(dyn_smem() + relax_dev_nbuf_offset<NX, CT>());
     __shared__ bool last;
     const int b = L.slots[L.off[level] + blockIdx.x];
     const int t = threadIdx.x;
@@ -30,7 +42,8 @@ __global__ void __launch_bounds__(NX* NX* NX)
     const int par = mode == 0 ? 0 : ctl->snap_par[level];
     const CT* snap_rd = snap + (size_t)par * snap_half;
     CT* snap_wr = snap + (size_t)(mode == 0 ? 0 : par ^ 1) * snap_half;
-    op_relax_pass<NX, CT>(g, bt, st, b, mode, snap_rd, snap_wr, stride, pres, sm);
+    op_relax_pass<NX, RelaxThreads<NX>::value, CT>(g, bt, st, b, mode, snap_rd, snap_wr, stride, pres, sm, t,
+                                                   BlockSync{});
     // last block: reduce and decide
     __threadfence();
     __syncthreads();
@@ -180,12 +193,36 @@ void launch_relax_dev(const Geom& g, const BrickTable& bt, const DevState& st, c
     if (n <= 0) return;
     // two buffers, each one stride per brick slot of the pool (FP32 entries
     // in the mixed form, in the same allocation)
-    if (g.precision == AMR_PREC_MIXED)
-        launch_k(k_relax_dev<8, float>, n, 512, 0, s, g, bt, st, L, level, mode, ratio, cond, ctl, pres, nest, counter,
-                 reinterpret_cast<float*>(snap), snap_stride, snap_stride * (size_t)L.cap);
-    else
-        launch_k(k_relax_dev<8, double>, n, 512, 0, s, g, bt, st, L, level, mode, ratio, cond, ctl, pres, nest,
-                 counter, snap, snap_stride, snap_stride * (size_t)L.cap);
+    float* snap32 = reinterpret_cast<float*>(snap);
+    const size_t half = snap_stride * (size_t)L.cap;
+    const bool f32 = g.precision == AMR_PREC_MIXED;
+    if (g.nx == 12) {
+        if (f32)
+            launch_k(k_relax_dev<12, float>, n, RelaxThreads<12>::value, relax_dev_smem<12, float>(), s, g, bt, st, L,
+                     level, mode, ratio, cond, ctl, pres, nest, counter, snap32, snap_stride, half);
+        else
+            launch_k(k_relax_dev<12, double>, n, RelaxThreads<12>::value, relax_dev_smem<12, double>(), s, g, bt, st,
+                     L, level, mode, ratio, cond, ctl, pres, nest, counter, snap, snap_stride, half);
+    } else {
+        if (f32)
+            launch_k(k_relax_dev<8, float>, n, RelaxThreads<8>::value, relax_dev_smem<8, float>(), s, g, bt, st, L,
+                     level, mode, ratio, cond, ctl, pres, nest, counter, snap32, snap_stride, half);
+        else
+            launch_k(k_relax_dev<8, double>, n, RelaxThreads<8>::value, relax_dev_smem<8, double>(), s, g, bt, st, L,
+                     level, mode, ratio, cond, ctl, pres, nest, counter, snap, snap_stride, half);
+    }
+}
+
+int relax_dev_attributes() {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* f, size_t bytes) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    };
+    set((const void*)k_relax_dev<8, float>, relax_dev_smem<8, float>());
+    set((const void*)k_relax_dev<8, double>, relax_dev_smem<8, double>());
+    set((const void*)k_relax_dev<12, float>, relax_dev_smem<12, float>());
+    set((const void*)k_relax_dev<12, double>, relax_dev_smem<12, double>());
+    return e == cudaSuccess ? 0 : -1;
 }
 
 void launch_error_dev(const Geom& g, const BrickTable& bt, const DevState& st, const LevelLists& L, int nlevels,

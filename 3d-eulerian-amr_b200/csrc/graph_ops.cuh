@@ -104,67 +104,13 @@ __device__ __forceinline__ CT ghost_dphi(const Geom& g, const BrickTable& bt, co
     return D[(size_t)nbr * P * P * P + (r2 * P + r1) * P + r0];
 }
 
-// One relaxation pass of brick b (block = NX^3 threads): mode 1 fills the
-// ghost faces from the snapshot snap_rd first; the relaxed interior goes to
-// dphi, its first interior layers to snap_wr, the last sweep's sum to
-// pres[b].  Called by every thread of the block.
-template <int NX, typename CT>
-__device__ __forceinline__ void op_relax_pass(const Geom& g, const BrickTable& bt, const DevState& st, int b,
-                                              int mode, const CT* snap_rd, CT* snap_wr, size_t stride,
-                                              double* pres, RelaxSmem<NX, CT>& sm) {
-    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX;
-    CT* D = Corr<CT>::dphi(st);
-    const size_t base = (size_t)b * P3;
-    const int t = threadIdx.x;
-    if (mode == 1 && t < 6 * F) {
-        const int face = t / F, qq = t % F;
-        const int t1 = qq % NX + 1, t2 = qq / NX + 1;
-        const CT gv = ghost_dphi<NX, CT>(g, bt, st, snap_rd, stride, b, face, t1, t2);
-        const int ax = face >> 1;
-        int d[3];
-        d[ax] = (face & 1) ? P - 1 : 0;
-        d[ax == 0 ? 1 : 0] = t1;
-        d[ax == 2 ? 1 : 2] = t2;
-        D[base + (d[2] * P + d[1]) * P + d[0]] = gv;
-    }
-    if (mode == 1) __syncthreads();
-    const int c = ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
-    const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
-    CT v;
-    const double resid = relax_brick<NX, CT>(sm, D + base, Corr<CT>::dphi1(st) + base, &v);
-    D[base + c] = v;
-    // publish first interior layers: layer of face f holds the cells adjacent to it
-    CT* sw = snap_wr + (size_t)b * stride;
-    if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = v;
-    if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = v;
-    if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = v;
-    if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = v;
-    if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = v;
-    if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v;
-    if (t == 0) pres[b] = resid;
-}
-
-// op_relax_pass in mode 1 split in two, so that a pass can be computed
-// before the loop has decided whether it runs.  op_relax_spec computes it
-// from the current dphi and the snapshot snap_rd with nothing written to
-// global memory (the ghost faces go to the staged brick only, where the
-// sweeps leave them); op_relax_commit then writes what op_relax_pass
-// writes: the ghost faces and the relaxed interior to dphi, the first
-// interior layers to snap_wr, the sum to pres[b].  Same values as
-// op_relax_pass; called by every thread, with the brick's shared memory
-// untouched in between.
-template <typename CT>
-struct RelaxSpec {
-    CT v;          // this thread's relaxed interior cell
-    double resid;  // the brick's last sweep sum
-};
-
-// ghost-face cell t (< 6 NX^2) of the (NX+2)^3 brick, and its face coordinates
+// Ghost face cell q (< 6 NX^2) of the (NX+2)^3 brick, and its face
+// coordinates.
 template <int NX>
-__device__ __forceinline__ int relax_ghost_cell(int t, int& face, int& t1, int& t2) {
+__device__ __forceinline__ int relax_ghost_cell(int q, int& face, int& t1, int& t2) {
     constexpr int P = NX + 2, F = NX * NX;
-    face = t / F;
-    const int qq = t % F;
+    face = q / F;
+    const int qq = q % F;
     t1 = qq % NX + 1;
     t2 = qq / NX + 1;
     const int ax = face >> 1;
@@ -175,103 +121,116 @@ __device__ __forceinline__ int relax_ghost_cell(int t, int& face, int& t1, int& 
     return (d[2] * P + d[1]) * P + d[0];
 }
 
+// Writes a relaxed interior value of cell t (interior index) to dphi and,
+// where the cell lies on a face, to that face's first-interior layer of the
+// snapshot (layer of face f holds the cells adjacent to it).
 template <int NX, typename CT>
-__device__ __forceinline__ RelaxSpec<CT> op_relax_spec(const Geom& g, const BrickTable& bt, const DevState& st,
-                                                       int b, const CT* snap_rd, size_t stride,
-                                                       RelaxSmem<NX, CT>& sm) {
-    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX, NT = NX * NX * NX;
-    const CT* D = Corr<CT>::dphi(st) + (size_t)b * P3;
-    const int t = threadIdx.x;
-    CT gv = CT(0);
-    int gi = -1;
-    if (t < 6 * F) {
-        int face, t1, t2;
-        gi = relax_ghost_cell<NX>(t, face, t1, t2);
-        gv = ghost_dphi<NX, CT>(g, bt, st, snap_rd, stride, b, face, t1, t2);
-    }
-    for (int q = t; q < P3; q += NT) {
-        const CT v = D[q];
-        sm.buf[0][q] = v;
-        sm.buf[1][q] = v;
-    }
-    const int c = relax_cell<NX>(t);
-    const CT d1 = (Corr<CT>::dphi1(st) + (size_t)b * P3)[c];
-    __syncthreads();
-    if (gi >= 0) {
-        sm.buf[0][gi] = gv;
-        sm.buf[1][gi] = gv;
-    }
-    __syncthreads();
-    RelaxSpec<CT> r;
-    r.resid = relax_sweeps<NX, CT>(sm, c, d1, &r.v);
-    return r;
-}
-
-template <int NX, typename CT>
-__device__ __forceinline__ void op_relax_commit(const DevState& st, int b, const RelaxSpec<CT>& r,
-                                                const RelaxSmem<NX, CT>& sm, CT* snap_wr, size_t stride,
-                                                double* pres) {
-    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX;
-    CT* D = Corr<CT>::dphi(st) + (size_t)b * P3;
-    const int t = threadIdx.x;
+__device__ __forceinline__ void relax_put(CT* D, CT* sw, int t, CT v) {
+    constexpr int P = NX + 2;
     const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
-    if (t < 6 * F) {
-        int face, t1, t2;
-        const int gi = relax_ghost_cell<NX>(t, face, t1, t2);
-        D[gi] = sm.buf[0][gi];
-    }
-    D[relax_cell<NX>(t)] = r.v;
-    CT* sw = snap_wr + (size_t)b * stride;
-    if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = r.v;
-    if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = r.v;
-    if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = r.v;
-    if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = r.v;
-    if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = r.v;
-    if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = r.v;
-    if (t == 0) pres[b] = r.resid;
+    D[(ck * P + cj) * P + ci] = v;
+    if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = v;
+    if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = v;
+    if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = v;
+    if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = v;
+    if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = v;
+    if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v;
 }
 
-// op_relax_pass for half a block (NX^3/2 threads, local index lt, barrier
-// `bar`): the same pass with two cells per thread (relax_brick_half), so
-// that one block relaxes two bricks at once.
-template <int NX, typename CT>
-__device__ __forceinline__ void op_relax_pass_half(const Geom& g, const BrickTable& bt, const DevState& st, int b,
-                                                   int mode, const CT* snap_rd, CT* snap_wr, size_t stride,
-                                                   double* pres, RelaxSmem<NX, CT>& sm, int lt, int bar) {
-    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX, HT = NX * NX * NX / 2;
-    CT* D = Corr<CT>::dphi(st);
-    const size_t base = (size_t)b * P3;
+// One relaxation pass of brick b by TH threads (local index lt, barrier
+// `sync`): mode 1 fills the ghost faces from the snapshot snap_rd first; the
+// relaxed interior goes to dphi, its first interior layers to snap_wr, the
+// last sweep's sum to pres[b].  Called by every one of the TH threads.
+template <int NX, int TH, typename CT, typename Sync>
+__device__ __forceinline__ void op_relax_pass(const Geom& g, const BrickTable& bt, const DevState& st, int b,
+                                              int mode, const CT* snap_rd, CT* snap_wr, size_t stride,
+                                              double* pres, RelaxSmem<NX, CT>& sm, int lt, Sync sync) {
+    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX, K = NX * NX * NX / TH;
+    CT* D = Corr<CT>::dphi(st) + (size_t)b * P3;
     if (mode == 1) {
-        for (int q = lt; q < 6 * F; q += HT) {
-            const int face = q / F, qq = q % F;
-            const int t1 = qq % NX + 1, t2 = qq / NX + 1;
-            const CT gv = ghost_dphi<NX, CT>(g, bt, st, snap_rd, stride, b, face, t1, t2);
-            const int ax = face >> 1;
-            int d[3];
-            d[ax] = (face & 1) ? P - 1 : 0;
-            d[ax == 0 ? 1 : 0] = t1;
-            d[ax == 2 ? 1 : 2] = t2;
-            D[base + (d[2] * P + d[1]) * P + d[0]] = gv;
+        for (int q = lt; q < 6 * F; q += TH) {
+            int face, t1, t2;
+            const int gi = relax_ghost_cell<NX>(q, face, t1, t2);
+            D[gi] = ghost_dphi<NX, CT>(g, bt, st, snap_rd, stride, b, face, t1, t2);
         }
-        named_sync(bar, HT);
+        sync();
     }
-    CT v[2];
-    const double resid = relax_brick_half<NX, CT>(sm, D + base, Corr<CT>::dphi1(st) + base, v, lt, bar);
+    int c[K];
+    CT v[K];
+    const double resid = relax_brick<NX, TH, CT>(sm, D, Corr<CT>::dphi1(st) + (size_t)b * P3, lt, c, v, sync);
     CT* sw = snap_wr + (size_t)b * stride;
 #pragma unroll
-    for (int h = 0; h < 2; h++) {
-        const int t = lt + h * HT;
-        const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
-        const int c = (ck * P + cj) * P + ci;
-        D[base + c] = v[h];
-        if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = v[h];
-        if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = v[h];
-        if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = v[h];
-        if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = v[h];
-        if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = v[h];
-        if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v[h];
-    }
+    for (int r = 0; r < K; r++) relax_put<NX, CT>(D, sw, lt + r * TH, v[r]);
     if (lt == 0) pres[b] = resid;
+}
+
+// op_relax_pass in mode 1 split in two, so that a pass can be computed
+// before the loop has decided whether it runs.  op_relax_spec computes it
+// from the current dphi and the snapshot snap_rd with nothing written to
+// global memory (the ghost faces go to the staged brick only, where the
+// sweeps leave them); op_relax_commit then writes what op_relax_pass
+// writes: the ghost faces and the relaxed interior to dphi, the first
+// interior layers to snap_wr, the sum to pres[b].  Same values as
+// op_relax_pass; called by every thread of a block of TH threads, with the
+// brick's shared memory untouched in between.
+template <typename CT, int K>
+struct RelaxSpec {
+    CT v[K];       // this thread's relaxed interior cells
+    double resid;  // the brick's last sweep sum
+};
+
+template <int NX, int TH, typename CT>
+__device__ __forceinline__ RelaxSpec<CT, NX * NX * NX / TH> op_relax_spec(const Geom& g, const BrickTable& bt,
+                                                                        const DevState& st, int b, const CT* snap_rd,
+                                                                        size_t stride, RelaxSmem<NX, CT>& sm) {
+    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX, K = NX * NX * NX / TH, G = (6 * F + TH - 1) / TH;
+    const CT* D = Corr<CT>::dphi(st) + (size_t)b * P3;
+    const int lt = threadIdx.x;
+    CT gv[G];
+    int gi[G];
+#pragma unroll
+    for (int r = 0; r < G; r++) {
+        const int q = lt + r * TH;
+        gi[r] = -1;
+        if (q < 6 * F) {
+            int face, t1, t2;
+            gi[r] = relax_ghost_cell<NX>(q, face, t1, t2);
+            gv[r] = ghost_dphi<NX, CT>(g, bt, st, snap_rd, stride, b, face, t1, t2);
+        }
+    }
+    relax_stage<NX, TH, CT>(sm, D, lt);
+    int c[K];
+    CT d1[K];
+    relax_cells<NX, TH, CT>(lt, Corr<CT>::dphi1(st) + (size_t)b * P3, c, d1);
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < G; r++)
+        if (gi[r] >= 0) {
+            sm.buf[0][gi[r]] = gv[r];
+            sm.buf[1][gi[r]] = gv[r];
+        }
+    __syncthreads();
+    RelaxSpec<CT, K> out;
+    out.resid = relax_sweeps<NX, TH, CT>(sm, lt, c, d1, out.v, BlockSync{});
+    return out;
+}
+
+template <int NX, int TH, typename CT>
+__device__ __forceinline__ void op_relax_commit(const DevState& st, int b, const RelaxSpec<CT, NX * NX * NX / TH>& r,
+                                                const RelaxSmem<NX, CT>& sm, CT* snap_wr, size_t stride,
+                                                double* pres) {
+    constexpr int P = NX + 2, P3 = P * P * P, F = NX * NX, K = NX * NX * NX / TH;
+    CT* D = Corr<CT>::dphi(st) + (size_t)b * P3;
+    const int lt = threadIdx.x;
+    for (int q = lt; q < 6 * F; q += TH) {
+        int face, t1, t2;
+        const int gi = relax_ghost_cell<NX>(q, face, t1, t2);
+        D[gi] = sm.buf[0][gi];
+    }
+    CT* sw = snap_wr + (size_t)b * stride;
+#pragma unroll
+    for (int q = 0; q < K; q++) relax_put<NX, CT>(D, sw, lt + q * TH, r.v[q]);
+    if (lt == 0) pres[b] = r.resid;
 }
 
 }  // namespace amr

@@ -27,7 +27,6 @@
 
 namespace amr {
 
-constexpr unsigned long long FUSED_WAIT_SPINS = 1ull << 24;
 
 // Six conserved fields of one cell, indexed only by compile-time constants
 // (stays in registers).
@@ -131,7 +130,7 @@ __device__ __forceinline__ void fused_cell(const FusedArgs& A, int b, int x, int
 __device__ __forceinline__ void fused_wait(const FusedArgs& A, int child) {
     unsigned long long spins = 0;
     while (*(volatile const int*)(A.done + child) != A.epoch) {
-        if (++spins > FUSED_WAIT_SPINS) {
+        if (++spins > A.wait_limit) {
             atomicOr(A.err, 1);
             break;
         }

@@ -28,6 +28,7 @@ struct FusedArgs {
     double* Fy;
     double* Fz;
     int* err;  // bit 0: a wait for a child ran out; bit 1: ghost chain too deep
+    unsigned long long wait_limit;  // polls of one wait for a child's faces before bit 0 is set
 };
 
 // Launch over a.nwork bricks; blocks_per_sm_cap > 0 limits the resident

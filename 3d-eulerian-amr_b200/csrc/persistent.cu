@@ -40,7 +40,16 @@ __device__ __forceinline__ unsigned ld_volatile(const unsigned* p) { return *(co
 // The arrival counter only grows: barrier k of the launch completes when it
 // reaches k * gridDim.x (target, kept by thread 0), so an arrival is one
 // fire-and-forget release add and the wait one acquire load per poll.
-__device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned& target, unsigned long long limit) {
+// A block whose wait runs out sets the abort word and records status 3
+// (AMR_ERR_TIMEOUT) in the control block itself, so the timeout is reported
+// whichever block meets it and whatever the other solves of a captured step
+// record after it (statuses only grow).
+__device__ __forceinline__ void give_up(GridBarrier* bar, int* status) {
+    atomicExch(&bar->abort, 1);
+    atomicMax(status, 3);
+}
+
+__device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned& target, unsigned long long limit, int* status) {
     __shared__ int ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -59,7 +68,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* bar, unsigned& target, un
                 break;
             }
             if (++spins > limit) {
-                atomicExch(&bar->abort, 1);
+                give_up(bar, status);
                 good = 0;
                 break;
             }
@@ -82,7 +91,8 @@ __device__ __forceinline__ void lsum_publish(GridBarrier* bar, unsigned g, doubl
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&bar->lsum_gen), "r"(g) : "memory");
 }
 
-__device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& r, unsigned long long limit) {
+__device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& r, unsigned long long limit,
+                                          int* status) {
     __shared__ double s_r;
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
@@ -97,7 +107,7 @@ __device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& 
                 break;
             }
             if (++spins > limit) {
-                atomicExch(&bar->abort, 1);
+                give_up(bar, status);
                 good = 0;
                 break;
             }
@@ -111,10 +121,25 @@ __device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& 
     return s_ok != 0;
 }
 
-template <typename CT>
+// Block layout of the solve for bricks of NX^3 interior cells: TPB threads
+// (the relaxation layout of one brick per block); with 8^3 bricks a block
+// relaxes two bricks at once (one per half) on levels with more bricks
+// than blocks, so it holds two staged bricks.
+template <int NX>
+struct SolveLayout {
+    static constexpr int TPB = RelaxThreads<NX>::value;
+    static constexpr bool HALVES = NX == 8;
+    static constexpr int NSM = HALVES ? 2 : 1;
+    // threads per face in the face-ghost phases
+    static constexpr int PF = NX * NX <= TPB / 6 ? NX * NX : TPB / 6;
+};
+
+template <int NX, typename CT>
 struct Solver {
+    using Lay = SolveLayout<NX>;
+    static constexpr int TPB = Lay::TPB;
     const SolveArgs& a;
-    RelaxSmem<8, CT>* sm;  // two: one per half block
+    RelaxSmem<NX, CT>* sm;  // Lay::NSM staged bricks
     double* red;
     double* nbuf;    // 2 * NEST_SMEM doubles of shared memory for the level sums
     double* nest;    // this block's scratch [cap] (level sums of larger trees)
@@ -142,7 +167,7 @@ struct Solver {
     // barrier closing a phase of class ph
     __device__ bool sync(int ph, int units) {
         const unsigned long long t_arrive = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
-        const bool ok = grid_sync(a.bar, bar_target, spin_limit);
+        const bool ok = grid_sync(a.bar, bar_target, spin_limit, &a.ctl->status);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             const unsigned long long t = now();
             ph_wait[ph] += t - t_arrive;
@@ -158,7 +183,7 @@ struct Solver {
     // of a phase: the arrays the phase must read and write once, at their
     // storage width (the correction dphi, dphi1 in CT).
     __device__ static double phase_bytes(int ph) {
-        constexpr double NX = 8, PNX = 10, H = NX / 2, C = sizeof(CT);
+        constexpr double PNX = NX + 2, H = NX / 2, C = sizeof(CT);
         switch (ph) {
             case PH_SOURCE: return 16 * PNX * PNX * PNX;                                  // rho -> S
             case PH_RESTRICT: return 8 * (8 * PNX * PNX * PNX + 8 * H * H * H);           // 8 children -> parent
@@ -186,19 +211,23 @@ struct Solver {
     }
 
     // one relaxation pass over the n bricks sl[]: one brick per block, or
-    // two per block (one per half, two cells per thread) when the level has
-    // more bricks than there are blocks; the results are the same either way
+    // (8^3 bricks) two per block, one per half with two cells per thread,
+    // when the level has more bricks than there are blocks; the results are
+    // the same either way
     __device__ void relax_pass(const int* sl, int n, int mode, const CT* rd, CT* wr, double* pres) {
-        if (n <= (int)gridDim.x) {
+        if (!Lay::HALVES || n <= (int)gridDim.x) {
             each(n, [&](int q) {
-                op_relax_pass<8, CT>(a.g, a.bt, a.st, sl[q], mode, rd, wr, a.stride, pres, sm[0]);
+                op_relax_pass<NX, TPB, CT>(a.g, a.bt, a.st, sl[q], mode, rd, wr, a.stride, pres, sm[0], threadIdx.x,
+                                           BlockSync{});
                 __syncthreads();
             });
         } else {
-            const int h = threadIdx.x >> 8, lt = threadIdx.x & 255;
+            constexpr int HT = TPB / 2;
+            const int h = threadIdx.x / HT, lt = threadIdx.x % HT;
             for (int q = 2 * blockIdx.x + h; q < n; q += 2 * gridDim.x) {
-                op_relax_pass_half<8, CT>(a.g, a.bt, a.st, sl[q], mode, rd, wr, a.stride, pres, sm[h], lt, 1 + h);
-                named_sync(1 + h, 256);
+                op_relax_pass<NX, HT, CT>(a.g, a.bt, a.st, sl[q], mode, rd, wr, a.stride, pres, sm[h & 1], lt,
+                                          NamedSync{1 + h, HT});
+                named_sync(1 + h, HT);
             }
         }
     }
@@ -211,8 +240,9 @@ struct Solver {
         const int* sl = level(l);
         const int n = a.L.cnt[l];
         const int t = threadIdx.x;
+        constexpr int PF = Lay::PF;
         each(n, [&](int q) {
-            if (t < 384) op_phi_faces(a.g, a.bt, a.st, a.aux, sl[q], t / 64, t % 64, 64);
+            if (t < 6 * PF) op_phi_faces(a.g, a.bt, a.st, a.aux, sl[q], t / PF, t % PF, PF);
         });
         if (!sync(PH_PHI_FACES, n)) return false;
         const int m = a.g.pnx - 2;
@@ -256,7 +286,7 @@ struct Solver {
     // time it waits for it)
     __device__ bool wait_sum(double& r) {
         const unsigned long long t0 = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
-        const bool ok = lsum_wait(a.bar, lsum_gen, r, spin_limit);
+        const bool ok = lsum_wait(a.bar, lsum_gen, r, spin_limit, &a.ctl->status);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             ph_wait[PH_COUNT] += now() - t0;
             ph_wait[PH_COUNT + 1]++;
@@ -272,8 +302,9 @@ struct Solver {
         const int n = a.L.cnt[l];
         const int t = threadIdx.x;
         CT* snap = reinterpret_cast<CT*>(a.snap);
+        constexpr int PF = Lay::PF;
         each(n, [&](int q) {
-            if (t < 384) op_dphi_faces<CT>(a.g, a.bt, a.st, a.aux, sl[q], t / 64, t % 64, 64);
+            if (t < 6 * PF) op_dphi_faces<CT>(a.g, a.bt, a.st, a.aux, sl[q], t / PF, t % PF, PF);
         });
         if (!sync(PH_DPHI_FACES, n)) return false;
         if (n < (int)gridDim.x) return relax_loop_overlapped(l, ratio, sl, n, snap);
@@ -321,7 +352,9 @@ struct Solver {
         const bool server = blockIdx.x == gridDim.x - 1;
         const int b = mine ? sl[blockIdx.x] : -1;
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
-        if (mine) op_relax_pass<8, CT>(a.g, a.bt, a.st, b, 0, snap, snap, a.stride, pres, sm[0]);
+        if (mine)
+            op_relax_pass<NX, TPB, CT>(a.g, a.bt, a.st, b, 0, snap, snap, a.stride, pres, sm[0], threadIdx.x,
+                                       BlockSync{});
         if (!sync(PH_RELAX_FIRST, n)) return false;
         count_pass(l);
         // pass 1 runs whatever the first sum; that sum is formed meanwhile
@@ -335,7 +368,9 @@ struct Solver {
                 const double r = level_sum(l, done);
                 if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
             }
-            if (mine) op_relax_pass<8, CT>(a.g, a.bt, a.st, b, 1, snap, snap + a.snap_half, a.stride, pres, sm[0]);
+            if (mine)
+                op_relax_pass<NX, TPB, CT>(a.g, a.bt, a.st, b, 1, snap, snap + a.snap_half, a.stride, pres, sm[0],
+                                           threadIdx.x, BlockSync{});
             if (!wait_sum(r0)) return false;
             if (!sync(PH_RELAX, n)) return false;
             count_pass(l);
@@ -351,8 +386,9 @@ struct Solver {
                 const double r = level_sum(l, done);
                 if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
             }
-            RelaxSpec<CT> sp;
-            if (mine) sp = op_relax_spec<8, CT>(a.g, a.bt, a.st, b, snap + (size_t)par * a.snap_half, a.stride, sm[0]);
+            RelaxSpec<CT, NX * NX * NX / TPB> sp;
+            if (mine)
+                sp = op_relax_spec<NX, TPB, CT>(a.g, a.bt, a.st, b, snap + (size_t)par * a.snap_half, a.stride, sm[0]);
             double r;
             if (!wait_sum(r)) return false;
             bool again = r / r0 > ratio;
@@ -362,7 +398,8 @@ struct Solver {
             }
             if (!again) break;
             if (mine)
-                op_relax_commit<8, CT>(a.st, b, sp, sm[0], snap + (size_t)(par ^ 1) * a.snap_half, a.stride, pres);
+                op_relax_commit<NX, TPB, CT>(a.st, b, sp, sm[0], snap + (size_t)(par ^ 1) * a.snap_half, a.stride,
+                                             pres);
             if (!sync(PH_RELAX, n)) return false;
             par ^= 1;
             count_pass(l);
@@ -381,7 +418,10 @@ struct Solver {
         if (!sync(PH_SOURCE, a.L.nall)) return false;
         for (int l = maxl - 1; l >= 0; l--) {
             const int* pl = a.parents + a.poff[l];
-            each(a.pcnt[l], [&](int q) { op_phi_from_children(a.g, a.bt, a.st, pl[q], t / 64, t % 64); });
+            constexpr int H3 = (NX / 2) * (NX / 2) * (NX / 2);
+            each(a.pcnt[l], [&](int q) {
+                for (int u = t; u < 8 * H3; u += TPB) op_phi_from_children(a.g, a.bt, a.st, pl[q], u / H3, u % H3);
+            });
             if (!sync(PH_RESTRICT, a.pcnt[l])) return false;
         }
         for (int l = 0; l <= maxl; l++)
@@ -452,16 +492,17 @@ struct Solver {
     }
 };
 
-template <typename CT>
-__global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
-    __shared__ RelaxSmem<8, CT> sm[2];
+template <int NX, typename CT>
+__global__ void __launch_bounds__(SolveLayout<NX>::TPB, 2) k_solve_persistent(SolveArgs a) {
+    // the staged bricks live in dynamic shared memory
+    RelaxSmem<NX, CT>* sm = reinterpret_cast<RelaxSmem<NX, CT>*>(dyn_smem());
     __shared__ double red[16];
     __shared__ double nbuf[2 * NEST_SMEM];
     __shared__ double s_err;
     // loop limits are read from the control block (set by the host before
     // every launch; a captured graph keeps its arguments)
     const int max_cycles = *(volatile int*)&a.ctl->max_cycles;
-    Solver<CT> s{a, sm, red, nbuf, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0,
+    Solver<NX, CT> s{a, sm, red, nbuf, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0,
                  *(volatile int*)&a.ctl->max_outer};
     __shared__ unsigned long long s_ph_ns[PH_COUNT];
     __shared__ unsigned s_ph_n[PH_COUNT];
@@ -479,7 +520,7 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
     s.ph_bytes = s_ph_bytes;
     s.ph_wait = s_ph_wait;
     if (threadIdx.x < PH_COUNT + 2) s_ph_wait[threadIdx.x] = 0;
-    s.t_last = Solver<CT>::now();
+    s.t_last = Solver<NX, CT>::now();
     if (threadIdx.x < PH_COUNT) {
         s_ph_ns[threadIdx.x] = 0;
         s_ph_n[threadIdx.x] = 0;
@@ -506,13 +547,13 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         Control* c = a.ctl;
         if (!ok) {
-            c->status = 3;
+            atomicMax(&c->status, 3);
         } else {
             c->err = err;
             c->cycles = cycles;
             c->cycles_total += cycles;
             c->relax_calls += s.relax_calls;
-            if (s.status) c->status = s.status;
+            if (s.status) atomicMax(&c->status, s.status);
             for (int p = 0; p < PH_COUNT; p++) {
                 c->phase_ns[p] += s.ph_ns[p];
                 c->phase_n[p] += s.ph_n[p];
@@ -528,26 +569,60 @@ __global__ void __launch_bounds__(512, 2) k_solve_persistent(SolveArgs a) {
 
 }  // namespace
 
-int solve_persistent_blocks(int precision, int per_sm_cap) {
-    int dev = 0, sms = 0, per = 0;
+template <int NX, typename CT>
+constexpr size_t solve_smem() {
+    return SolveLayout<NX>::NSM * sizeof(RelaxSmem<NX, CT>);
+}
+
+int solve_persistent_attributes() {
+    cudaError_t e = cudaSuccess;
+    auto set = [&](const void* f, size_t bytes) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    };
+    set((const void*)k_solve_persistent<8, float>, solve_smem<8, float>());
+    set((const void*)k_solve_persistent<8, double>, solve_smem<8, double>());
+    set((const void*)k_solve_persistent<12, float>, solve_smem<12, float>());
+    set((const void*)k_solve_persistent<12, double>, solve_smem<12, double>());
+    return e == cudaSuccess ? 0 : -1;
+}
+
+namespace {
+template <int NX, typename CT>
+int occupancy() {
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_persistent<NX, CT>, SolveLayout<NX>::TPB,
+                                                      solve_smem<NX, CT>()) != cudaSuccess)
+        return -1;
+    return per;
+}
+template <int NX, typename CT>
+cudaError_t launch(const SolveArgs& a, int blocks, cudaStream_t s) {
+    void* args[] = {const_cast<SolveArgs*>(&a)};
+    return cudaLaunchCooperativeKernel((const void*)k_solve_persistent<NX, CT>, dim3(blocks),
+                                       dim3(SolveLayout<NX>::TPB), args, solve_smem<NX, CT>(), s);
+}
+}  // namespace
+
+int solve_persistent_blocks(int nx, int precision, int per_sm_cap) {
+    int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-    const cudaError_t e =
-        precision == AMR_PREC_MIXED
-            ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_persistent<float>, 512, 0)
-            : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_persistent<double>, 512, 0);
-    if (e != cudaSuccess || per <= 0) return -1;
+    const bool f32 = precision == AMR_PREC_MIXED;
+    int per = -1;
+    if (nx == 8)
+        per = f32 ? occupancy<8, float>() : occupancy<8, double>();
+    else if (nx == 12)
+        per = f32 ? occupancy<12, float>() : occupancy<12, double>();
+    if (per <= 0) return -1;
     if (per_sm_cap > 0 && per_sm_cap < per) per = per_sm_cap;
     return sms * per;
 }
 
 cudaError_t launch_solve_persistent(const SolveArgs& a, int blocks, cudaStream_t s) {
     ++g_launch_tally;
-    void* args[] = {const_cast<SolveArgs*>(&a)};
-    if (a.g.precision == AMR_PREC_MIXED)
-        return cudaLaunchCooperativeKernel((const void*)k_solve_persistent<float>, dim3(blocks), dim3(512), args, 0,
-                                           s);
-    return cudaLaunchCooperativeKernel((const void*)k_solve_persistent<double>, dim3(blocks), dim3(512), args, 0, s);
+    const bool f32 = a.g.precision == AMR_PREC_MIXED;
+    if (a.g.nx == 12) return f32 ? launch<12, float>(a, blocks, s) : launch<12, double>(a, blocks, s);
+    return f32 ? launch<8, float>(a, blocks, s) : launch<8, double>(a, blocks, s);
 }
 
 }  // namespace amr

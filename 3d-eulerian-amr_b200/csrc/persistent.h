@@ -50,7 +50,10 @@ struct SolveArgs {
 
 // Blocks of one cooperative launch on the current device (all resident),
 // at most per_sm_cap per SM when per_sm_cap > 0.
-int solve_persistent_blocks(int precision, int per_sm_cap);
+int solve_persistent_blocks(int nx, int precision, int per_sm_cap);
+// raises the dynamic shared-memory limit of the solve kernels (call outside
+// stream capture)
+int solve_persistent_attributes();
 cudaError_t launch_solve_persistent(const SolveArgs& a, int blocks, cudaStream_t s);
 
 }  // namespace amr

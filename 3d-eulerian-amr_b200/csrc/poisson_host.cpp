@@ -120,7 +120,7 @@ int relax(amr_ctx* c, int l, double* resid) {
         bad = launch_relax(c->geom, c->st, lvl(c, l), nlvl(c, l), c->d_pres, c->stream);
     }
     if (bad) {
-        c->err = "relaxation kernel built for nx == 8 only";
+        c->err = "relaxation kernels built for nx == 8 or 12";
         return AMR_ERR_ARG;
     }
     TRY(check_launch(c));

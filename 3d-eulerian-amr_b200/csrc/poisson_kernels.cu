@@ -101,21 +101,23 @@ __global__ void k_phys_top(Geom g, BrickTable bt, const int* __restrict__ bfaces
 }
 // Poisson::vcycle_relax (poisson.cpp:88-130): Jacobi sweeps on one brick
 // with its ghost dphi frozen, until the sweep's sum of squared updates drops
-// below half the first sweep's or 16 sweeps.  Block = one brick, thread per
-// interior cell, dphi staged in shared memory.  out[e] = last sweep's sum.
+// below half the first sweep's or 16 sweeps.  Block = one brick
+// (RelaxThreads<NX> threads), dphi staged in dynamic shared memory.
+// out[e] = last sweep's sum.
 template <int NX, typename CT>
-__global__ void __launch_bounds__(NX* NX* NX) k_relax(Geom g, DevState st, const int* __restrict__ slots,
-                                                      double* __restrict__ out) {
-    constexpr int P = NX + 2, P3 = P * P * P;
-    __shared__ RelaxSmem<NX, CT> sm;
+__global__ void __launch_bounds__(RelaxThreads<NX>::value) k_relax(Geom g, DevState st, const int* __restrict__ slots,
+                                                                   double* __restrict__ out) {
+    constexpr int P = NX + 2, P3 = P * P * P, TH = RelaxThreads<NX>::value, K = NX * NX * NX / TH;
+    RelaxSmem<NX, CT>& sm = *reinterpret_cast<RelaxSmem<NX, CT>*>(dyn_smem());
     const int b = slots[blockIdx.x];
     const size_t base = (size_t)b * P3;
     const int t = threadIdx.x;
-    const int c = ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
     CT* D = Corr<CT>::dphi(st);
-    CT v;
-    const double resid = relax_brick<NX, CT>(sm, D + base, Corr<CT>::dphi1(st) + base, &v);
-    D[base + c] = v;
+    int c[K];
+    CT v[K];
+    const double resid = relax_brick<NX, TH, CT>(sm, D + base, Corr<CT>::dphi1(st) + base, t, c, v, BlockSync{});
+#pragma unroll
+    for (int r = 0; r < K; r++) D[base + c[r]] = v[r];
     if (t == 0) out[b] = resid;
 }
 // Poisson::store_phi / restore_phi / restore_half_phi (poisson.cpp:166-221).
@@ -307,11 +309,23 @@ void launch_vdown(const Geom& g, const BrickTable& bt, const DevState& st, const
 }
 int launch_relax(const Geom& g, const DevState& st, const int* slots, int n, double* out, cudaStream_t s) {
     if (n <= 0) return 0;
-    if (g.nx != 8) return -1;
-    if (g.precision == AMR_PREC_MIXED)
-        launch_k(k_relax<8, float>, n, 512, 0, s, g, st, slots, out);
-    else
-        launch_k(k_relax<8, double>, n, 512, 0, s, g, st, slots, out);
+    const bool f32 = g.precision == AMR_PREC_MIXED;
+    if (g.nx == 8) {
+        if (f32)
+            launch_k(k_relax<8, float>, n, RelaxThreads<8>::value, sizeof(RelaxSmem<8, float>), s, g, st, slots, out);
+        else
+            launch_k(k_relax<8, double>, n, RelaxThreads<8>::value, sizeof(RelaxSmem<8, double>), s, g, st, slots,
+                     out);
+    } else if (g.nx == 12) {
+        if (f32)
+            launch_k(k_relax<12, float>, n, RelaxThreads<12>::value, sizeof(RelaxSmem<12, float>), s, g, st, slots,
+                     out);
+        else
+            launch_k(k_relax<12, double>, n, RelaxThreads<12>::value, sizeof(RelaxSmem<12, double>), s, g, st, slots,
+                     out);
+    } else {
+        return -1;
+    }
     return 0;
 }
 void launch_coarse_correction(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,

@@ -1,13 +1,21 @@
 // Jacobi sweeps of Poisson::vcycle_relax (poisson.cpp:88-130) on one brick
-// staged in shared memory, one thread per interior cell.
+// staged in shared memory.
 //
 // Each sweep computes tmp0 = dphi1 + lap(dphi)/6 for every cell from the
 // previous sweep's values and adds it; the sweep's sum of tmp0^2 decides the
 // loop (ratio to the first sweep's > 0.5, at most 16 sweeps).  The two shared
-// buffers alternate so one block barrier per sweep suffices; every thread
-// adds the per-warp partial sums itself along the same fixed pairwise tree,
-// so all threads take the same loop decision.  (The reference adds the
-// squares sequentially; the sums differ in the last bits only.)
+// buffers alternate so one barrier per sweep suffices; every thread adds the
+// per-warp partial sums itself along the same fixed pairwise tree, so all
+// threads take the same loop decision.  (The reference adds the squares
+// sequentially; the sums differ in the last bits only.)
+//
+// Thread layout: TH threads (a multiple of 32 that divides NX^3) relax one
+// brick, K = NX^3 / TH cells each; thread lt owns interior cells
+// lt + r TH, r < K, counted x fastest.  Cell c's square enters the partial
+// of its 32-cell group c / 32 at lane c % 32 whatever TH is, so the warp
+// partials, their pairwise sum and every loop decision are the same bit for
+// bit for every layout: a whole block of 512 threads on an 8^3 brick, two
+// bricks of 256 threads each in one block, 576 threads on a 12^3 brick.
 #pragma once
 
 namespace amr {
@@ -19,130 +27,126 @@ struct RelaxSmem {
     double red[2][NW];
 };
 
-// The sweeps on a brick staged in both buffers (every cell, ghosts
-// included): thread t owns interior cell c with dphi1 value d1.  Returns the
-// last sweep's sum and leaves the relaxed value of cell c in *out.
-template <int NX, typename CT = double>
-__device__ __forceinline__ double relax_sweeps(RelaxSmem<NX, CT>& sm, int c, CT d1, CT* out) {
-    constexpr int P = RelaxSmem<NX, CT>::P, NW = RelaxSmem<NX, CT>::NW;
-    const int t = threadIdx.x;
-    double resid0 = 0.0, resid = 0.0;
-    int iters = 0, cur = 0;
-    do {
-        const CT* d = sm.buf[cur];
-        const CT div = (d[c + 1] + d[c - 1] + d[c + P] + d[c - P] + d[c + P * P] + d[c - P * P]) - (d[c] * CT(6.0));
-        const CT tmp0 = d1 + div * (CT(1.0) / CT(6.0));
-        sm.buf[cur ^ 1][c] = d[c] + tmp0;
-        double sq = double(tmp0) * double(tmp0);
-        for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-        if ((t & 31) == 0) sm.red[cur][t >> 5] = sq;
-        __syncthreads();
-        // pairwise sum of the warp partials (fixed tree, identical in every
-        // thread): log2(NW) dependent additions instead of NW
-        double r[NW];
-#pragma unroll
-        for (int w = 0; w < NW; w++) r[w] = sm.red[cur][w];
-#pragma unroll
-        for (int span = 1; span < NW; span <<= 1)
-#pragma unroll
-            for (int w = 0; w + span < NW; w += 2 * span) r[w] = r[w] + r[w + span];
-        resid = r[0];
-        if (iters == 0) resid0 = resid;
-        iters++;
-        cur ^= 1;
-    } while (resid / resid0 > 0.5 && iters < 16);
-    *out = sm.buf[cur][c];
-    return resid;
+// Threads of a whole block relaxing one brick of NX^3 interior cells.
+template <int NX>
+struct RelaxThreads;
+template <>
+struct RelaxThreads<8> {
+    static constexpr int value = 512;  // one cell per thread
+};
+template <>
+struct RelaxThreads<12> {
+    static constexpr int value = 576;  // three cells per thread
+};
+
+// Barrier over the threads that relax one brick.
+struct BlockSync {
+    __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+// Barrier over `n` threads with id `id` (1..15; 0 is __syncthreads).
+__device__ __forceinline__ void named_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+struct NamedSync {
+    int id, n;
+    __device__ __forceinline__ void operator()() const { named_sync(id, n); }
+};
+
+// Dynamic shared memory of a kernel (one declaration for every kernel).
+__device__ __forceinline__ unsigned char* dyn_smem() {
+    extern __shared__ __align__(16) unsigned char amr_dyn_smem[];
+    return amr_dyn_smem;
 }
 
-// Interior cell of thread t in the (NX+2)^3 brick.
+// Interior cell t of the (NX+2)^3 brick.
 template <int NX>
 __device__ __forceinline__ int relax_cell(int t) {
     constexpr int P = NX + 2;
     return ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
 }
 
-// Stages the brick (slot base) into both buffers;
-// returns the last sweep's sum and leaves the relaxed interior value of this
-// thread's cell in *out.  CT is the correction's storage and arithmetic type
-// (FP64, or FP32 in the mixed form); the sums of squares are formed in FP64
-// either way.
-template <int NX, typename CT = double>
-__device__ __forceinline__ double relax_brick(RelaxSmem<NX, CT>& sm, const CT* __restrict__ dphi,
-                                              const CT* __restrict__ dphi1, CT* out) {
-    constexpr int P3 = RelaxSmem<NX, CT>::P3, NT = RelaxSmem<NX, CT>::NT;
-    const int t = threadIdx.x;
-    for (int q = t; q < P3; q += NT) {
-        const CT v = dphi[q];
-        sm.buf[0][q] = v;
-        sm.buf[1][q] = v;
-    }
-    const int c = relax_cell<NX>(t);
-    const CT d1 = dphi1[c];
-    __syncthreads();
-    return relax_sweeps<NX, CT>(sm, c, d1, out);
-}
-
-// Barrier over `n` threads with id `id` (1..15; 0 is __syncthreads).
-__device__ __forceinline__ void named_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
-
-// relax_brick with half the threads: NX^3/2 threads (lt = 0 .. NX^3/2 - 1,
-// synchronised by barrier `bar`) each relax cells lt and lt + NX^3/2, so two
-// bricks share one block.  Cell c of warp lane l lies in the same 32-cell
-// warp group with the same lane as in relax_brick, so the warp partials, their
-// pairwise sum and every loop decision are bit for bit those of relax_brick.
-// out[0], out[1] receive the two cells' relaxed values.
-template <int NX, typename CT = double>
-__device__ __forceinline__ double relax_brick_half(RelaxSmem<NX, CT>& sm, const CT* __restrict__ dphi,
-                                                   const CT* __restrict__ dphi1, CT* out, int lt, int bar) {
-    constexpr int P = RelaxSmem<NX, CT>::P, P3 = RelaxSmem<NX, CT>::P3, NT = RelaxSmem<NX, CT>::NT,
-                  NW = RelaxSmem<NX, CT>::NW, HT = NT / 2;
-    for (int q = lt; q < P3; q += HT) {
-        const CT v = dphi[q];
-        sm.buf[0][q] = v;
-        sm.buf[1][q] = v;
-    }
-    int c[2];
-    CT d1[2];
-#pragma unroll
-    for (int h = 0; h < 2; h++) {
-        const int t = lt + h * HT;
-        const int i = t % NX + 1, j = (t / NX) % NX + 1, k = t / (NX * NX) + 1;
-        c[h] = (k * P + j) * P + i;
-        d1[h] = dphi1[c[h]];
-    }
-    named_sync(bar, HT);
+// The sweeps on a brick staged in both buffers (every cell, ghosts
+// included): thread lt owns the K cells c[r] with dphi1 values d1[r].
+// Returns the last sweep's sum and leaves the relaxed values in out[r].
+template <int NX, int TH, typename CT, typename Sync>
+__device__ __forceinline__ double relax_sweeps(RelaxSmem<NX, CT>& sm, int lt, const int* c, const CT* d1, CT* out,
+                                               Sync sync) {
+    constexpr int P = RelaxSmem<NX, CT>::P, NW = RelaxSmem<NX, CT>::NW, K = NX * NX * NX / TH, WT = TH / 32;
+    static_assert((NX * NX * NX) % TH == 0 && TH % 32 == 0, "relaxation layout");
     double resid0 = 0.0, resid = 0.0;
     int iters = 0, cur = 0;
     do {
         const CT* d = sm.buf[cur];
+        double sq[K];
 #pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const int cc = c[h];
-            const CT div =
-                (d[cc + 1] + d[cc - 1] + d[cc + P] + d[cc - P] + d[cc + P * P] + d[cc - P * P]) - (d[cc] * CT(6.0));
-            const CT tmp0 = d1[h] + div * (CT(1.0) / CT(6.0));
+        for (int r = 0; r < K; r++) {
+            const int cc = c[r];
+            const CT div = (d[cc + 1] + d[cc - 1] + d[cc + P] + d[cc - P] + d[cc + P * P] + d[cc - P * P]) - (d[cc] * CT(6.0));
+            const CT tmp0 = d1[r] + div * (CT(1.0) / CT(6.0));
             sm.buf[cur ^ 1][cc] = d[cc] + tmp0;
-            double sq = double(tmp0) * double(tmp0);
-            for (int o = 16; o > 0; o >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, o);
-            if ((lt & 31) == 0) sm.red[cur][h * (HT >> 5) + (lt >> 5)] = sq;
+            sq[r] = double(tmp0) * double(tmp0);
         }
-        named_sync(bar, HT);
-        double r[NW];
 #pragma unroll
-        for (int w = 0; w < NW; w++) r[w] = sm.red[cur][w];
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int r = 0; r < K; r++) sq[r] += __shfl_xor_sync(0xffffffffu, sq[r], o);
+        if ((lt & 31) == 0) {
+#pragma unroll
+            for (int r = 0; r < K; r++) sm.red[cur][r * WT + (lt >> 5)] = sq[r];
+        }
+        sync();
+        // pairwise sum of the warp partials (fixed tree, identical in every
+        // thread): log2(NW) dependent additions instead of NW
+        double w[NW];
+#pragma unroll
+        for (int q = 0; q < NW; q++) w[q] = sm.red[cur][q];
 #pragma unroll
         for (int span = 1; span < NW; span <<= 1)
 #pragma unroll
-            for (int w = 0; w + span < NW; w += 2 * span) r[w] = r[w] + r[w + span];
-        resid = r[0];
+            for (int q = 0; q + span < NW; q += 2 * span) w[q] = w[q] + w[q + span];
+        resid = w[0];
         if (iters == 0) resid0 = resid;
         iters++;
         cur ^= 1;
     } while (resid / resid0 > 0.5 && iters < 16);
-    out[0] = sm.buf[cur][c[0]];
-    out[1] = sm.buf[cur][c[1]];
+#pragma unroll
+    for (int r = 0; r < K; r++) out[r] = sm.buf[cur][c[r]];
     return resid;
+}
+
+// This thread's cells and their dphi1 values.
+template <int NX, int TH, typename CT>
+__device__ __forceinline__ void relax_cells(int lt, const CT* __restrict__ dphi1, int* c, CT* d1) {
+    constexpr int K = NX * NX * NX / TH;
+#pragma unroll
+    for (int r = 0; r < K; r++) {
+        c[r] = relax_cell<NX>(lt + r * TH);
+        d1[r] = dphi1[c[r]];
+    }
+}
+
+// Stages the brick (dphi with ghosts) into both buffers.
+template <int NX, int TH, typename CT>
+__device__ __forceinline__ void relax_stage(RelaxSmem<NX, CT>& sm, const CT* __restrict__ dphi, int lt) {
+    constexpr int P3 = RelaxSmem<NX, CT>::P3;
+    for (int q = lt; q < P3; q += TH) {
+        const CT v = dphi[q];
+        sm.buf[0][q] = v;
+        sm.buf[1][q] = v;
+    }
+}
+
+// Stages the brick and relaxes it: returns the last sweep's sum and leaves
+// the relaxed interior values of this thread's cells c[r] in out[r].  CT is
+// the correction's storage and arithmetic type (FP64, or FP32 in the mixed
+// form); the sums of squares are formed in FP64 either way.
+template <int NX, int TH, typename CT, typename Sync>
+__device__ __forceinline__ double relax_brick(RelaxSmem<NX, CT>& sm, const CT* __restrict__ dphi,
+                                              const CT* __restrict__ dphi1, int lt, int* c, CT* out, Sync sync) {
+    constexpr int K = NX * NX * NX / TH;
+    relax_stage<NX, TH, CT>(sm, dphi, lt);
+    CT d1[K];
+    relax_cells<NX, TH, CT>(lt, dphi1, c, d1);
+    sync();
+    return relax_sweeps<NX, TH, CT>(sm, lt, c, d1, out, sync);
 }
 
 }  // namespace amr

@@ -252,7 +252,9 @@ int amr_m1m2data(amr_ctx* ctx, double* out, double* l1);
  * state and sets the time and the root's flow-off; it checks the offsets and
  * the file length against the context's BW, GNX and NF (AMR_ERR_STATE).
  * The potential is not part of the format (Binary::pot_from_grid rebuilds
- * it from the pot field). */
+ * it from the pot field).  refine_alpha is the value of the reference's
+ * static GridNode::refine_alpha written with every brick; a negative value
+ * writes the one the last amr_read_checkpoint found (1.0 before any). */
 typedef struct amr_binary_header {
     double l1x, h, M1, fill_factor, n, R1, q, a, K1, K2, phi0_1, phi0_2, Omega, phase, Omega0;
     int accretor_type, donor_type;
@@ -310,8 +312,11 @@ int amr_relax_passes(amr_ctx* ctx, long long* per_level, int n);
  * level sums) makes before the solve gives up: the waiting block sets the
  * abort word, every block leaves at its next wait, and amr_graph_solve (or
  * the step that called it) returns AMR_ERR_TIMEOUT with the context still
- * usable.  Replaces the reference's unbounded loops; 0 restores the default
- * 2^22 polls (seconds). */
+ * usable.  The same limit bounds the fused substep's wait for a finer
+ * neighbour's published faces (amr_fused_sub_step then returns
+ * AMR_ERR_TIMEOUT; the state is the caller's to restore).  Replaces the
+ * reference's unbounded loops; 0 restores the defaults (2^22 polls for the
+ * solve, 2^24 for the substep: seconds). */
 int amr_set_wait_limit(amr_ctx* ctx, int polls);
 /* Of those phase times, the part spent at each phase's closing grid barrier
  * (block 0, from its arrival to the barrier's exit: the slowest block's extra
