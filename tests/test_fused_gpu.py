@@ -98,3 +98,39 @@ def test_fused_rejects_ppm(gpu):
         a.fused_sub_step(a.max_dt(), 1.0, 0)
     assert e.value.code == -1
     a.close()
+
+
+@pytest.mark.gpu
+def test_fused_wait_limit_times_out_and_context_recovers(gpu):
+    """A wait limit of one poll makes a coarse brick's wait for a finer
+    neighbour's published faces run out (no block is made to fault or hang;
+    the whole three-level tree is resident at once, so coarse bricks meet
+    children still in flight): the substep returns AMR_ERR_TIMEOUT, and with
+    the default limit back the same context steps bit for bit like the plain
+    substep."""
+    g = load_golden("hydro_bump_zr_L3")
+    maxl = int(g["init_level"].max())
+    a, b = make(gpu, "zr", maxl), make(gpu, "zr", maxl)
+    load_state(a, g)
+    dt = a.max_dt()
+    b.set_wait_limit(1)
+    timed_out = False
+    for _ in range(5):
+        load_state(b, g)
+        b.store()
+        try:
+            b.fused_sub_step(dt, 1.0, 0)
+        except gpu.AmrError as e:
+            assert e.code == -5  # AMR_ERR_TIMEOUT
+            timed_out = True
+            break
+    assert timed_out
+    b.set_wait_limit(0)
+    load_state(b, g)
+    b.set_flow_off(np.zeros(b.nf))  # the failed substep's flow-off went in
+    rk3(a, dt, False)
+    rk3(b, dt, True)
+    assert np.array_equal(interior(a), interior(b))
+    assert np.array_equal(a.flow_off(), b.flow_off())
+    a.close()
+    b.close()

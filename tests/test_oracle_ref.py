@@ -20,13 +20,13 @@ make_golden = importlib.util.module_from_spec(spec)
 spec.loader.exec_module(make_golden)
 
 
-@pytest.mark.parametrize("name", ["hydro_bump_L2", "hydro_ppm_bump_L2", "grav_poly_L2", "ztwd_L2"])
+@pytest.mark.parametrize("name", ["hydro_bump_L2", "hydro_ppm_bump_L2", "grav_poly_L2", "ztwd_L2", "ztwd12_L2"])
 def test_golden_is_reference_output(name, table_path):
     variant = make_golden.CASES[name][0]
     if ref_binary(variant) is None:
         pytest.skip("oracle/_ref/%s_harness not built" % variant)
     with tempfile.TemporaryDirectory() as td:
-        if variant == "ztwd":
+        if variant in ("ztwd", "ztwd12"):
             os.symlink(table_path, os.path.join(td, "helmholtz.table"))
         res = make_golden.run_case(name, td)
     g = np.load(os.path.join(GOLDEN, name + ".npz"))

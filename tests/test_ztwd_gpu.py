@@ -4,11 +4,11 @@ ztwd_*: the reference's own two-polytrope initial data (binary/initialize.cpp)
 for a q = 0.7 binary in the co-rotating frame, then BinaryDriver::step
 (binary/binary_driver.cpp:346-459) with dt from GridNode::max_dt and the
 MAXDTINC clamp, run by oracle/harness/ztwd_harness.cpp on the reference's
-BINARY build (ZTWD state, PPM, BW 3, 8^3 bricks) reading the synthetic
-Helmholtz table.  The library replays the same steps (amr_ztwd_step); trees
-must match bit for bit, dt to 1e-12 and every field to 1e-12
-(max |a-b| / max |b| per field).  ztwd_L3 regrids at its step 8 (the tree
-changes), so its final state is compared through per-brick sums.
+BINARY build (ZTWD state, PPM, BW 3; ztwd12_* on its own 12^3 bricks,
+ztwd_* on 8^3 bricks) reading the synthetic Helmholtz table.  The library
+replays the same steps (amr_ztwd_step); trees must match bit for bit, dt to
+1e-12 and every cell of every field to 1e-12 (max |a-b| / max |b| per
+field), across the regrids at steps 0 and 8.
 """
 
 import os
@@ -25,10 +25,10 @@ DYNAMIC_RANGE = 1.0e6  # binary/binary_defs.h:14
 MIXED_RTOL = 1.0e-6    # mixed + persistent form against FP64, density / energy rel L1 after the run
 
 
-def ztwd_config(maxlevel, **kw):
+def ztwd_config(maxlevel, nx=8, **kw):
     """The BINARY build's compile-time constants (binary/binary_defs.h) with
-    8^3 interior cells per brick."""
-    cfg = dict(physics=2, nf=13, bw=3, nx=8, reconstruction=1, grid_dim=1.0, z_reflect=1, mirror_refine_y=1,
+    nx^3 interior cells per brick (12 in the reference's build)."""
+    cfg = dict(physics=2, nf=13, bw=3, nx=nx, reconstruction=1, grid_dim=1.0, z_reflect=1, mirror_refine_y=1,
                max_refine_level=maxlevel, rho_floor=1.0e-10, cfl=0.3, maxdtinc=1.25, max_bricks=1024)
     cfg.update(kw)
     return cfg
@@ -38,7 +38,7 @@ def make(gpu, g, table_path, **kw):
     helm = _load_pkg_module("helm_b200", "helm.py").Helm(table_path)
     K1, Ucm, Ug, Us, omega, omega0 = [float(x) for x in g["extra"][:6]]
     helm.set_cgs_units(Ucm, Ug, Us, 1.0)  # Binary::set_units (binary/binary.h:17-35)
-    a = gpu.AMR(**ztwd_config(int(g["init_level"].max()), **kw))
+    a = gpu.AMR(**ztwd_config(int(g["init_level"].max()), nx=int(g["nx"]), **kw))
     a.ztwd_set_eos(helm)
     a.ztwd_set_frame(omega, omega0, 0.0, 0.0)
     a.load_tree(g["init_level"], g["init_loc"], g["init_age"])
@@ -68,7 +68,7 @@ def interior(a):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["ztwd_L2", "ztwd_L3"])
+@pytest.mark.parametrize("name", ["ztwd_L2", "ztwd_L3", "ztwd12_L2", "ztwd12_L3"])
 def test_ztwd_steps_match_reference(gpu, table_path, name):
     g = load_golden(name)
     nsteps = int(g["args"][1])
@@ -93,11 +93,12 @@ def test_ztwd_steps_match_reference(gpu, table_path, name):
 
 
 @pytest.mark.gpu
-def test_ztwd_mixed_persistent_close_to_fp64(gpu, table_path):
+@pytest.mark.parametrize("name", ["ztwd_L2", "ztwd12_L2"])
+def test_ztwd_mixed_persistent_close_to_fp64(gpu, table_path, name):
     """FP32 multigrid correction in the persistent solve, against the FP64
     form after the same steps: same trees and steps, density and energy
     within MIXED_RTOL (relative L1)."""
-    g = load_golden("ztwd_L2")
+    g = load_golden(name)
     nsteps = int(g["args"][1])
     a = make(gpu, g, table_path)
     b = make(gpu, g, table_path, precision=gpu.PREC_MIXED, persistent_solve=2)
@@ -168,4 +169,31 @@ def test_ztwd_m1m2data_matches_reference(gpu, table_path):
     bad = [(i, out[i], ref[i]) for i in range(28) if out[i] != ref[i]]
     assert not bad, bad
     assert d["m1"] > 0 and d["m2"] > 0 and 0.0 < d["q"] < 2.0
+    a.close()
+
+
+@pytest.mark.gpu
+def test_ztwd_configured_size_matches_reference(gpu, table_path, tmp_path):
+    """The headline configuration: the 5-level binary on the BINARY build's
+    12^3 bricks, 10 BinaryDriver steps (regrids at steps 0 and 8), plain
+    FP64 form.  The reference's initial state comes from a zero-step run of
+    its harness (checked against the golden's sums); trees bit for bit, dt
+    to 1e-12, every cell of 24 sampled bricks to 1e-12 of the field maxima,
+    every brick's sums to 1e-11, the potential of the sampled bricks to
+    1e-12, the flow-off."""
+    from cases import check_final_sampled, check_initial_sums, live_initial_state
+    g = load_golden("ztwd12_L5")
+    levels, nsteps = int(g["args"][0]), int(g["args"][1])
+    d0 = live_initial_state("ztwd12", ["ztwd", levels, 0], str(tmp_path), table_path)
+    check_initial_sums(d0, g)
+    init = {"init_level": d0.level, "init_loc": d0.loc, "init_age": d0.age, "extra": g["extra"],
+            "init_U": d0.U[:, :, 3:-3, 3:-3, 3:-3], "nx": g["nx"]}
+    a = make(gpu, init, table_path, max_bricks=2048)
+    dts = run(a, nsteps)
+    np.testing.assert_allclose(dts, g["extra"][8:8 + nsteps], rtol=DT_RTOL)
+    t = a.get_tree()
+    assert same_tree(t, g, "final_")
+    check_final_sampled(interior(a), a.download_poisson()[0], g)
+    fo = a.flow_off()
+    np.testing.assert_allclose(fo, g["final_FO"], rtol=1e-10, atol=1e-13 * max(1.0, np.abs(g["final_FO"]).max()))
     a.close()
