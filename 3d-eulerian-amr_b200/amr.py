@@ -22,6 +22,7 @@ RECON_MINMOD = 0
 RECON_PPM = 1
 PREC_FP64 = 0
 PREC_MIXED = 1
+PREC_MIXED_SOLVE = 2
 
 ERRORS = {
     -1: "AMR_ERR_ARG", -2: "AMR_ERR_CUDA", -3: "AMR_ERR_RANGE", -4: "AMR_ERR_NOCONVERGE",

@@ -478,6 +478,7 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
     if (cfg->physics < AMR_PHYSICS_EULER || cfg->physics > AMR_PHYSICS_ZTWD ||
         (ztwd && (cfg->reconstruction != AMR_RECON_PPM || (cfg->nx != 8 && cfg->nx != 12))))
         return AMR_ERR_ARG;
+    if (cfg->precision < AMR_PREC_FP64 || cfg->precision > AMR_PREC_MIXED_SOLVE) return AMR_ERR_ARG;
     if (cfg->nf != (ztwd ? (int)ZTWD_NF : 6) || cfg->bw < min_bw || cfg->bw > 4 || cfg->nx < 4 || (cfg->nx % 4) != 0 ||
         cfg->max_refine_level < 0 || cfg->max_refine_level > 12 || cfg->max_bricks < 0 ||
         (cfg->reconstruction != AMR_RECON_MINMOD && cfg->reconstruction != AMR_RECON_PPM))
@@ -502,7 +503,9 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
     g.pnx3 = g.pnx * g.pnx * g.pnx;
     g.ucount = g.nf * g.gnx3;
     g.z_reflect = cfg->z_reflect;
-    g.precision = cfg->precision;
+    // AMR_PREC_MIXED_SOLVE: the mixed multigrid correction, fluxes in FP64
+    g.precision = cfg->precision == AMR_PREC_FP64 ? AMR_PREC_FP64 : AMR_PREC_MIXED;
+    g.flux32 = cfg->precision == AMR_PREC_MIXED;
     g.recon = cfg->reconstruction;
     g.grid_dim = cfg->grid_dim;
     g.h0 = tp.h0;
@@ -538,7 +541,7 @@ int amr_create(const amr_config* cfg, amr_ctx** out) {
             double** parr[8] = {&c->st.phi, &c->st.phi0, &c->st.dphi, &c->st.dphi1,
                                 &c->st.S,   &c->st.fx,   &c->st.fy,   &c->st.fz};
             for (auto p : parr) rc |= dev_alloc(c, p, (size_t)cap * g.pnx3);
-            if (cfg->precision == AMR_PREC_MIXED) {
+            if (g.precision == AMR_PREC_MIXED) {
                 rc |= dev_alloc(c, &c->st.fdphi, (size_t)cap * g.pnx3);
                 rc |= dev_alloc(c, &c->st.fdphi1, (size_t)cap * g.pnx3);
             }
@@ -1028,7 +1031,7 @@ int amr_fused_sub_step(amr_ctx* c, double dt, double beta, int blocks_per_sm) {
     cudaError_t e;
     {
         ProfScope ps_(c->prof, KC_FUSED, c->stream, (long long)c->nfwork);
-        e = c->geom.precision == AMR_PREC_MIXED ? launch_substep_fused_f32(a, blocks_per_sm, c->stream, &c->fused_blocks)
+        e = c->geom.flux32 ? launch_substep_fused_f32(a, blocks_per_sm, c->stream, &c->fused_blocks)
                                                 : launch_substep_fused_f64(a, blocks_per_sm, c->stream, &c->fused_blocks);
     }
     if (e != cudaSuccess) {

@@ -22,7 +22,8 @@ struct Geom {
     int bw, nx, gnx, nf, pnx;
     int gnx3, pnx3, ucount;  // gnx^3, pnx^3, nf*gnx^3
     int z_reflect;
-    int precision;  // AMR_PREC_FP64 / AMR_PREC_MIXED
+    int precision;  // correction type of the multigrid solve: AMR_PREC_FP64 / AMR_PREC_MIXED (FP32)
+    int flux32;     // the KT reconstruction and flux in FP32 (AMR_PREC_MIXED)
     int recon;      // AMR_RECON_MINMOD / AMR_RECON_PPM (same values as RECON_* in recon.cuh)
     double grid_dim, h0;
     double origin[3];

@@ -68,6 +68,7 @@ struct GraphState {
     double* d_pres3 = nullptr;
     double* d_pnest = nullptr;
     GridBarrier* d_bar = nullptr;
+    unsigned* d_rpub = nullptr;  // [cap] relaxation pass words of the persistent solve
     cudaEvent_t ev_ps[2] = {nullptr, nullptr};  // around the last persistent launch
     double ps_ms_total = 0.0;                   // persistent launches of amr_graph_solve: device time, count
     long long ps_count = 0;
@@ -98,7 +99,7 @@ int ensure_state(amr_ctx* c) {
     CUDA_TRY(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CUDA_TRY(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned int) * 4, c->stream));
     if (c->cfg.persistent_solve) {
-        g->pblocks = solve_persistent_blocks(c->geom.nx, c->cfg.precision, c->cfg.persistent_solve);
+        g->pblocks = solve_persistent_blocks(c->geom.nx, c->geom.precision, c->cfg.persistent_solve);
         if (g->pblocks <= 0) {
             c->err = "no cooperative launch configuration for the persistent solve";
             return AMR_ERR_CUDA;
@@ -106,6 +107,7 @@ int ensure_state(amr_ctx* c) {
         CUDA_TRY(cudaMalloc(&g->d_pres3, sizeof(double) * 3 * (size_t)c->cap));
         CUDA_TRY(cudaMalloc(&g->d_pnest, sizeof(double) * (size_t)g->pblocks * c->cap));
         CUDA_TRY(cudaMalloc(&g->d_bar, sizeof(GridBarrier)));
+        CUDA_TRY(cudaMalloc(&g->d_rpub, sizeof(unsigned) * (size_t)c->cap));
         CUDA_TRY(cudaEventCreate(&g->ev_ps[0]));
         CUDA_TRY(cudaEventCreate(&g->ev_ps[1]));
     }
@@ -305,6 +307,8 @@ int rec_persistent(amr_ctx* c, cudaStream_t s, double tol) {
     a.snap_half = snap_stride(c) * (size_t)c->cap;
     a.bar = g->d_bar;
     CUDA_TRY(cudaMemsetAsync(g->d_bar, 0, sizeof(GridBarrier), s));
+    a.rpub = g->d_rpub;
+    CUDA_TRY(cudaMemsetAsync(g->d_rpub, 0, sizeof(unsigned) * (size_t)c->cap, s));
     // event nodes bracketing the launch: the elapsed time of the latest
     // replay is the kernel's duration on this stream
     CUDA_TRY(cudaEventRecordWithFlags(g->ev_ps[0], s, cudaEventRecordExternal));
@@ -506,6 +510,7 @@ void graph_release(amr_ctx* c) {
     if (g->d_pres3) cudaFree(g->d_pres3);
     if (g->d_pnest) cudaFree(g->d_pnest);
     if (g->d_bar) cudaFree(g->d_bar);
+    if (g->d_rpub) cudaFree(g->d_rpub);
     for (cudaEvent_t e : g->ev_ps)
         if (e) cudaEventDestroy(e);
     delete g;

@@ -79,9 +79,12 @@ __device__ inline double nested_sum_smem(const LevelLists& L, const double* leaf
     return r;
 }
 
+// `self`, when given, holds the brick's own values before this pass (a
+// brick kept in shared memory); else they are read from dphi.
 template <int NX, typename CT>
 __device__ __forceinline__ CT ghost_dphi(const Geom& g, const BrickTable& bt, const DevState& st, const CT* snap_rd,
-                                         size_t stride, int b, int face, int t1, int t2) {
+                                         size_t stride, int b, int face, int t1, int t2,
+                                         const CT* self = nullptr) {
     constexpr int P = NX + 2;
     const int kind = bt.ftype[6 * b + face];
     const int nbr = bt.fnbr[6 * b + face];
@@ -95,7 +98,7 @@ __device__ __forceinline__ CT ghost_dphi(const Geom& g, const BrickTable& bt, co
     const int q2 = ax == 2 ? qa : t2;
     if (kind == FACE_REFLECT) {  // own value mirrored through z = 0, before this pass
         const int kk = q2 == 1 ? P - 2 : 1;
-        return D[(size_t)b * P * P * P + (kk * P + q1) * P + q0];
+        return self ? self[(kk * P + q1) * P + q0] : D[(size_t)b * P * P * P + (kk * P + q1) * P + q0];
     }
     const int v = (face & 1) ? 1 : -1;
     const int r0 = (bt.off[3 * b + 0] + (ax == 0 ? v * (P - 2) : 0) - 2 * bt.off[3 * nbr + 0] - (g.bw - 1) + q0) / 2;
@@ -121,20 +124,26 @@ __device__ __forceinline__ int relax_ghost_cell(int q, int& face, int& t1, int& 
     return (d[2] * P + d[1]) * P + d[0];
 }
 
-// Writes a relaxed interior value of cell t (interior index) to dphi and,
-// where the cell lies on a face, to that face's first-interior layer of the
-// snapshot (layer of face f holds the cells adjacent to it).
+// Where interior cell t (interior index) lies on a face, writes its value to
+// that face's first-interior layer of the snapshot (layer of face f holds
+// the cells adjacent to it).
 template <int NX, typename CT>
-__device__ __forceinline__ void relax_put(CT* D, CT* sw, int t, CT v) {
-    constexpr int P = NX + 2;
+__device__ __forceinline__ void relax_layer_put(CT* sw, int t, CT v) {
     const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
-    D[(ck * P + cj) * P + ci] = v;
     if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = v;
     if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = v;
     if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = v;
     if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = v;
     if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = v;
     if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v;
+}
+
+// Writes a relaxed interior value of cell t to dphi and to the snapshot.
+template <int NX, typename CT>
+__device__ __forceinline__ void relax_put(CT* D, CT* sw, int t, CT v) {
+    constexpr int P = NX + 2;
+    D[((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1] = v;
+    relax_layer_put<NX, CT>(sw, t, v);
 }
 
 // One relaxation pass of brick b by TH threads (local index lt, barrier

@@ -412,7 +412,7 @@ void launch_ghost_fill(const Geom& g, const BrickTable& bt, const DevState& st, 
 }
 void launch_flux(const Geom& g, const DevState& st, const int* slots, int n, cudaStream_t s) {
     if (n <= 0) return;
-    if (g.precision == AMR_PREC_MIXED) {
+    if (g.flux32) {
         launch_flux_f32(g, st, slots, n, s);
         return;
     }

@@ -140,6 +140,7 @@ struct Solver {
     static constexpr int TPB = Lay::TPB;
     const SolveArgs& a;
     RelaxSmem<NX, CT>* sm;  // Lay::NSM staged bricks
+    CT* xbuf;               // a third brick buffer of (NX+2)^3 entries
     double* red;
     double* nbuf;    // 2 * NEST_SMEM doubles of shared memory for the level sums
     double* nest;    // this block's scratch [cap] (level sums of larger trees)
@@ -149,6 +150,8 @@ struct Solver {
     int max_outer;
     unsigned bar_target = 0;    // thread 0: arrivals that complete the next barrier
     unsigned lsum_gen = 0;      // level sums published so far in this launch
+    unsigned pass_seq = 0;      // last pass word used by the shared-memory relaxation loops
+    unsigned arrivals = 0;      // their arrivals released so far in this launch
     unsigned long long spin_limit = BARRIER_SPINS;  // polls per bounded wait
     unsigned long long t_last;  // block 0: global time at the last barrier exit
     // block 0's phase accounting, in shared memory
@@ -307,7 +310,7 @@ struct Solver {
             if (t < 6 * PF) op_dphi_faces<CT>(a.g, a.bt, a.st, a.aux, sl[q], t / PF, t % PF, PF);
         });
         if (!sync(PH_DPHI_FACES, n)) return false;
-        if (n < (int)gridDim.x) return relax_loop_overlapped(l, ratio, sl, n, snap);
+        if (n < (int)gridDim.x) return relax_loop_resident(l, ratio, sl, n, snap);
         int par = 0;
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
         relax_pass(sl, n, 0, snap, snap, pres);
@@ -339,23 +342,130 @@ struct Solver {
         return true;
     }
 
-    // The relaxation loop of a level with fewer bricks than blocks (one
-    // brick per block, the last block without one), with the level sums off
-    // the critical path: after each pass's barrier the last block forms the
-    // pass's nested sum and publishes it, while every brick computes the
-    // next pass without writing anything (op_relax_spec).  The pass is
-    // written (op_relax_commit) once the sum says the loop goes on, and
-    // dropped when it ends.  Passes written, their values, the sums and the
-    // loop decisions are those of the loop in relax_until.
-    __device__ bool relax_loop_overlapped(int l, double ratio, const int* sl, int n, CT* snap) {
+    // Thread 0 of lanes: waits until the word at p reaches target (acquire);
+    // false when the solve aborted or the wait ran out.
+    __device__ bool wait_word(const unsigned* p, unsigned target) {
+        unsigned long long spins = 0;
+        for (;;) {
+            unsigned v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+            if ((int)(v - target) >= 0) return true;
+            if ((spins & 63) == 63 && ld_volatile(&a.bar->abort)) return false;
+            if (++spins > spin_limit) {
+                give_up(a.bar, &a.ctl->status);
+                return false;
+            }
+            if (spins > 32) __nanosleep(20);
+        }
+    }
+
+    // Waits (lanes 0-5 of warp 0, one per face) until brick b's same-level
+    // neighbours have published pass `seq`; every thread then sees their
+    // snapshot layers.
+    __device__ bool wait_neighbours(int b, unsigned seq) {
+        __shared__ int s_ok;
+        if (threadIdx.x < 32) {
+            int good = 1;
+            const int f = threadIdx.x;
+            if (f < 6 && a.bt.ftype[6 * b + f] == FACE_SIB) good = wait_word(a.rpub + a.bt.fnbr[6 * b + f], seq);
+            good = __all_sync(0xffffffffu, good);
+            if (threadIdx.x == 0) s_ok = good;
+        }
+        __syncthreads();
+        return s_ok != 0;
+    }
+
+    // Publishes the relaxed brick `res` as a pass: its first interior layers
+    // to snapshot `wr`, its sum to pres[b]; then brick b's pass word is
+    // released as `seq` and the level's arrival count raised.
+    __device__ void resident_publish(int b, const CT* res, const int* c, CT* wr, double* pres, double resid,
+                                     unsigned seq) {
+        constexpr int K = NX * NX * NX / TPB;
+        CT* sw = wr + (size_t)b * a.stride;
+#pragma unroll
+        for (int r = 0; r < K; r++) relax_layer_put<NX, CT>(sw, threadIdx.x + r * TPB, res[c[r]]);
+        if (threadIdx.x == 0) pres[b] = resid;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(a.rpub + b), "r"(seq) : "memory");
+            asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&a.bar->relax_arrivals), "r"(1u)
+                         : "memory");
+        }
+    }
+
+    // One pass of brick b from its committed values in `base`, ghost faces
+    // from snapshot `rd` (the parent across coarse-fine faces, the mirror of
+    // `base` across z = 0, 0 on outflow faces), swept in x and y; nothing is
+    // written outside shared memory.  Returns the sum and the buffer with the
+    // relaxed brick (x or y).
+    __device__ double resident_pass(int b, CT* base, CT* x, CT* y, const CT* rd, const int* c, const CT* d1,
+                                    CT** res) {
+        constexpr int K = NX * NX * NX / TPB, F = NX * NX;
+#pragma unroll
+        for (int r = 0; r < K; r++) x[c[r]] = base[c[r]];
+        for (int q = threadIdx.x; q < 6 * F; q += TPB) {
+            int face, t1, t2;
+            const int gi = relax_ghost_cell<NX>(q, face, t1, t2);
+            const CT v = ghost_dphi<NX, CT>(a.g, a.bt, a.st, rd, a.stride, b, face, t1, t2, base);
+            x[gi] = v;
+            y[gi] = v;
+        }
+        __syncthreads();
+        return relax_sweeps_in<NX, TPB, CT>(x, y, &sm[0].red[0][0], threadIdx.x, c, d1, res, BlockSync{});
+    }
+
+    // The server's part of a pass: waits until the level's bricks have all
+    // released `target` arrivals, forms the level sum of `done` and publishes
+    // it as generation lsum_gen.
+    __device__ bool serve_sum(int l, const double* done, unsigned target) {
+        __shared__ int s_ok;
+        if (threadIdx.x == 0) s_ok = wait_word(&a.bar->relax_arrivals, target);
+        __syncthreads();
+        if (!s_ok) return false;
+        const double r = level_sum(l, done);
+        if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
+        return true;
+    }
+
+    // The relaxation loop of a level with fewer bricks than blocks: one
+    // brick per block, the brick kept in shared memory for the whole loop,
+    // the last block (which has no brick) forming the level sums.  No grid
+    // barrier between passes: a brick waits only for its same-level
+    // neighbours' published face layers (their pass words), computes the
+    // next pass from shared memory while the server forms the last pass's
+    // nested sum, and publishes it (snapshot layers, sum, pass word) once
+    // the sum says the loop goes on -- else the pass is dropped.  The loop
+    // ends with one write of each brick (interior and ghost faces) back to
+    // dphi and one grid barrier.  Passes written, their values, the sums
+    // and every loop decision are those of the loop in relax_until.
+    __device__ bool relax_loop_resident(int l, double ratio, const int* sl, int n, CT* snap) {
+        constexpr int K = NX * NX * NX / TPB, P3 = (NX + 2) * (NX + 2) * (NX + 2), F = NX * NX;
         const bool mine = (int)blockIdx.x < n;
         const bool server = blockIdx.x == gridDim.x - 1;
         const int b = mine ? sl[blockIdx.x] : -1;
+        CT* bufs[3] = {sm[0].buf[0], sm[0].buf[1], xbuf};
+        int ib = 0;  // buffer holding the committed brick
+        int c[K];
+        CT d1[K];
+        const unsigned seq0 = pass_seq + 1;  // pass word of pass 0
+        const unsigned arr0 = arrivals;
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
-        if (mine)
-            op_relax_pass<NX, TPB, CT>(a.g, a.bt, a.st, b, 0, snap, snap, a.stride, pres, sm[0], threadIdx.x,
-                                       BlockSync{});
-        if (!sync(PH_RELAX_FIRST, n)) return false;
+        if (mine) {
+            // pass 0: the ghost faces are in dphi (filled by the face phase)
+            const CT* D = Corr<CT>::dphi(a.st) + (size_t)b * P3;
+            for (int q = threadIdx.x; q < P3; q += TPB) {
+                const CT v = D[q];
+                bufs[0][q] = v;
+                bufs[1][q] = v;
+            }
+            relax_cells<NX, TPB, CT>(threadIdx.x, Corr<CT>::dphi1(a.st) + (size_t)b * P3, c, d1);
+            __syncthreads();
+            CT* res;
+            const double r = relax_sweeps_in<NX, TPB, CT>(bufs[0], bufs[1], &sm[0].red[0][0], threadIdx.x, c, d1,
+                                                          &res, BlockSync{});
+            ib = res == bufs[0] ? 0 : 1;
+            resident_publish(b, res, c, snap, pres, r, seq0);
+        }
         count_pass(l);
         // pass 1 runs whatever the first sum; that sum is formed meanwhile
         double r0;
@@ -364,31 +474,33 @@ struct Solver {
             relax_par ^= 1;
             pres = a.pres + (size_t)relax_par * a.L.cap;
             ++lsum_gen;
-            if (server) {
-                const double r = level_sum(l, done);
-                if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
+            if (server && !serve_sum(l, done, arr0 + n)) return false;
+            if (mine) {
+                if (!wait_neighbours(b, seq0)) return false;
+                CT* res;
+                const double r = resident_pass(b, bufs[ib], bufs[(ib + 1) % 3], bufs[(ib + 2) % 3], snap, c, d1, &res);
+                ib = res == bufs[(ib + 1) % 3] ? (ib + 1) % 3 : (ib + 2) % 3;
+                resident_publish(b, bufs[ib], c, snap + a.snap_half, pres, r, seq0 + 1);
             }
-            if (mine)
-                op_relax_pass<NX, TPB, CT>(a.g, a.bt, a.st, b, 1, snap, snap + a.snap_half, a.stride, pres, sm[0],
-                                           threadIdx.x, BlockSync{});
             if (!wait_sum(r0)) return false;
-            if (!sync(PH_RELAX, n)) return false;
             count_pass(l);
         }
-        int par = 1;  // snapshot buffer written by the last pass
+        int par = 1;         // snapshot buffer written by the last published pass
+        unsigned k = 1;      // last published pass
         int outer = 1;
         for (;;) {
             const double* done = pres;
             relax_par ^= 1;
             pres = a.pres + (size_t)relax_par * a.L.cap;
             ++lsum_gen;
-            if (server) {
-                const double r = level_sum(l, done);
-                if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
+            if (server && !serve_sum(l, done, arr0 + n * (k + 1))) return false;
+            CT* res = nullptr;
+            double rr = 0.0;
+            if (mine) {
+                if (!wait_neighbours(b, seq0 + k)) return false;
+                rr = resident_pass(b, bufs[ib], bufs[(ib + 1) % 3], bufs[(ib + 2) % 3], snap + (size_t)par * a.snap_half,
+                                   c, d1, &res);
             }
-            RelaxSpec<CT, NX * NX * NX / TPB> sp;
-            if (mine)
-                sp = op_relax_spec<NX, TPB, CT>(a.g, a.bt, a.st, b, snap + (size_t)par * a.snap_half, a.stride, sm[0]);
             double r;
             if (!wait_sum(r)) return false;
             bool again = r / r0 > ratio;
@@ -397,15 +509,30 @@ struct Solver {
                 status = 1;
             }
             if (!again) break;
-            if (mine)
-                op_relax_commit<NX, TPB, CT>(a.st, b, sp, sm[0], snap + (size_t)(par ^ 1) * a.snap_half, a.stride,
-                                             pres);
-            if (!sync(PH_RELAX, n)) return false;
+            if (mine) {
+                ib = res == bufs[(ib + 1) % 3] ? (ib + 1) % 3 : (ib + 2) % 3;
+                resident_publish(b, bufs[ib], c, snap + (size_t)(par ^ 1) * a.snap_half, pres, rr, seq0 + k + 1);
+            }
             par ^= 1;
+            ++k;
             count_pass(l);
             ++outer;
         }
-        return true;
+        if (mine) {
+            // the committed brick back to dphi: interior and ghost faces
+            CT* D = Corr<CT>::dphi(a.st) + (size_t)b * P3;
+            const CT* B = bufs[ib];
+#pragma unroll
+            for (int r = 0; r < K; r++) D[c[r]] = B[c[r]];
+            for (int q = threadIdx.x; q < 6 * F; q += TPB) {
+                int face, t1, t2;
+                const int gi = relax_ghost_cell<NX>(q, face, t1, t2);
+                D[gi] = B[gi];
+            }
+        }
+        pass_seq = seq0 + k;
+        arrivals = arr0 + n * (k + 1);
+        return sync(PH_RELAX, n * (k + 1));
     }
 
     // Poisson::vcycle (poisson.cpp:1069-1074) = vcycle0 (poisson.cpp:53-84)
@@ -502,7 +629,10 @@ __global__ void __launch_bounds__(SolveLayout<NX>::TPB, 2) k_solve_persistent(So
     // loop limits are read from the control block (set by the host before
     // every launch; a captured graph keeps its arguments)
     const int max_cycles = *(volatile int*)&a.ctl->max_cycles;
-    Solver<NX, CT> s{a, sm, red, nbuf, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0,
+    // the third brick buffer: the second half's staging buffer where the
+    // layout has one, else the dynamic shared memory after the staged brick
+    CT* xbuf = SolveLayout<NX>::NSM == 2 ? sm[1].buf[0] : reinterpret_cast<CT*>(sm + 1);
+    Solver<NX, CT> s{a, sm, xbuf, red, nbuf, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0,
                  *(volatile int*)&a.ctl->max_outer};
     __shared__ unsigned long long s_ph_ns[PH_COUNT];
     __shared__ unsigned s_ph_n[PH_COUNT];
@@ -571,7 +701,8 @@ __global__ void __launch_bounds__(SolveLayout<NX>::TPB, 2) k_solve_persistent(So
 
 template <int NX, typename CT>
 constexpr size_t solve_smem() {
-    return SolveLayout<NX>::NSM * sizeof(RelaxSmem<NX, CT>);
+    return SolveLayout<NX>::NSM * sizeof(RelaxSmem<NX, CT>) +
+           (SolveLayout<NX>::NSM == 1 ? sizeof(CT) * (NX + 2) * (NX + 2) * (NX + 2) : 0);
 }
 
 int solve_persistent_attributes() {

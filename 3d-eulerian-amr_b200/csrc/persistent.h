@@ -20,6 +20,10 @@ struct GridBarrier {
     unsigned int lsum_gen;
     unsigned int pad1;
     double lsum_val[2];
+    // passes published by the bricks of the shared-memory relaxation loops
+    // (one release add per brick and pass); grows over the launch
+    unsigned int relax_arrivals;
+    unsigned int pad2;
 };
 
 struct SolveArgs {
@@ -43,6 +47,7 @@ struct SolveArgs {
     double* pres;  // [3][cap]: two relaxation buffers, one for the L1 error
     double* nest;  // [blocks][cap] per-block nested-sum scratch
     void* snap;    // [2][cap][stride] face snapshots (CT entries)
+    unsigned* rpub;  // [cap] last pass a brick published in the shared-memory relaxation loops (zero per launch)
     size_t stride;
     size_t snap_half;
     GridBarrier* bar;

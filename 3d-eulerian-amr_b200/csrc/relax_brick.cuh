@@ -63,41 +63,45 @@ __device__ __forceinline__ int relax_cell(int t) {
     return ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
 }
 
-// The sweeps on a brick staged in both buffers (every cell, ghosts
-// included): thread lt owns the K cells c[r] with dphi1 values d1[r].
-// Returns the last sweep's sum and leaves the relaxed values in out[r].
+// The sweeps on a brick staged in two buffers x, y (x holds every cell,
+// ghosts included; y the same ghost faces): thread lt owns the K cells c[r]
+// with dphi1 values d1[r]; red holds the per-sweep warp partials
+// (2 x NX^3 / 32).  Returns the last sweep's sum and the buffer that holds
+// the relaxed brick.
 template <int NX, int TH, typename CT, typename Sync>
-__device__ __forceinline__ double relax_sweeps(RelaxSmem<NX, CT>& sm, int lt, const int* c, const CT* d1, CT* out,
-                                               Sync sync) {
-    constexpr int P = RelaxSmem<NX, CT>::P, NW = RelaxSmem<NX, CT>::NW, K = NX * NX * NX / TH, WT = TH / 32;
+__device__ __forceinline__ double relax_sweeps_in(CT* x, CT* y, double* red, int lt, const int* c, const CT* d1,
+                                                  CT** result, Sync sync) {
+    constexpr int P = NX + 2, NW = NX * NX * NX / 32, K = NX * NX * NX / TH, WT = TH / 32;
     static_assert((NX * NX * NX) % TH == 0 && TH % 32 == 0, "relaxation layout");
     double resid0 = 0.0, resid = 0.0;
     int iters = 0, cur = 0;
     do {
-        const CT* d = sm.buf[cur];
+        const CT* d = cur ? y : x;
+        CT* w_ = cur ? x : y;
         double sq[K];
 #pragma unroll
         for (int r = 0; r < K; r++) {
             const int cc = c[r];
             const CT div = (d[cc + 1] + d[cc - 1] + d[cc + P] + d[cc - P] + d[cc + P * P] + d[cc - P * P]) - (d[cc] * CT(6.0));
             const CT tmp0 = d1[r] + div * (CT(1.0) / CT(6.0));
-            sm.buf[cur ^ 1][cc] = d[cc] + tmp0;
+            w_[cc] = d[cc] + tmp0;
             sq[r] = double(tmp0) * double(tmp0);
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
             for (int r = 0; r < K; r++) sq[r] += __shfl_xor_sync(0xffffffffu, sq[r], o);
+        double* rd = red + cur * NW;
         if ((lt & 31) == 0) {
 #pragma unroll
-            for (int r = 0; r < K; r++) sm.red[cur][r * WT + (lt >> 5)] = sq[r];
+            for (int r = 0; r < K; r++) rd[r * WT + (lt >> 5)] = sq[r];
         }
         sync();
         // pairwise sum of the warp partials (fixed tree, identical in every
         // thread): log2(NW) dependent additions instead of NW
         double w[NW];
 #pragma unroll
-        for (int q = 0; q < NW; q++) w[q] = sm.red[cur][q];
+        for (int q = 0; q < NW; q++) w[q] = rd[q];
 #pragma unroll
         for (int span = 1; span < NW; span <<= 1)
 #pragma unroll
@@ -107,9 +111,21 @@ __device__ __forceinline__ double relax_sweeps(RelaxSmem<NX, CT>& sm, int lt, co
         iters++;
         cur ^= 1;
     } while (resid / resid0 > 0.5 && iters < 16);
-#pragma unroll
-    for (int r = 0; r < K; r++) out[r] = sm.buf[cur][c[r]];
+    *result = cur ? y : x;
     return resid;
+}
+
+// The same sweeps on a RelaxSmem's two buffers; the relaxed values of this
+// thread's cells go to out[r].
+template <int NX, int TH, typename CT, typename Sync>
+__device__ __forceinline__ double relax_sweeps(RelaxSmem<NX, CT>& sm, int lt, const int* c, const CT* d1, CT* out,
+                                               Sync sync) {
+    constexpr int K = NX * NX * NX / TH;
+    CT* res;
+    const double r = relax_sweeps_in<NX, TH, CT>(sm.buf[0], sm.buf[1], &sm.red[0][0], lt, c, d1, &res, sync);
+#pragma unroll
+    for (int q = 0; q < K; q++) out[q] = res[c[q]];
+    return r;
 }
 
 // This thread's cells and their dphi1 values.

@@ -110,7 +110,7 @@ int zt_solve(amr_ctx* c, double tol) {
         c->zt_first_solve = 0;
     }
     const int max_cycles = 10000;  // MAX_POISSON_ITER (defs.h:25)
-    if (c->cfg.persistent_solve > 0 || c->cfg.precision == AMR_PREC_MIXED)
+    if (c->cfg.persistent_solve > 0 || c->geom.precision == AMR_PREC_MIXED)
         TRY(amr_graph_solve(c, tol, max_cycles, nullptr, nullptr));
     else
         TRY(amr_poisson_solve(c, tol, max_cycles, nullptr, nullptr));

@@ -146,16 +146,17 @@ __global__ void k_zt_prim(Geom g, BrickTable bt, DevState st, ZtwdPar P, const i
 }
 
 // Colella-Woodward monotonisation of one cell's edges (reconstruct.cpp:40-53)
-__device__ __forceinline__ void cw_mono(double q0, double& lo, double& hi) {
-    const double six = 1.0 / 6.0;
-    const double tmp1 = hi - lo;
-    const double tmp2 = hi + lo;
-    if ((hi - q0) * (q0 - lo) <= 0.0) {
+template <typename T>
+__device__ __forceinline__ void cw_mono(T q0, T& lo, T& hi) {
+    const T six = T(1.0) / T(6.0);
+    const T tmp1 = hi - lo;
+    const T tmp2 = hi + lo;
+    if ((hi - q0) * (q0 - lo) <= T(0.0)) {
         hi = lo = q0;
-    } else if (tmp1 * (q0 - 0.5 * tmp2) > six * tmp1 * tmp1) {
-        lo = 3.0 * q0 - 2.0 * hi;
-    } else if (-six * tmp1 * tmp1 > tmp1 * (q0 - 0.5 * tmp2)) {
-        hi = 3.0 * q0 - 2.0 * lo;
+    } else if (tmp1 * (q0 - T(0.5) * tmp2) > six * tmp1 * tmp1) {
+        lo = T(3.0) * q0 - T(2.0) * hi;
+    } else if (-six * tmp1 * tmp1 > tmp1 * (q0 - T(0.5) * tmp2)) {
+        hi = T(3.0) * q0 - T(2.0) * lo;
     }
 }
 
@@ -163,33 +164,34 @@ __device__ __forceinline__ void cw_mono(double q0, double& lo, double& hi) {
 // states by Reconstruct::ppm as called (reconstruct.cpp:22-58, 94) from the
 // primitives of cells f-3 .. f+2; the potential is a low-order and smooth
 // field (state_ztwd.cpp:50-56): plain interface average, no monotonisation.
-__device__ __forceinline__ void zt_face_states(const Geom& g, const double* W, int base, int stride, int f,
-                                               double* ql, double* qr) {
-    const double six = 1.0 / 6.0;
+template <typename T>
+__device__ __forceinline__ void zt_face_states(const Geom& g, const double* W, int base, int stride, int f, T* ql,
+                                               T* qr) {
+    const T six = T(1.0) / T(6.0);
 #pragma unroll
     for (int l = 0; l < ZT_NF; l++) {
         const double* w = W + l * g.gnx3 + base;
-        double q[6];
+        T q[6];
 #pragma unroll
-        for (int m = 0; m < 6; m++) q[m] = w[(f - 3 + m) * stride];
+        for (int m = 0; m < 6; m++) q[m] = T(w[(f - 3 + m) * stride]);
         if (l == ZT_POT) {
-            const double I = (q[2] + q[3]) * 0.5;
+            const T I = (q[2] + q[3]) * T(0.5);
             ql[l] = I;
             qr[l] = I;
             continue;
         }
-        double s[5];
+        T s[5];
 #pragma unroll
-        for (int m = 1; m <= 4; m++) s[m] = minmod_theta(q[m + 1] - q[m], q[m] - q[m - 1], 2.0);
-        double I[4];
+        for (int m = 1; m <= 4; m++) s[m] = minmod_theta(q[m + 1] - q[m], q[m] - q[m - 1], T(2.0));
+        T I[4];
 #pragma unroll
         for (int m = 1; m <= 3; m++) {
-            I[m] = (q[m] + q[m + 1]) * 0.5;
+            I[m] = (q[m] + q[m + 1]) * T(0.5);
             I[m] += (s[m] - s[m + 1]) * six;
         }
-        double lo1 = I[1], hi1 = I[2];  // cell f-1
+        T lo1 = I[1], hi1 = I[2];  // cell f-1
         cw_mono(q[2], lo1, hi1);
-        double lo2 = I[2], hi2 = I[3];  // cell f
+        T lo2 = I[2], hi2 = I[3];  // cell f
         cw_mono(q[3], lo2, hi2);
         ql[l] = hi1;
         qr[l] = lo2;
@@ -244,7 +246,12 @@ __device__ __forceinline__ void face_X(const Geom& g, const BrickTable& bt, int 
 // EOS call per face state, and the face-averaged normal velocity.
 // Binary::compute_*_flux's adjust_rho_fluxes (binary.cpp:1171-1235) has an
 // empty body (state_ztwd.cpp:445-480).  Block = one brick, thread per face.
+// T = double: the plain form.  T = float: the mixed form's reconstruction,
+// to_con and KT combination in FP32 from the FP64 primitives, the EOS in
+// FP64 (zt_eos_of), the fluxes and face velocities stored in FP64 for the
+// FP64 flux correction and conservative update.
 // ---------------------------------------------------------------------------
+template <typename T>
 __global__ void __launch_bounds__(128) k_zt_flux(Geom g, BrickTable bt, DevState st, ZtwdPar P,
                                                  const int* __restrict__ slots, int* err) {
     const int b = slots[blockIdx.x];
@@ -257,28 +264,34 @@ __global__ void __launch_bounds__(128) k_zt_flux(Geom g, BrickTable bt, DevState
         face_decode(d, nx, r, fi, t1, t2);
         pencil_of(g, d, t1, t2, base, stride);
         const int f = fi + bw;
-        double ql[ZT_NF], qr[ZT_NF], X[3];
+        T ql[ZT_NF], qr[ZT_NF], X[3];
         zt_face_states(g, W, base, stride, f, ql, qr);
-        face_X(g, bt, b, d, f, t1, t2, X);
+        {
+            double Xd[3];
+            face_X(g, bt, b, d, f, t1, t2, Xd);
+#pragma unroll
+            for (int e = 0; e < 3; e++) X[e] = T(Xd[e]);
+        }
         zt_to_con(P, ql, X);
         zt_to_con(P, qr, X);
-        double pl, csl, pr, csr;
-        zt_fail(err, zt_eos(P, ql, &pl, &csl));
-        zt_fail(err, zt_eos(P, qr, &pr, &csr));
-        const double al = fabs(zt_v(P, ql, X, d)) + csl;
-        const double ar = fabs(zt_v(P, qr, X, d)) + csr;
-        const double a = zmax(al, ar);
-        double avg[ZT_NF];
+        T pl, csl, pr, csr;
+        zt_fail(err, zt_eos_of(P, ql, &pl, &csl));
+        zt_fail(err, zt_eos_of(P, qr, &pr, &csr));
+        const T al = fabs(zt_v(P, ql, X, d)) + csl;
+        const T ar = fabs(zt_v(P, qr, X, d)) + csr;
+        const T a = al > ar ? al : ar;
+        T avg[ZT_NF];
 #pragma unroll
-        for (int l = 0; l < ZT_NF; l++) avg[l] = (ql[l] + qr[l]) * 0.5;
+        for (int l = 0; l < ZT_NF; l++) avg[l] = (ql[l] + qr[l]) * T(0.5);
         double* F = (d == 0 ? st.Fx : (d == 1 ? st.Fy : st.Fz)) + (size_t)b * g.nf * fstride;
         double* V = (d == 0 ? st.Vx : (d == 1 ? st.Vy : st.Vz)) + (size_t)b * fstride;
-        V[r] = zt_v(P, avg, X, d);
-        double fl[ZT_NF], fr[ZT_NF];
+        V[r] = double(zt_v(P, avg, X, d));
+        T fl[ZT_NF], fr[ZT_NF];
         zt_flux(P, ql, X, d, pl, fl);
         zt_flux(P, qr, X, d, pr, fr);
 #pragma unroll
-        for (int l = 0; l < ZT_NF; l++) F[l * fstride + r] = ((fl[l] + fr[l]) - (qr[l] - ql[l]) * a) * 0.5;
+        for (int l = 0; l < ZT_NF; l++)
+            F[l * fstride + r] = double(((fl[l] + fr[l]) - (qr[l] - ql[l]) * a) * T(0.5));
     }
 }
 
@@ -541,7 +554,10 @@ void launch_zt_flux(const Geom& g, const BrickTable& bt, const DevState& st, con
                     int n, int* err, cudaStream_t s) {
     if (n <= 0) return;
     launch_k(k_zt_prim, n, 256, 0, s, g, bt, st, P, slots);
-    launch_k(k_zt_flux, n, 128, 0, s, g, bt, st, P, slots, err);
+    if (g.flux32)
+        launch_k(k_zt_flux<float>, n, 128, 0, s, g, bt, st, P, slots, err);
+    else
+        launch_k(k_zt_flux<double>, n, 128, 0, s, g, bt, st, P, slots, err);
 }
 void launch_zt_max_dt(const Geom& g, const BrickTable& bt, const DevState& st, const ZtwdPar& P, const int* slots,
                       int n, double* dt_out, int* err, cudaStream_t s) {

@@ -1,6 +1,9 @@
 // The ZTWD binary state (binary/state_ztwd.cpp, binary/state.h) on one cell
-// or face, FP64, in the reference's operation order (include only from
-// translation units compiled without FMA contraction).
+// or face, in the reference's operation order (include only from
+// translation units compiled without FMA contraction).  The functions the
+// flux uses are templates over the arithmetic type T: FP64 in the plain
+// form (every cast below is then the identity), FP32 for the face states
+// and fluxes of the mixed form, whose EOS calls stay FP64 (zt_eos_of).
 //
 // Fields (state_ztwd.cpp:16-26): 0 rho, 1 rho_acc, 2 rho_don, 3 sr (radial
 // momentum), 4 lz (inertial angular momentum), 5 sz, 6 pot, 7 et, 8 tau
@@ -23,36 +26,44 @@ constexpr int ZT_D = 0, ZT_ACC = 1, ZT_DON = 2, ZT_SR = 3, ZT_LZ = 4, ZT_SZ = 5,
 // real.h max/min: a > b ? a : b / a > b ? b : a
 __device__ __forceinline__ double zmax(double a, double b) { return a > b ? a : b; }
 
-__device__ __forceinline__ double zt_R(const double* X) { return sqrt(X[0] * X[0] + X[1] * X[1]); }
+template <typename T>
+__device__ __forceinline__ T zt_R(const T* X) { return sqrt(X[0] * X[0] + X[1] * X[1]); }
 
 // State::A, State::Z (state_ztwd.cpp:33-45)
-__device__ __forceinline__ double zt_abar(const ZtwdPar& P, const double* u) {
-    double sum = 0.0;
+template <typename T>
+__device__ __forceinline__ T zt_abar(const ZtwdPar& P, const T* u) {
+    T sum = T(0.0);
 #pragma unroll
-    for (int i = 0; i < ZT_NSPECIES; i++) sum += u[ZT_SPECIE + i] / P.abar[i];
+    for (int i = 0; i < ZT_NSPECIES; i++) sum += u[ZT_SPECIE + i] / T(P.abar[i]);
     sum = u[ZT_D] / sum;
     return sum;
 }
 
 // State::st (:241-243): lz/R - rho R Omega
-__device__ __forceinline__ double zt_st(const ZtwdPar& P, const double* u, const double* X) {
-    return u[ZT_LZ] / zt_R(X) - u[ZT_D] * zt_R(X) * P.omega;
+template <typename T>
+__device__ __forceinline__ T zt_st(const ZtwdPar& P, const T* u, const T* X) {
+    return u[ZT_LZ] / zt_R(X) - u[ZT_D] * zt_R(X) * T(P.omega);
 }
-__device__ __forceinline__ double zt_vx(const ZtwdPar& P, const double* u, const double* X) {
+template <typename T>
+__device__ __forceinline__ T zt_vx(const ZtwdPar& P, const T* u, const T* X) {
     return (X[0] * u[ZT_SR] - X[1] * zt_st(P, u, X)) / zt_R(X) / u[ZT_D];
 }
-__device__ __forceinline__ double zt_vy(const ZtwdPar& P, const double* u, const double* X) {
+template <typename T>
+__device__ __forceinline__ T zt_vy(const ZtwdPar& P, const T* u, const T* X) {
     return (X[1] * u[ZT_SR] + X[0] * zt_st(P, u, X)) / zt_R(X) / u[ZT_D];
 }
-__device__ __forceinline__ double zt_vz(const double* u) { return u[ZT_SZ] / u[ZT_D]; }
+template <typename T>
+__device__ __forceinline__ T zt_vz(const T* u) { return u[ZT_SZ] / u[ZT_D]; }
 // normal velocity of direction d (State::vx/vy/vz, :249-267)
-__device__ __forceinline__ double zt_v(const ZtwdPar& P, const double* u, const double* X, int d) {
+template <typename T>
+__device__ __forceinline__ T zt_v(const ZtwdPar& P, const T* u, const T* X, int d) {
     return d == 0 ? zt_vx(P, u, X) : (d == 1 ? zt_vy(P, u, X) : zt_vz(u));
 }
 // State::ek (:158-160)
-__device__ __forceinline__ double zt_ek(const ZtwdPar& P, const double* u, const double* X) {
-    const double st = zt_st(P, u, X);
-    return 0.5 * (u[ZT_SR] * u[ZT_SR] + st * st + u[ZT_SZ] * u[ZT_SZ]) / u[ZT_D];
+template <typename T>
+__device__ __forceinline__ T zt_ek(const ZtwdPar& P, const T* u, const T* X) {
+    const T st = zt_st(P, u, X);
+    return T(0.5) * (u[ZT_SR] * u[ZT_SR] + st * st + u[ZT_SZ] * u[ZT_SZ]) / u[ZT_D];
 }
 // State::ei (:140-156): et - ek, or tau when that is below 0.001 et
 __device__ __forceinline__ double zt_ei(const ZtwdPar& P, const double* u, const double* X) {
@@ -72,21 +83,36 @@ __device__ __forceinline__ int zt_eos(const ZtwdPar& P, const double* u, double*
     return o.status;
 }
 
+// State::compute_eos in FP64 for a state held in T: the EOS inputs (rho,
+// T, the species mix) are widened to FP64 first
+template <typename T>
+__device__ __forceinline__ int zt_eos_of(const ZtwdPar& P, const T* u, T* p, T* cs) {
+    double w[ZT_NF];
+#pragma unroll
+    for (int l = 0; l < ZT_NF; l++) w[l] = double(u[l]);
+    double pd, csd;
+    const int st = zt_eos(P, w, &pd, &csd);
+    *p = T(pd);
+    *cs = T(csd);
+    return st;
+}
+
 // State::to_con (:560-585) at position X
-__device__ __forceinline__ void zt_to_con(const ZtwdPar& P, double* u, const double* X) {
-    const double R = zt_R(X);
+template <typename T>
+__device__ __forceinline__ void zt_to_con(const ZtwdPar& P, T* u, const T* X) {
+    const T R = zt_R(X);
     u[ZT_SZ] *= u[ZT_D];
     u[ZT_POT] *= u[ZT_D];
     u[ZT_SR] *= u[ZT_D];
-    u[ZT_LZ] += P.omega * R;
+    u[ZT_LZ] += T(P.omega) * R;
     u[ZT_LZ] *= u[ZT_D] * R;
     u[ZT_ET] += zt_ek(P, u, X);
-    double sum = 0.0;
+    T sum = T(0.0);
 #pragma unroll
     for (int i = 0; i < ZT_NSPECIES; i++) sum += u[ZT_SPECIE + i];
 #pragma unroll
     for (int i = 0; i < ZT_NSPECIES; i++) u[ZT_SPECIE + i] /= sum;
-    sum = 0.0;
+    sum = T(0.0);
     sum += u[ZT_DON];
     sum += u[ZT_ACC];
     u[ZT_DON] /= sum;
@@ -113,19 +139,19 @@ __device__ __forceinline__ void zt_to_prim(const ZtwdPar& P, double* u, const do
 }
 
 // State::x_flux / y_flux / z_flux (:360-396) for direction d with pressure p
-__device__ __forceinline__ void zt_flux(const ZtwdPar& P, const double* u, const double* X, int d, double p,
-                                        double* f) {
-    const double v = zt_v(P, u, X, d);
+template <typename T>
+__device__ __forceinline__ void zt_flux(const ZtwdPar& P, const T* u, const T* X, int d, T p, T* f) {
+    const T v = zt_v(P, u, X, d);
 #pragma unroll
     for (int i = 0; i < ZT_NF; i++) f[i] = v * u[i];
     if (d == 0) {
         f[ZT_SR] += X[0] * p / zt_R(X);
         f[ZT_LZ] -= X[1] * p;
-        f[ZT_ET] += (v + (-X[1] * (P.omega - P.omega0))) * p;
+        f[ZT_ET] += (v + (-X[1] * T(P.omega - P.omega0))) * p;
     } else if (d == 1) {
         f[ZT_SR] += X[1] * p / zt_R(X);
         f[ZT_LZ] += X[0] * p;
-        f[ZT_ET] += (v + X[0] * (P.omega - P.omega0)) * p;
+        f[ZT_ET] += (v + X[0] * T(P.omega - P.omega0)) * p;
     } else {
         f[ZT_SZ] += p;
         f[ZT_ET] += v * p;

@@ -49,7 +49,10 @@ extern "C" {
 #define AMR_RECON_PPM 1    /* Reconstruct::ppm (reconstruct.cpp:22-58), PPM builds; needs bw >= 3 */
 
 #define AMR_PREC_FP64 0  /* plain form: FP64 throughout, reference operation order */
-#define AMR_PREC_MIXED 1 /* FP32 flux/smoother inside FP64 state and defect correction */
+#define AMR_PREC_MIXED 1 /* FP32 KT reconstruction and flux (fluxes accumulated into the FP64 state; the
+                            Helmholtz EOS stays FP64) and the FP32 multigrid correction inside FP64
+                            defect correction */
+#define AMR_PREC_MIXED_SOLVE 2 /* the FP32 multigrid correction only; fluxes in FP64 */
 
 typedef struct amr_ctx amr_ctx;
 

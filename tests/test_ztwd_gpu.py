@@ -94,14 +94,16 @@ def test_ztwd_steps_match_reference(gpu, table_path, name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["ztwd_L2", "ztwd12_L2"])
-def test_ztwd_mixed_persistent_close_to_fp64(gpu, table_path, name):
-    """FP32 multigrid correction in the persistent solve, against the FP64
-    form after the same steps: same trees and steps, density and energy
-    within MIXED_RTOL (relative L1)."""
+@pytest.mark.parametrize("prec", ["PREC_MIXED", "PREC_MIXED_SOLVE"])
+def test_ztwd_mixed_persistent_close_to_fp64(gpu, table_path, name, prec):
+    """The mixed forms in the persistent solve -- FP32 multigrid correction,
+    with (PREC_MIXED) or without (PREC_MIXED_SOLVE) the FP32 reconstruction
+    and KT flux -- against the FP64 form after the same steps: same trees and
+    steps, density and energy within MIXED_RTOL (relative L1)."""
     g = load_golden(name)
     nsteps = int(g["args"][1])
     a = make(gpu, g, table_path)
-    b = make(gpu, g, table_path, precision=gpu.PREC_MIXED, persistent_solve=2)
+    b = make(gpu, g, table_path, precision=getattr(gpu, prec), persistent_solve=2)
     run(a, nsteps)
     run(b, nsteps)
     assert same_tree(b.get_tree(), {"final_" + k: v for k, v in a.get_tree().items()}, "final_")
