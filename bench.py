@@ -48,7 +48,7 @@ ZT_NX = 12  # interior cells per brick edge of the BINARY build (binary/binary_d
 ZT_TOL = 1.0e-7  # ELL_TOLER of the BINARY build (binary/binary_defs.h:64)
 ZT_STEPS_TOTAL = 100
 DYNAMIC_RANGE = 1.0e6
-REF_CXXFLAGS = "g++ -O2 -fopenmp -ffp-contract=off"  # oracle/build_ref.py CXXFLAGS
+REF_CXXFLAGS = "g++ -O3 -fopenmp -ffp-contract=off"  # oracle/build_ref.py CXXFLAGS
 METRIC = "cell-updates/s (hydro+gravity step), 1 B200: mixed+batched vs FP64 at set error"
 UNIT = "cell-updates/s"
 WORKLOAD = "single star: n=1.5 polytrope, 4 levels, RK3 hydro + multigrid gravity (L1 tol 1e-6)"
@@ -148,7 +148,7 @@ class ClockSampler:
 
 def run_reference_steps(levels, threads, warm, steps, timeout=3000):
     """The reference's own CPU code (oracle/_ref, built from the reference
-    sources, g++ -O2 -fopenmp) on the same workload: `warm` untimed RK3 steps
+    sources, g++ -O3 -fopenmp) on the same workload: `warm` untimed RK3 steps
     (the first includes the initial solve from phi = 0), then `steps` timed
     steps.  Returns per-step seconds, leaf cells and bricks."""
     exe = os.path.join(ROOT, "oracle", "_ref", "g05_harness")
@@ -178,7 +178,7 @@ def ztwd_harness(nx):
 
 
 def run_reference_ztwd(threads, warm, steps, nx=ZT_NX, timeout=1500):
-    """The reference's BINARY build (oracle/_ref, g++ -O2 -fopenmp) on the
+    """The reference's BINARY build (oracle/_ref, g++ -O3 -fopenmp) on the
     headline workload: `warm` untimed BinaryDriver steps (the first solves
     from the initial potential), then `steps` timed ones."""
     exe = ztwd_harness(nx)
@@ -245,7 +245,7 @@ def reference_arm_single_star(args):
         return 0
     t = sum(s["seconds"])
     value = sum(s["leaf_cells"]) / t
-    sample = ("reference CPU code (oracle/_ref, g++ -O2 -fopenmp, %d threads): %d full RK3 steps after %d "
+    sample = ("reference CPU code (oracle/_ref, g++ -O3 -fopenmp, %d threads): %d full RK3 steps after %d "
               "untimed (the first solves from phi = 0), %d bricks, %.1f V-cycles/step" %
               (s["threads"], len(s["seconds"]), warm, s["bricks"], sum(s["vcycles"]) / len(s["vcycles"])))
     out = {

@@ -8,7 +8,7 @@ that links Silo.  This recipe
      oracle/_ref/src_<variant>/ (the sources are never committed),
   2. applies the minimal scripted patches listed in PATCHES below,
   3. compiles the reference's own grid/, oct_node/, euler/, poisson/ sources
-     together with the harness in oracle/harness/ using g++ -O2 -fopenmp
+     together with the harness in oracle/harness/ using g++ -O3 -fopenmp
      -ffp-contract=off (no FMA contraction, like the reference's x86-64 build),
   4. writes the executables to oracle/_ref/<variant>_harness.
 
@@ -69,7 +69,7 @@ BINARY_SOURCES = COMMON_SOURCES + [
     "helmholtz/helmeos.cpp",
 ]
 
-CXXFLAGS = ["-O2", "-fopenmp", "-ffp-contract=off", "-DNDEBUG", "-w"]
+CXXFLAGS = ["-O3", "-fopenmp", "-ffp-contract=off", "-DNDEBUG", "-w"]
 
 
 def _replace(path, old, new, count=1):
