@@ -350,7 +350,9 @@ void launch_forces(const Geom& g, const BrickTable& bt, const DevState& st, cons
     if (n > 0) launch_k(k_forces, n, 256, 0, s, g, bt, st, slots);
 }
 void launch_adjust_force(const Geom& g, const DevState& st, const RefluxItem* items, int n, cudaStream_t s) {
-    if (n > 0) launch_k(k_adjust_force, n, 32, 0, s, g, st, items);
+    // one thread per coarse face of the item's quadrant: (nx/2)^2 of them
+    const int half = (g.pnx - 2) / 2;
+    if (n > 0) launch_k(k_adjust_force, n, ((half * half + 31) / 32) * 32, 0, s, g, st, items);
 }
 void launch_solution_error(const Geom& g, const BrickTable& bt, const DevState& st, const int* slots, int n,
                            double* out, cudaStream_t s) {

@@ -11,9 +11,15 @@ covered cells (grid_node.cpp:1035-1074) and the regrid's prolongation
 round-off for every field without a source:
 
 * the Euler blast (no gravity): mass, the three momenta and the energy;
-* the self-gravitating star and the ZTWD binary: the mass (the momenta and
-  energies have the gravity sources; the binary's angular momentum and
-  radial momentum the rotating frame's).
+* the self-gravitating star: the mass (the momenta and energy have the
+  gravity sources).
+
+The ZTWD binary is not conservative in the reference itself: State::floor
+(binary/state_ztwd.cpp:482-554) raises the density of evacuated cells to
+rho_floor, which adds mass (3.2e-9 of the total over the 9 steps of ztwd_L3,
+1.4e-9 for ztwd12_L3, computed from the reference's own initial and final
+states in the goldens).  There the test holds the library's drift of the
+total density and of the two stars' densities to the reference's drift.
 
 The bound is round-off: 1e-13 of the field's total absolute content
 (sum |u| dV) per step.
@@ -106,23 +112,50 @@ def test_self_gravitating_star_conserves_mass(gpu):
     a.close()
 
 
+def reference_drift(g, fields):
+    """state_sum + FO of the reference's final state minus its initial one,
+    from a golden holding both states per cell, over sum |u| dV."""
+    nx = int(g["nx"])
+    half = nx // 2
+    idx = np.arange(nx) // half
+    oc = idx[None, None, :] | (idx[None, :, None] << 1) | (idx[:, None, None] << 2)
+
+    def tot(prefix):
+        h = 2.0 * 1.0 / nx / 2.0 ** g[prefix + "level"]
+        leaf = ((g[prefix + "child_mask"][:, None, None, None] >> oc[None]) & 1) == 0
+        vol = (h ** 3)[:, None, None, None] * leaf
+        U = g[prefix + "U"]
+        return (np.array([(U[:, f] * vol).sum() for f in fields]) + g[prefix + "FO"][fields],
+                np.array([(np.abs(U[:, f]) * vol).sum() for f in fields]))
+
+    m0, s0 = tot("init_")
+    m1, _ = tot("final_")
+    return (m1 - m0) / s0
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["ztwd_L3", "ztwd12_L3"])
-def test_ztwd_binary_conserves_mass(gpu, table_path, name):
-    """Total density and the two stars' tracer densities over the binary's
-    steps, across its step-8 regrid, plain FP64 and mixed persistent."""
+def test_ztwd_binary_mass_drift_is_the_references(gpu, table_path, name):
+    """Total density and the two stars' densities over the binary's steps
+    (regrids at steps 0 and 8): the change of state_sum + FO equals the
+    reference's own (its density floor adds mass) to round-off in the plain
+    FP64 form, and to 1e-3 of it in the mixed form (FP32 fluxes stay
+    conservative; only the floored cells differ)."""
     g = load_golden(name)
     n = int(g["args"][1])
+    fields = [0, 1, 2]
+    ref = reference_drift(g, fields)
     for kw in ({}, {"precision": gpu.PREC_MIXED, "persistent_solve": 2}):
         a = make_ztwd(gpu, g, table_path, **kw)
-        state = {"last": 0.0}
-
-        def step(s):
+        m0, s0 = totals(a, fields)
+        last = 0.0
+        for s in range(n):
             dt = a.max_dt()
             if s > 0:
-                dt = min(1.25 * state["last"], dt)
-            state["last"] = a.ztwd_step(dt, ELL_TOLER, DYNAMIC_RANGE, s)
-
-        worst = check_run(a, step, n, [0, 1, 2])
-        assert np.all(worst <= ROUNDOFF_PER_STEP * n), (kw, worst)
+                dt = min(1.25 * last, dt)
+            last = a.ztwd_step(dt, ELL_TOLER, DYNAMIC_RANGE, s)
+        m1, _ = totals(a, fields)
+        drift = (m1 - m0) / s0
+        tol = ROUNDOFF_PER_STEP * n + (1e-3 * np.abs(ref) if kw else 0.0)
+        assert np.all(np.abs(drift - ref) <= tol), (kw, drift, ref)
         a.close()
