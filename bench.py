@@ -800,6 +800,73 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL, n
     return res
 
 
+def run_error_study(amr, ini, torch, nx=ZT_NX, total=ZT_STEPS_TOTAL, snaps=(1, 10, 100)):
+    """What the mixed forms' potential error means: trajectories of the binary
+    over `total` steps in
+      fp64          the plain FP64 result (persistent FP64 form, bitwise the
+                    plain form) at the reference's tolerance ELL_TOLER
+      fp64_perturbed the same with the initial density scaled by (1 + 1e-15):
+                    how far round-off alone moves the trajectory
+      fp64_tight    FP64 with the solve converged 10^4 times further (L1
+                    tolerance ELL_TOLER / 1e4): the FP64 form's own solver
+                    error at ELL_TOLER is fp64 against this one
+      mixed         AMR_PREC_MIXED (FP32 flux and FP32 correction)
+      mixed_solve   AMR_PREC_MIXED_SOLVE (FP32 correction, FP64 flux)
+    and their potential relative L2 and density relative L1 differences at
+    the snapshot steps.  ms per step is the mean device time per step."""
+    helm_table = _load_module("helm_table", os.path.join(PKG, "helm_table.py"))
+    helm_mod = _load_module("helm_b200", os.path.join(PKG, "helm.py"))
+    tdir = tempfile.mkdtemp(prefix="ztwd_err_")
+    table = helm_table.ensure_table(tdir)
+    runs = (("fp64", amr.PREC_FP64, ZT_TOL, False), ("fp64_perturbed", amr.PREC_FP64, ZT_TOL, True),
+            ("fp64_tight", amr.PREC_FP64, ZT_TOL * 1e-4, False), ("mixed", amr.PREC_MIXED, ZT_TOL, False),
+            ("mixed_solve", amr.PREC_MIXED_SOLVE, ZT_TOL, False))
+    out = {"nx": nx, "steps": total, "tol_l1": ZT_TOL, "runs": {}}
+    shots = {}
+    for name, prec, tol, perturb in runs:
+        a = ztwd_context(amr, ini, helm_mod, table, ZT_LEVELS, prec, 2, nx=nx)
+        if perturb:
+            U = a.download_state()
+            U[:, 0] *= 1.0 + 1e-15
+            a.upload_state(U)
+        stream = torch.cuda.ExternalStream(a.stream_handle())
+        last, ms = 0.0, []
+        for s in range(total):
+            dt = a.max_dt()
+            if s > 0:
+                dt = min(1.25 * last, dt)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            last = a.ztwd_step(dt, tol, DYNAMIC_RANGE, s)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            if s + 1 in snaps:
+                t = a.get_tree()
+                b = a.bw
+                shots[(name, s + 1)] = {"rho": a.download_state()[:, 0, b:-b, b:-b, b:-b].copy(),
+                                        "phi": a.download_poisson()[0][:, 1:-1, 1:-1, 1:-1].copy(),
+                                        "level": t["level"], "loc": t["loc"]}
+        out["runs"][name] = {"tol_l1": tol, "ms_per_step": statistics.mean(ms[3:]) if total > 3 else None,
+                             "bricks": a.nbricks}
+        a.close()
+    import shutil
+    shutil.rmtree(tdir, ignore_errors=True)
+
+    def diff(x, y):
+        if not (np.array_equal(x["level"], y["level"]) and np.array_equal(x["loc"], y["loc"])):
+            return None
+        return {"phi_rel_l2": float(np.linalg.norm(x["phi"] - y["phi"]) / np.linalg.norm(y["phi"])),
+                "rho_rel_l1": float(np.abs(x["rho"] - y["rho"]).sum() / np.abs(y["rho"]).sum())}
+
+    pairs = {"mixed_vs_fp64": ("mixed", "fp64"), "mixed_solve_vs_fp64": ("mixed_solve", "fp64"),
+             "fp64_vs_fp64_tight": ("fp64", "fp64_tight"), "mixed_vs_fp64_tight": ("mixed", "fp64_tight"),
+             "fp64_perturbed_vs_fp64": ("fp64_perturbed", "fp64")}
+    out["differences"] = {k: {str(s): diff(shots[(x, s)], shots[(y, s)]) for s in snaps}
+                          for k, (x, y) in pairs.items()}
+    return out
+
+
 def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
     """The headline: W untimed then K timed BinaryDriver steps of the 5-level
     ZTWD binary in the mixed persistent form (L2 flushed between timed steps,
@@ -1107,6 +1174,9 @@ def main():
     ap.add_argument("--sections", action="store_true",
                     help="also run the secondary sections (single star, random-field octree substep, Helmholtz "
                          "EOS) and write them with the binary's details to the --json-out sidecar")
+    ap.add_argument("--error-study", action="store_true",
+                    help="also run the binary's error study (FP64 at a tight tolerance, round-off perturbation, "
+                         "both mixed forms over 100 steps) into the --json-out sidecar")
     ap.add_argument("--json-out", default=None,
                     help="sidecar JSON file: the headline line plus the binary's per-form details and, with "
                          "--sections, the secondary sections")
@@ -1138,6 +1208,8 @@ def main():
     if rank == 0 and not args.no_compare:
         ztwd = run_ztwd(amr, ini, torch, args.steps, max(args.warmup, 3), not args.no_cpu_baseline, nx=nx)
     sections = {}
+    if rank == 0 and args.error_study:
+        sections["error_study"] = run_error_study(amr, ini, torch, nx=nx)
     if rank == 0 and args.sections:
         sections["single_star"] = run_single_star(amr, ini, args, world, local, torch, dist)
         sections["batched_substep"] = run_batched_substep(amr, ini, torch, max(args.steps, 3), max(args.warmup, 3))
