@@ -138,6 +138,9 @@ def load_library(path=LIB_PATH):
                 lib.amr_relax_passes.argtypes = [P, ctypes.POINTER(ctypes.c_longlong), I]
             if hasattr(lib, "amr_set_wait_limit"):
                 lib.amr_set_wait_limit.argtypes = [P, I]
+            lib.amr_set_solve_layout.argtypes = [P, I, I]
+            lib.amr_get_solve_layout.argtypes = [P, ip, ip, ip, ip, ip]
+            lib.amr_autotune_solve.argtypes = [P, D, I, I, dp, I, ip, ip]
         _lib = lib
     return _lib
 
@@ -444,6 +447,24 @@ class AMR:
         n = ctypes.c_longlong()
         self._check(self.lib.amr_solve_totals(self.ctx, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+    def set_solve_layout(self, layout, blocks_per_sm=0):
+        self._check(self.lib.amr_set_solve_layout(self.ctx, int(layout), int(blocks_per_sm)))
+
+    def solve_layout(self):
+        """(layout, blocks per SM cap, threads per block, blocks, layouts of this brick size)"""
+        v = [ctypes.c_int() for _ in range(5)]
+        self._check(self.lib.amr_get_solve_layout(self.ctx, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def autotune_solve(self, tol, max_cycles=10000, reps=2):
+        """Times the persistent solve in every layout and blocks-per-SM cap,
+        keeps the fastest; returns (per-trial ms or None, best trial)."""
+        ms = np.zeros(16)
+        nt, best = ctypes.c_int(), ctypes.c_int()
+        self._check(self.lib.amr_autotune_solve(self.ctx, float(tol), int(max_cycles), int(reps), _dptr(ms), 16,
+                                                ctypes.byref(nt), ctypes.byref(best)))
+        return [None if m < 0 else float(m) for m in ms[:nt.value]], best.value
 
     def set_wait_limit(self, polls):
         """Polls per bounded wait of the persistent solve (0: the default)."""

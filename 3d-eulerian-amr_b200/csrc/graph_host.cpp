@@ -65,6 +65,9 @@ struct GraphState {
     // persistent solve: cooperative blocks, [3][cap] per-brick sums,
     // [blocks][cap] nested-sum scratch, barrier word
     int pblocks = 0;
+    int layout = 0;        // block layout of the solve kernel (solve_layout_threads)
+    int per_sm = 0;        // blocks per SM cap of the launch (0: as many as fit)
+    int pnest_blocks = 0;  // blocks d_pnest has room for (the most of any layout)
     double* d_pres3 = nullptr;
     double* d_pnest = nullptr;
     GridBarrier* d_bar = nullptr;
@@ -99,13 +102,18 @@ int ensure_state(amr_ctx* c) {
     CUDA_TRY(cudaMalloc(&g->d_counter, sizeof(unsigned int) * 4));
     CUDA_TRY(cudaMemsetAsync(g->d_counter, 0, sizeof(unsigned int) * 4, c->stream));
     if (c->cfg.persistent_solve) {
-        g->pblocks = solve_persistent_blocks(c->geom.nx, c->geom.precision, c->cfg.persistent_solve);
+        g->layout = 0;
+        g->per_sm = c->cfg.persistent_solve;
+        g->pblocks = solve_persistent_blocks(c->geom.nx, c->geom.precision, g->per_sm, g->layout);
         if (g->pblocks <= 0) {
             c->err = "no cooperative launch configuration for the persistent solve";
             return AMR_ERR_CUDA;
         }
+        g->pnest_blocks = g->pblocks;
+        for (int l = 0; l < solve_layouts(c->geom.nx); l++)
+            g->pnest_blocks = std::max(g->pnest_blocks, solve_persistent_blocks(c->geom.nx, c->geom.precision, 0, l));
         CUDA_TRY(cudaMalloc(&g->d_pres3, sizeof(double) * 3 * (size_t)c->cap));
-        CUDA_TRY(cudaMalloc(&g->d_pnest, sizeof(double) * (size_t)g->pblocks * c->cap));
+        CUDA_TRY(cudaMalloc(&g->d_pnest, sizeof(double) * (size_t)g->pnest_blocks * c->cap));
         CUDA_TRY(cudaMalloc(&g->d_bar, sizeof(GridBarrier)));
         CUDA_TRY(cudaMalloc(&g->d_rpub, sizeof(unsigned) * (size_t)c->cap));
         CUDA_TRY(cudaEventCreate(&g->ev_ps[0]));
@@ -312,7 +320,7 @@ int rec_persistent(amr_ctx* c, cudaStream_t s, double tol) {
     // event nodes bracketing the launch: the elapsed time of the latest
     // replay is the kernel's duration on this stream
     CUDA_TRY(cudaEventRecordWithFlags(g->ev_ps[0], s, cudaEventRecordExternal));
-    CUDA_TRY(launch_solve_persistent(a, g->pblocks, s));
+    CUDA_TRY(launch_solve_persistent(a, g->pblocks, g->layout, s));
     CUDA_TRY(cudaEventRecordWithFlags(g->ev_ps[1], s, cudaEventRecordExternal));
     g->k_vbody = 0;
     g->k_rbody = 0;
@@ -594,6 +602,112 @@ int amr_solve_last_ms(amr_ctx* c, float* ms) {
     CUDA_TRY(cudaEventSynchronize(c->gs->ev_ps[1]));
     CUDA_TRY(cudaEventElapsedTime(ms, c->gs->ev_ps[0], c->gs->ev_ps[1]));
     return AMR_OK;
+}
+
+// Block layout of the persistent solve kernel: layout (0 .. count-1 of the
+// brick size's layouts) and blocks per SM (0: as many as fit).  Every layout
+// gives the same results bit for bit; the captured graphs are re-captured
+// with the new launch at their next call.
+int amr_set_solve_layout(amr_ctx* c, int layout, int blocks_per_sm) {
+    TRY(need(c));
+    GraphState* g = c->gs;
+    if (!c->cfg.persistent_solve) {
+        c->err = "solve layouts belong to the persistent solve (amr_config.persistent_solve > 0)";
+        return AMR_ERR_STATE;
+    }
+    if (layout < 0 || layout >= solve_layouts(c->geom.nx) || blocks_per_sm < 0) return AMR_ERR_ARG;
+    const int nb = solve_persistent_blocks(c->geom.nx, c->geom.precision, blocks_per_sm, layout);
+    if (nb <= 0 || nb > g->pnest_blocks) {
+        c->err = "no cooperative launch configuration for this layout";
+        return AMR_ERR_ARG;
+    }
+    g->layout = layout;
+    g->per_sm = blocks_per_sm;
+    g->pblocks = nb;
+    g->solve_version = -1;
+    g->step_version = -1;
+    return AMR_OK;
+}
+
+int amr_get_solve_layout(amr_ctx* c, int* layout, int* blocks_per_sm, int* threads, int* blocks, int* count) {
+    TRY(need(c));
+    GraphState* g = c->gs;
+    if (layout) *layout = g->layout;
+    if (blocks_per_sm) *blocks_per_sm = g->per_sm;
+    if (threads) *threads = solve_layout_threads(c->geom.nx, g->layout);
+    if (blocks) *blocks = g->pblocks;
+    if (count) *count = solve_layouts(c->geom.nx);
+    return AMR_OK;
+}
+
+// Times one persistent solve (to L1 tolerance tol) from the context's
+// current potential in every layout and blocks-per-SM cap (1, 2, as many as
+// fit) of its brick size -- reps timed solves each after an untimed one,
+// the potential restored before every solve -- keeps the fastest and leaves
+// the potential as it was.  ms[t] receives the mean time of trial t
+// (layout = t / 3, cap = 1, 2, 0 for t % 3; a negative value where the
+// trial gives the same launch as an earlier one or has none); *ntrials the
+// trials (3 per layout), *best the fastest.
+int amr_autotune_solve(amr_ctx* c, double tol, int max_cycles, int reps, double* ms, int ms_cap, int* ntrials,
+                       int* best) {
+    TRY(need(c));
+    GraphState* g = c->gs;
+    if (!c->cfg.persistent_solve) {
+        c->err = "the autotuner times the persistent solve (amr_config.persistent_solve > 0)";
+        return AMR_ERR_STATE;
+    }
+    if (reps < 1 || max_cycles < 1) return AMR_ERR_ARG;
+    const int nl = solve_layouts(c->geom.nx);
+    const int caps[3] = {1, 2, 0};
+    const int nt = 3 * nl;
+    if (ntrials) *ntrials = nt;
+    const size_t bytes = sizeof(double) * (size_t)c->cap * c->geom.pnx3;
+    double* saved = nullptr;
+    CUDA_TRY(cudaMalloc(&saved, bytes));
+    CUDA_TRY(cudaMemcpyAsync(saved, c->st.phi, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    const int l0 = g->layout, p0 = g->per_sm;
+    double best_ms = 1e300;
+    int best_t = -1;
+    int rc = AMR_OK;
+    std::vector<std::pair<int, int>> seen;  // (layout, blocks)
+    for (int t = 0; t < nt && rc == AMR_OK; t++) {
+        const int l = t / 3, cap = caps[t % 3];
+        const int nb = solve_persistent_blocks(c->geom.nx, c->geom.precision, cap, l);
+        double mean = -1.0;
+        bool dup = nb <= 0 || nb > g->pnest_blocks;
+        for (auto& q : seen) dup = dup || (q.first == l && q.second == nb);
+        if (!dup) {
+            seen.push_back({l, nb});
+            rc = amr_set_solve_layout(c, l, cap);
+            double sum = 0.0;
+            for (int r = 0; r <= reps && rc == AMR_OK; r++) {
+                if (cudaMemcpyAsync(c->st.phi, saved, bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess) {
+                    rc = AMR_ERR_CUDA;
+                    break;
+                }
+                rc = amr_graph_solve(c, tol, max_cycles, nullptr, nullptr);
+                float one = 0.0f;
+                if (rc == AMR_OK) rc = amr_solve_last_ms(c, &one);
+                if (r > 0) sum += one;
+            }
+            mean = sum / reps;
+            if (rc == AMR_OK && mean < best_ms) {
+                best_ms = mean;
+                best_t = t;
+            }
+        }
+        if (ms && t < ms_cap) ms[t] = mean;
+    }
+    if (cudaMemcpyAsync(c->st.phi, saved, bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess && rc == AMR_OK)
+        rc = AMR_ERR_CUDA;
+    cudaStreamSynchronize(c->stream);
+    cudaFree(saved);
+    if (rc != AMR_OK) {
+        amr_set_solve_layout(c, l0, p0);
+        return rc;
+    }
+    if (best) *best = best_t;
+    return amr_set_solve_layout(c, best_t / 3, caps[best_t % 3]);
 }
 
 // The Poisson solve as one graph launch (see amr_poisson_solve).

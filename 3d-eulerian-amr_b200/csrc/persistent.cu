@@ -122,21 +122,25 @@ __device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& 
 }
 
 // Block layout of the solve for bricks of NX^3 interior cells: TPB threads
-// (the relaxation layout of one brick per block); with 8^3 bricks a block
-// relaxes two bricks at once (one per half) on levels with more bricks
-// than blocks, so it holds two staged bricks.
-template <int NX>
+// per block, NX^3 / TPB cells per thread in the relaxation (every layout
+// gives the same results bit for bit).  With 8^3 bricks and 512 threads a
+// block relaxes two bricks at once (one per half) on levels with more
+// bricks than blocks, so it holds two staged bricks; the other layouts take
+// such levels brick by brick.  MINB: blocks per SM the registers are
+// budgeted for.
+template <int NX, int TPB_>
 struct SolveLayout {
-    static constexpr int TPB = RelaxThreads<NX>::value;
-    static constexpr bool HALVES = NX == 8;
+    static constexpr int TPB = TPB_;
+    static constexpr bool HALVES = NX == 8 && TPB == 512;
     static constexpr int NSM = HALVES ? 2 : 1;
+    static constexpr int MINB = TPB >= 864 ? 1 : (TPB > 288 ? 2 : (TPB > 256 ? 3 : 4));
     // threads per face in the face-ghost phases
     static constexpr int PF = NX * NX <= TPB / 6 ? NX * NX : TPB / 6;
 };
 
-template <int NX, typename CT>
+template <int NX, int TPB_, typename CT>
 struct Solver {
-    using Lay = SolveLayout<NX>;
+    using Lay = SolveLayout<NX, TPB_>;
     static constexpr int TPB = Lay::TPB;
     const SolveArgs& a;
     RelaxSmem<NX, CT>* sm;  // Lay::NSM staged bricks
@@ -224,7 +228,7 @@ struct Solver {
                                            BlockSync{});
                 __syncthreads();
             });
-        } else {
+        } else if constexpr (Lay::HALVES) {
             constexpr int HT = TPB / 2;
             const int h = threadIdx.x / HT, lt = threadIdx.x % HT;
             for (int q = 2 * blockIdx.x + h; q < n; q += 2 * gridDim.x) {
@@ -619,8 +623,8 @@ struct Solver {
     }
 };
 
-template <int NX, typename CT>
-__global__ void __launch_bounds__(SolveLayout<NX>::TPB, 2) k_solve_persistent(SolveArgs a) {
+template <int NX, int TPB, typename CT>
+__global__ void __launch_bounds__(TPB, SolveLayout<NX, TPB>::MINB) k_solve_persistent(SolveArgs a) {
     // the staged bricks live in dynamic shared memory
     RelaxSmem<NX, CT>* sm = reinterpret_cast<RelaxSmem<NX, CT>*>(dyn_smem());
     __shared__ double red[16];
@@ -631,8 +635,8 @@ __global__ void __launch_bounds__(SolveLayout<NX>::TPB, 2) k_solve_persistent(So
     const int max_cycles = *(volatile int*)&a.ctl->max_cycles;
     // the third brick buffer: the second half's staging buffer where the
     // layout has one, else the dynamic shared memory after the staged brick
-    CT* xbuf = SolveLayout<NX>::NSM == 2 ? sm[1].buf[0] : reinterpret_cast<CT*>(sm + 1);
-    Solver<NX, CT> s{a, sm, xbuf, red, nbuf, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0,
+    CT* xbuf = SolveLayout<NX, TPB>::NSM == 2 ? sm[1].buf[0] : reinterpret_cast<CT*>(sm + 1);
+    Solver<NX, TPB, CT> s{a, sm, xbuf, red, nbuf, a.nest + (size_t)blockIdx.x * a.L.cap, 0, 0, 0,
                  *(volatile int*)&a.ctl->max_outer};
     __shared__ unsigned long long s_ph_ns[PH_COUNT];
     __shared__ unsigned s_ph_n[PH_COUNT];
@@ -650,7 +654,7 @@ __global__ void __launch_bounds__(SolveLayout<NX>::TPB, 2) k_solve_persistent(So
     s.ph_bytes = s_ph_bytes;
     s.ph_wait = s_ph_wait;
     if (threadIdx.x < PH_COUNT + 2) s_ph_wait[threadIdx.x] = 0;
-    s.t_last = Solver<NX, CT>::now();
+    s.t_last = Solver<NX, TPB, CT>::now();
     if (threadIdx.x < PH_COUNT) {
         s_ph_ns[threadIdx.x] = 0;
         s_ph_n[threadIdx.x] = 0;
@@ -699,61 +703,104 @@ __global__ void __launch_bounds__(SolveLayout<NX>::TPB, 2) k_solve_persistent(So
 
 }  // namespace
 
-template <int NX, typename CT>
+template <int NX, int TPB, typename CT>
 constexpr size_t solve_smem() {
-    return SolveLayout<NX>::NSM * sizeof(RelaxSmem<NX, CT>) +
-           (SolveLayout<NX>::NSM == 1 ? sizeof(CT) * (NX + 2) * (NX + 2) * (NX + 2) : 0);
+    using Lay = SolveLayout<NX, TPB>;
+    return Lay::NSM * sizeof(RelaxSmem<NX, CT>) + (Lay::NSM == 1 ? sizeof(CT) * (NX + 2) * (NX + 2) * (NX + 2) : 0);
+}
+
+namespace {
+
+// The layouts of each brick size, in the order of their layout number.
+constexpr int LAYOUTS_8[] = {512, 256};
+constexpr int LAYOUTS_12[] = {576, 864, 288};
+
+template <int NX, int TPB, typename CT>
+cudaError_t set_attr() {
+    return cudaFuncSetAttribute((const void*)k_solve_persistent<NX, TPB, CT>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem<NX, TPB, CT>());
+}
+template <int NX, int TPB, typename CT>
+int occupancy() {
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_persistent<NX, TPB, CT>, TPB,
+                                                      solve_smem<NX, TPB, CT>()) != cudaSuccess)
+        return -1;
+    return per;
+}
+template <int NX, int TPB, typename CT>
+cudaError_t launch(const SolveArgs& a, int blocks, cudaStream_t s) {
+    void* args[] = {const_cast<SolveArgs*>(&a)};
+    return cudaLaunchCooperativeKernel((const void*)k_solve_persistent<NX, TPB, CT>, dim3(blocks), dim3(TPB), args,
+                                       solve_smem<NX, TPB, CT>(), s);
+}
+
+// Calls OP<NX, TPB, CT>::run(args...) for the layout (nx, layout, FP32?);
+// returns `bad` for an unknown one.
+#define AMR_SOLVE_DISPATCH(nx, layout, f32, bad, CALL)                  \
+    do {                                                                \
+        if ((nx) == 8) {                                                \
+            if ((layout) == 0) return (f32) ? CALL(8, 512, float) : CALL(8, 512, double);   \
+            if ((layout) == 1) return (f32) ? CALL(8, 256, float) : CALL(8, 256, double);   \
+        } else if ((nx) == 12) {                                        \
+            if ((layout) == 0) return (f32) ? CALL(12, 576, float) : CALL(12, 576, double); \
+            if ((layout) == 1) return (f32) ? CALL(12, 864, float) : CALL(12, 864, double); \
+            if ((layout) == 2) return (f32) ? CALL(12, 288, float) : CALL(12, 288, double); \
+        }                                                               \
+        return (bad);                                                   \
+    } while (0)
+
+#define AMR_OCC(NX, TPB, CT) occupancy<NX, TPB, CT>()
+#define AMR_LAUNCH(NX, TPB, CT) launch<NX, TPB, CT>(a, blocks, s)
+
+int occupancy_of(int nx, int layout, bool f32) { AMR_SOLVE_DISPATCH(nx, layout, f32, -1, AMR_OCC); }
+
+}  // namespace
+
+int solve_layouts(int nx) {
+    return nx == 8 ? (int)(sizeof(LAYOUTS_8) / sizeof(int)) : nx == 12 ? (int)(sizeof(LAYOUTS_12) / sizeof(int)) : 0;
+}
+
+int solve_layout_threads(int nx, int layout) {
+    if (layout < 0 || layout >= solve_layouts(nx)) return -1;
+    return nx == 8 ? LAYOUTS_8[layout] : LAYOUTS_12[layout];
 }
 
 int solve_persistent_attributes() {
     cudaError_t e = cudaSuccess;
-    auto set = [&](const void* f, size_t bytes) {
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    auto chk = [&](cudaError_t r) {
+        if (e == cudaSuccess) e = r;
     };
-    set((const void*)k_solve_persistent<8, float>, solve_smem<8, float>());
-    set((const void*)k_solve_persistent<8, double>, solve_smem<8, double>());
-    set((const void*)k_solve_persistent<12, float>, solve_smem<12, float>());
-    set((const void*)k_solve_persistent<12, double>, solve_smem<12, double>());
+    chk(set_attr<8, 512, float>());
+    chk(set_attr<8, 512, double>());
+    chk(set_attr<8, 256, float>());
+    chk(set_attr<8, 256, double>());
+    chk(set_attr<12, 576, float>());
+    chk(set_attr<12, 576, double>());
+    chk(set_attr<12, 864, float>());
+    chk(set_attr<12, 864, double>());
+    chk(set_attr<12, 288, float>());
+    chk(set_attr<12, 288, double>());
     return e == cudaSuccess ? 0 : -1;
 }
 
-namespace {
-template <int NX, typename CT>
-int occupancy() {
-    int per = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_solve_persistent<NX, CT>, SolveLayout<NX>::TPB,
-                                                      solve_smem<NX, CT>()) != cudaSuccess)
-        return -1;
-    return per;
-}
-template <int NX, typename CT>
-cudaError_t launch(const SolveArgs& a, int blocks, cudaStream_t s) {
-    void* args[] = {const_cast<SolveArgs*>(&a)};
-    return cudaLaunchCooperativeKernel((const void*)k_solve_persistent<NX, CT>, dim3(blocks),
-                                       dim3(SolveLayout<NX>::TPB), args, solve_smem<NX, CT>(), s);
-}
-}  // namespace
-
-int solve_persistent_blocks(int nx, int precision, int per_sm_cap) {
+int solve_persistent_blocks(int nx, int precision, int per_sm_cap, int layout) {
     int dev = 0, sms = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return -1;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-    const bool f32 = precision == AMR_PREC_MIXED;
-    int per = -1;
-    if (nx == 8)
-        per = f32 ? occupancy<8, float>() : occupancy<8, double>();
-    else if (nx == 12)
-        per = f32 ? occupancy<12, float>() : occupancy<12, double>();
+    int per = occupancy_of(nx, layout, precision == AMR_PREC_MIXED);
     if (per <= 0) return -1;
     if (per_sm_cap > 0 && per_sm_cap < per) per = per_sm_cap;
     return sms * per;
 }
 
-cudaError_t launch_solve_persistent(const SolveArgs& a, int blocks, cudaStream_t s) {
+cudaError_t launch_solve_persistent(const SolveArgs& a, int blocks, int layout, cudaStream_t s) {
     ++g_launch_tally;
-    const bool f32 = a.g.precision == AMR_PREC_MIXED;
-    if (a.g.nx == 12) return f32 ? launch<12, float>(a, blocks, s) : launch<12, double>(a, blocks, s);
-    return f32 ? launch<8, float>(a, blocks, s) : launch<8, double>(a, blocks, s);
+    AMR_SOLVE_DISPATCH(a.g.nx, layout, a.g.precision == AMR_PREC_MIXED, cudaErrorInvalidValue, AMR_LAUNCH);
 }
+
+#undef AMR_OCC
+#undef AMR_LAUNCH
+#undef AMR_SOLVE_DISPATCH
 
 }  // namespace amr

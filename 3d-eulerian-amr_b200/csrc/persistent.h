@@ -53,12 +53,17 @@ struct SolveArgs {
     GridBarrier* bar;
 };
 
-// Blocks of one cooperative launch on the current device (all resident),
-// at most per_sm_cap per SM when per_sm_cap > 0.
-int solve_persistent_blocks(int nx, int precision, int per_sm_cap);
+// Block layouts of the solve kernel for nx^3 bricks (threads per block,
+// cells per thread in the relaxation; the same results bit for bit): how
+// many there are, and the threads of one (-1 for none).
+int solve_layouts(int nx);
+int solve_layout_threads(int nx, int layout);
+// Blocks of one cooperative launch of a layout on the current device (all
+// resident), at most per_sm_cap per SM when per_sm_cap > 0.
+int solve_persistent_blocks(int nx, int precision, int per_sm_cap, int layout);
 // raises the dynamic shared-memory limit of the solve kernels (call outside
 // stream capture)
 int solve_persistent_attributes();
-cudaError_t launch_solve_persistent(const SolveArgs& a, int blocks, cudaStream_t s);
+cudaError_t launch_solve_persistent(const SolveArgs& a, int blocks, int layout, cudaStream_t s);
 
 }  // namespace amr

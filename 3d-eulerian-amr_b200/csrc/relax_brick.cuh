@@ -63,6 +63,32 @@ __device__ __forceinline__ int relax_cell(int t) {
     return ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
 }
 
+// Sum of the NW warp partials p[0..NW-1] along a fixed pairwise tree
+// (identical in every thread, log2(NW) dependent additions instead of NW):
+// neighbours are added first, then pairs of pairs, and so on -- at span s
+// = 1, 2, 4, ... every partial q that is a multiple of 2s takes q + s when
+// that exists, left operand first.  Formed as a binary counter over a
+// small stack (at most log2(NW) + 1 partials live, which keeps the tree in
+// registers for the 54 partials of a 12^3 brick): after partial q is pushed
+// as many merges run as q + 1 has trailing zero bits, and the partials left
+// at the end are combined from the top, which adds exactly the operands the
+// tree adds, in its order.
+template <int NW>
+__device__ __forceinline__ double pairwise_sum(const double* p) {
+    double stk[8];
+    int top = 0;
+#pragma unroll
+    for (int q = 0; q < NW; q++) {
+        double v = p[q];
+#pragma unroll
+        for (int m = q; m & 1; m >>= 1) v = stk[--top] + v;
+        stk[top++] = v;
+    }
+#pragma unroll
+    for (; top > 1; top--) stk[top - 2] = stk[top - 2] + stk[top - 1];
+    return stk[0];
+}
+
 // The sweeps on a brick staged in two buffers x, y (x holds every cell,
 // ghosts included; y the same ghost faces): thread lt owns the K cells c[r]
 // with dphi1 values d1[r]; red holds the per-sweep warp partials
@@ -97,16 +123,7 @@ __device__ __forceinline__ double relax_sweeps_in(CT* x, CT* y, double* red, int
             for (int r = 0; r < K; r++) rd[r * WT + (lt >> 5)] = sq[r];
         }
         sync();
-        // pairwise sum of the warp partials (fixed tree, identical in every
-        // thread): log2(NW) dependent additions instead of NW
-        double w[NW];
-#pragma unroll
-        for (int q = 0; q < NW; q++) w[q] = rd[q];
-#pragma unroll
-        for (int span = 1; span < NW; span <<= 1)
-#pragma unroll
-            for (int q = 0; q + span < NW; q += 2 * span) w[q] = w[q] + w[q + span];
-        resid = w[0];
+        resid = pairwise_sum<NW>(rd);
         if (iters == 0) resid0 = resid;
         iters++;
         cur ^= 1;

@@ -321,6 +321,26 @@ int amr_relax_passes(amr_ctx* ctx, long long* per_level, int n);
  * reference's unbounded loops; 0 restores the defaults (2^22 polls for the
  * solve, 2^24 for the substep: seconds). */
 int amr_set_wait_limit(amr_ctx* ctx, int polls);
+/* Block layout of the persistent solve kernel (no reference counterpart:
+ * the reference has no kernels): layout 0 .. count-1 of the brick size
+ * (8^3: 512 threads, one cell each, two bricks per block on levels with
+ * more bricks than blocks; 256 threads, two cells each.  12^3: 576 threads,
+ * three cells each; 864, two; 288, six) and the blocks per SM of the launch
+ * (0: as many as fit).  Every layout gives the same results bit for bit.
+ * The captured graphs are re-captured at their next call.  Needs
+ * amr_config.persistent_solve > 0. */
+int amr_set_solve_layout(amr_ctx* ctx, int layout, int blocks_per_sm);
+int amr_get_solve_layout(amr_ctx* ctx, int* layout, int* blocks_per_sm, int* threads, int* blocks, int* count);
+/* Autotuner of the persistent solve: times a solve to L1 tolerance tol from
+ * the context's current potential in every layout with 1, 2 and as many
+ * blocks per SM as fit (reps timed solves after an untimed one, the
+ * potential restored before each), keeps the fastest and leaves the
+ * potential as it was.  ms[t] (t < ms_cap) receives trial t's mean device
+ * time (layout t / 3, blocks per SM 1, 2, all for t % 3; -1 where the trial
+ * repeats an earlier launch), *ntrials the number of trials, *best the one
+ * kept. */
+int amr_autotune_solve(amr_ctx* ctx, double tol, int max_cycles, int reps, double* ms, int ms_cap, int* ntrials,
+                       int* best);
 /* Of those phase times, the part spent at each phase's closing grid barrier
  * (block 0, from its arrival to the barrier's exit: the slowest block's extra
  * work plus the barrier itself), and the time spent forming the relaxation
