@@ -140,3 +140,46 @@ def test_persistent_wait_limit_times_out_and_context_recovers(gpu):
     assert np.array_equal(a.download_poisson()[0], b.download_poisson()[0])
     a.close()
     b.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["poisson_poly_L2", "ztwd12_L2"])
+def test_solve_layouts_bitwise_and_autotuner(gpu, table_path, case):
+    """Every block layout of the persistent solve kernel (threads per block,
+    cells per thread, blocks per SM) gives the plain form's potential bit for
+    bit; the autotuner times them all on the context's own solve, keeps one
+    and leaves the potential unchanged."""
+    if case.startswith("ztwd"):
+        from test_ztwd_gpu import make as make_ztwd
+        g = load_golden(case)
+        a = make_ztwd(gpu, g, table_path, persistent_solve=2)
+        a.ztwd_pot(1)  # pot_from_grid: phi from the state
+        tol = 1.0e-7
+    else:
+        g = load_golden(case)
+        a = make(gpu, 2, 2)
+        load_state(a, g)
+        tol = 1.0e-7
+    P0 = a.download_poisson()
+    _, _, _, _, count = a.solve_layout()
+    assert count >= 2
+    ref = None
+    for layout in range(count):
+        for per_sm in (1, 0):
+            a.set_solve_layout(layout, per_sm)
+            a.upload_poisson(P0)
+            e, n = a.graph_solve(tol)
+            phi = a.download_poisson()[0]
+            if ref is None:
+                ref = (e, n, phi)
+            else:
+                assert (e, n) == ref[:2], (layout, per_sm)
+                assert np.array_equal(phi, ref[2]), (layout, per_sm)
+    a.upload_poisson(P0)
+    ms, best = a.autotune_solve(tol, reps=1)
+    assert 0 <= best < len(ms) and ms[best] is not None and ms[best] > 0
+    assert all(m is None or m >= ms[best] for m in ms)
+    assert np.array_equal(a.download_poisson()[0], P0[0])
+    lay = a.solve_layout()
+    assert lay[0] == best // 3
+    a.close()
