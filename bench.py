@@ -884,9 +884,13 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
         if world > 1:
             dist.barrier()
 
+    tuned = {}
+
     def warmed():
         """A fresh context of the workload after the W warm-up steps, and its
-        step function (dt from max_dt with the MAXDTINC clamp)."""
+        step function (dt from max_dt with the MAXDTINC clamp); the first
+        one runs the solve autotuner after its warm-up, the second takes its
+        choice."""
         a = ztwd_context(amr, ini, helm_mod, table, ZT_LEVELS, amr.PREC_MIXED, 2, nx=args.zt_nx)
         state = {"step": 0, "last": 0.0}
 
@@ -900,6 +904,23 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
 
         for _ in range(args.warmup):
             one_step()
+        if not tuned and not args.no_autotune:
+            # a representative solve: from the potential of the step's start
+            # (phi0) to the current density, as the third substep solves
+            P = a.download_poisson()
+            Pk = P.copy()
+            Pk[0] = P[1]
+            a.upload_poisson(Pk)
+            ms, best = a.autotune_solve(ZT_TOL, reps=2)
+            a.upload_poisson(P)
+            lay = a.solve_layout()
+            tuned.update({"trials_ms": [None if m is None else round(m, 4) for m in ms], "best_trial": best,
+                          "layout": lay[0], "blocks_per_sm": lay[1], "threads": lay[2], "blocks": lay[3],
+                          "layouts": lay[4],
+                          "trial": "layout = trial // 3, blocks per SM = (1, 2, all)[trial % 3]; one persistent "
+                                   "solve from the step's starting potential, mean of 2 after 1 untimed"})
+        elif tuned:
+            a.set_solve_layout(tuned["layout"], tuned["blocks_per_sm"])
         return a, one_step
 
     a, one_step = warmed()
@@ -926,7 +947,7 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
         times.append(ev0.elapsed_time(ev1))
         cells += n
     barrier()
-    res = {"clocks": sampler.stop(), "gpu_launches": a.launch_count() - k0, "bricks": a.nbricks,
+    res = {"clocks": sampler.stop(), "gpu_launches": a.launch_count() - k0, "bricks": a.nbricks, "autotune": tuned,
            "ms_steps": [round(x, 3) for x in times]}
     ph1, w1, tot1 = a.solve_phases(), a.solve_phase_waits(), a.solve_totals()
     launches = max(tot1[1] - tot0[1], 1)
@@ -1169,6 +1190,7 @@ def main():
     ap.add_argument("--zt-nx", type=int, default=ZT_NX, choices=[8, 12],
                     help="interior cells per brick edge of the binary (12: the reference's BINARY build)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the solve's default block layout")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 forms and the 100-step error comparison of the binary")
     ap.add_argument("--sections", action="store_true",
@@ -1235,6 +1257,8 @@ def main():
                              "ncu DRAM read+write per solve launch on this workload (L2-resident arrays: far "
                              "below the algorithmic bytes)"),
             "cpu_baseline": cpu, "e2e": head["e2e"],
+            "autotune": {k: head["autotune"].get(k) for k in ("layout", "blocks_per_sm", "threads", "blocks",
+                                                            "trials_ms")} if head.get("autotune") else None,
             "clocks": head["clocks"], "gpu_launches": head["gpu_launches"],
         }
         if ztwd is not None:
