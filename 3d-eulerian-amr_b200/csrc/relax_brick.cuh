@@ -63,30 +63,32 @@ __device__ __forceinline__ int relax_cell(int t) {
     return ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
 }
 
-// Sum of the NW warp partials p[0..NW-1] along a fixed pairwise tree
-// (identical in every thread, log2(NW) dependent additions instead of NW):
-// neighbours are added first, then pairs of pairs, and so on -- at span s
-// = 1, 2, 4, ... every partial q that is a multiple of 2s takes q + s when
-// that exists, left operand first.  Formed as a binary counter over a
-// small stack (at most log2(NW) + 1 partials live, which keeps the tree in
-// registers for the 54 partials of a 12^3 brick): after partial q is pushed
-// as many merges run as q + 1 has trailing zero bits, and the partials left
-// at the end are combined from the top, which adds exactly the operands the
-// tree adds, in its order.
+// Sum of the NW warp partials p[0..NW-1] (NW <= 64; every partial is a sum
+// of squares, so >= 0) along a fixed pairwise tree, identical in every
+// thread: at span s = 1, 2, 4, ... every partial q that is a multiple of 2s
+// takes q + s when that exists, left operand first.  Each warp forms it with
+// a shuffle butterfly over lanes holding partials q and 32 + q (0 where
+// there is none): lane q adds the partial of lane q ^ s, which is q + s's
+// for q a multiple of 2s, and an absent partner adds +0.0, which leaves a
+// non-negative value unchanged; the other lanes add the same pairs in
+// swapped order, which IEEE addition does not distinguish.  So every lane
+// ends with the tree's sum bit for bit, from two shared loads per lane.
 template <int NW>
 __device__ __forceinline__ double pairwise_sum(const double* p) {
-    double stk[8];
-    int top = 0;
+    static_assert(NW <= 64, "at most 64 warp partials");
+    const int q = threadIdx.x & 31;
+    double lo = q < NW ? p[q] : 0.0;
+    double hi = (NW > 32 && 32 + q < NW) ? p[32 + q] : 0.0;
 #pragma unroll
-    for (int q = 0; q < NW; q++) {
-        double v = p[q];
-#pragma unroll
-        for (int m = q; m & 1; m >>= 1) v = stk[--top] + v;
-        stk[top++] = v;
+    for (int s = 1; s < 32; s <<= 1) {
+        const double a = __shfl_xor_sync(0xffffffffu, lo, s);
+        lo = (q & s) ? a + lo : lo + a;
+        if (NW > 32) {
+            const double b = __shfl_xor_sync(0xffffffffu, hi, s);
+            hi = (q & s) ? b + hi : hi + b;
+        }
     }
-#pragma unroll
-    for (; top > 1; top--) stk[top - 2] = stk[top - 2] + stk[top - 1];
-    return stk[0];
+    return NW > 32 ? lo + hi : lo;
 }
 
 // The sweeps on a brick staged in two buffers x, y (x holds every cell,

@@ -673,7 +673,7 @@ def run_batched_substep(amr, ini, torch, steps, warmup, levels=5):
     return out
 
 
-def ztwd_context(amr, ini, helm_mod, table, levels, prec, persistent, nx=ZT_NX):
+def ztwd_context(amr, ini, helm_mod, table, levels, prec, persistent, nx=ZT_NX, max_bricks=4096):
     """A ZTWD binary context on the 5-level tree of the reference's two-polytrope
     initial data (binary/initialize.cpp), EOS units of Binary::set_units."""
     P = ini.binary_params()
@@ -681,7 +681,7 @@ def ztwd_context(amr, ini, helm_mod, table, levels, prec, persistent, nx=ZT_NX):
     h.set_cgs_units(P["cm"], P["g"], P["s"], 1.0)
     a = amr.AMR(physics=amr.PHYSICS_ZTWD, nf=13, bw=3, nx=nx, reconstruction=amr.RECON_PPM, grid_dim=1.0,
                 z_reflect=1, mirror_refine_y=1, max_refine_level=levels, rho_floor=ini.BINARY["rho_floor"], cfl=0.3,
-                maxdtinc=1.25, max_bricks=4096, precision=prec, persistent_solve=persistent)
+                maxdtinc=1.25, max_bricks=max_bricks, precision=prec, persistent_solve=persistent)
     a.ztwd_set_eos(h)
     a.ztwd_set_frame(P["omega"], P["omega"], 0.0, 0.0)
     a.init()
@@ -1009,7 +1009,7 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
     return res
 
 
-def run_case(case, nx=ZT_NX):
+def run_case(case, nx=ZT_NX, layout=None):
     """One small run of a single kernel family, for profiler captures:
     solve_L3      one Poisson solve (L1 tol 1e-6) of the 3-level star, mixed
                   persistent form (k_solve_persistent)
@@ -1077,8 +1077,12 @@ def run_case(case, nx=ZT_NX):
         helm_mod = _load_module("helm_b200", os.path.join(PKG, "helm.py"))
         tdir = tempfile.mkdtemp(prefix="ztwd_")
         mixed = case == "ztwd_mixed_L5"
+        # a pool of 640 bricks (the tree has about 320): a few GB on the
+        # device, so that a profiler's save and restore stay small
         a = ztwd_context(amr, ini, helm_mod, helm_table.ensure_table(tdir), ZT_LEVELS,
-                         amr.PREC_MIXED if mixed else amr.PREC_FP64, 2 if mixed else 0, nx=nx)
+                         amr.PREC_MIXED if mixed else amr.PREC_FP64, 2 if mixed else 0, nx=nx, max_bricks=640)
+        if mixed and layout is not None:
+            a.set_solve_layout(*layout)
         last = 0.0
         nsteps = 4 if mixed else 2
         solve = {}
@@ -1191,6 +1195,8 @@ def main():
                     help="interior cells per brick edge of the binary (12: the reference's BINARY build)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the solve's default block layout")
+    ap.add_argument("--solve-layout", default=None,
+                    help="LAYOUT:BLOCKS_PER_SM of the persistent solve for --case runs (amr_set_solve_layout)")
     ap.add_argument("--no-compare", action="store_true",
                     help="skip the FP64 forms and the 100-step error comparison of the binary")
     ap.add_argument("--sections", action="store_true",
@@ -1208,7 +1214,8 @@ def main():
                     help="run one small case for a profiler capture and exit")
     args = ap.parse_args()
     if args.case:
-        return run_case(args.case, args.zt_nx)
+        return run_case(args.case, args.zt_nx,
+                        tuple(int(x) for x in args.solve_layout.split(":")) if args.solve_layout else None)
     if args.impl == "reference":
         return reference_arm(args)
 
