@@ -139,6 +139,8 @@ def load_library(path=LIB_PATH):
             if hasattr(lib, "amr_set_wait_limit"):
                 lib.amr_set_wait_limit.argtypes = [P, I]
             lib.amr_set_solve_layout.argtypes = [P, I, I]
+            lib.amr_solve_relax_split.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong),
+                                                  ctypes.POINTER(ctypes.c_longlong)]
             lib.amr_get_solve_layout.argtypes = [P, ip, ip, ip, ip, ip]
             lib.amr_autotune_solve.argtypes = [P, D, I, I, dp, I, ip, ip]
         _lib = lib
@@ -447,6 +449,16 @@ class AMR:
         n = ctypes.c_longlong()
         self._check(self.lib.amr_solve_totals(self.ctx, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+    def solve_relax_split(self):
+        """Block 0's view of the shared-memory relaxation loops: ms waiting
+        for neighbours, computing, waiting for the decision, publishing;
+        passes and sweeps."""
+        ms = np.zeros(4)
+        p, s = ctypes.c_longlong(), ctypes.c_longlong()
+        self._check(self.lib.amr_solve_relax_split(self.ctx, _dptr(ms), ctypes.byref(p), ctypes.byref(s)))
+        return {"wait_neighbours_ms": ms[0], "pass_ms": ms[1], "wait_decision_ms": ms[2], "publish_ms": ms[3],
+                "passes": p.value, "sweeps": s.value}
 
     def set_solve_layout(self, layout, blocks_per_sm=0):
         self._check(self.lib.amr_set_solve_layout(self.ctx, int(layout), int(blocks_per_sm)))

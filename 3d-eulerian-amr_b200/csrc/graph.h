@@ -58,6 +58,11 @@ struct Control {
     long long relax_level[MAX_LEVELS];  // relaxation passes per level
     int wait_limit;                     // persistent solve: polls per bounded wait (<= 0: default)
     int pad2;
+    // the shared-memory relaxation loops as block 0 sees them: time waiting
+    // for the neighbours' passes, computing passes (ghosts and sweeps),
+    // waiting for the loop decision, publishing; passes and sweeps counted
+    unsigned long long relax_split_ns[4];
+    unsigned long long relax_split_passes, relax_split_sweeps;
 };
 
 // phase classes of the persistent solve

@@ -563,6 +563,24 @@ int amr_solve_phase_waits(amr_ctx* c, double* wait_ms, int n, double* level_sum_
     return AMR_OK;
 }
 
+// The shared-memory relaxation loops of the persistent solve as block 0
+// sees them (its brick is in every level): ms[0..3] = waiting for the
+// neighbours' passes, computing passes, waiting for the loop decision,
+// publishing; the passes and the Jacobi sweeps block 0 computed.
+int amr_solve_relax_split(amr_ctx* c, double* ms, long long* passes, long long* sweeps) {
+    if (!c || !ms || !passes || !sweeps) return AMR_ERR_ARG;
+    if (!c->gs) {
+        for (int q = 0; q < 4; q++) ms[q] = 0.0;
+        *passes = *sweeps = 0;
+        return AMR_OK;
+    }
+    TRY(read_ctl(c));
+    for (int q = 0; q < 4; q++) ms[q] = c->gs->h_ctl->relax_split_ns[q] * 1e-6;
+    *passes = (long long)c->gs->h_ctl->relax_split_passes;
+    *sweeps = (long long)c->gs->h_ctl->relax_split_sweeps;
+    return AMR_OK;
+}
+
 // Device time and number of the persistent solve launches made by
 // amr_graph_solve (CUDA events around each launch on its stream).
 int amr_solve_totals(amr_ctx* c, double* ms, long long* count) {

@@ -164,6 +164,7 @@ struct Solver {
     double* ph_bytes;
     unsigned long long* ph_wait;  // [PH_COUNT], then level-sum time and count
     unsigned* lvl_n;              // relaxation passes per level
+    unsigned long long* rsplit;   // block 0: the resident loops' time split [4], passes, sweeps
 
     __device__ static unsigned long long now() {
         unsigned long long t;
@@ -415,7 +416,22 @@ struct Solver {
             y[gi] = v;
         }
         __syncthreads();
-        return relax_sweeps_in<NX, TPB, CT>(x, y, &sm[0].red[0][0], threadIdx.x, c, d1, res, BlockSync{});
+        int sw;
+        const double r = relax_sweeps_in<NX, TPB, CT>(x, y, &sm[0].red[0][0], threadIdx.x, c, d1, res, BlockSync{}, &sw);
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            rsplit[4]++;
+            rsplit[5] += sw;
+        }
+        return r;
+    }
+
+    // block 0, thread 0: adds the time since *t to split s and restarts *t
+    __device__ void split(int s, unsigned long long& t) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            const unsigned long long u = now();
+            rsplit[s] += u - t;
+            t = u;
+        }
     }
 
     // The server's part of a pass: waits until the level's bricks have all
@@ -500,13 +516,17 @@ struct Solver {
             if (server && !serve_sum(l, done, arr0 + n * (k + 1))) return false;
             CT* res = nullptr;
             double rr = 0.0;
+            unsigned long long tt = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
             if (mine) {
                 if (!wait_neighbours(b, seq0 + k)) return false;
+                split(0, tt);
                 rr = resident_pass(b, bufs[ib], bufs[(ib + 1) % 3], bufs[(ib + 2) % 3], snap + (size_t)par * a.snap_half,
                                    c, d1, &res);
+                split(1, tt);
             }
             double r;
             if (!wait_sum(r)) return false;
+            split(2, tt);
             bool again = r / r0 > ratio;
             if (again && outer > max_outer) {
                 again = false;
@@ -516,6 +536,7 @@ struct Solver {
             if (mine) {
                 ib = res == bufs[(ib + 1) % 3] ? (ib + 1) % 3 : (ib + 2) % 3;
                 resident_publish(b, bufs[ib], c, snap + (size_t)(par ^ 1) * a.snap_half, pres, rr, seq0 + k + 1);
+                split(3, tt);
             }
             par ^= 1;
             ++k;
@@ -648,6 +669,9 @@ __global__ void __launch_bounds__(TPB, SolveLayout<NX, TPB>::MINB) k_solve_persi
     }
     __shared__ unsigned s_lvl_n[MAX_LEVELS];
     s.lvl_n = s_lvl_n;
+    __shared__ unsigned long long s_rsplit[6];
+    s.rsplit = s_rsplit;
+    if (threadIdx.x < 6) s_rsplit[threadIdx.x] = 0;
     if (threadIdx.x < MAX_LEVELS) s_lvl_n[threadIdx.x] = 0;
     s.ph_ns = s_ph_ns;
     s.ph_n = s_ph_n;
@@ -697,6 +721,9 @@ __global__ void __launch_bounds__(TPB, SolveLayout<NX, TPB>::MINB) k_solve_persi
             c->level_sum_ns += s.ph_wait[PH_COUNT];
             c->level_sum_n += s.ph_wait[PH_COUNT + 1];
             for (int l = 0; l < MAX_LEVELS; l++) c->relax_level[l] += s.lvl_n[l];
+            for (int q = 0; q < 4; q++) c->relax_split_ns[q] += s.rsplit[q];
+            c->relax_split_passes += s.rsplit[4];
+            c->relax_split_sweeps += s.rsplit[5];
         }
     }
 }

@@ -98,7 +98,7 @@ __device__ __forceinline__ double pairwise_sum(const double* p) {
 // the relaxed brick.
 template <int NX, int TH, typename CT, typename Sync>
 __device__ __forceinline__ double relax_sweeps_in(CT* x, CT* y, double* red, int lt, const int* c, const CT* d1,
-                                                  CT** result, Sync sync) {
+                                                  CT** result, Sync sync, int* sweeps = nullptr) {
     constexpr int P = NX + 2, NW = NX * NX * NX / 32, K = NX * NX * NX / TH, WT = TH / 32;
     static_assert((NX * NX * NX) % TH == 0 && TH % 32 == 0, "relaxation layout");
     double resid0 = 0.0, resid = 0.0;
@@ -131,6 +131,7 @@ __device__ __forceinline__ double relax_sweeps_in(CT* x, CT* y, double* red, int
         cur ^= 1;
     } while (resid / resid0 > 0.5 && iters < 16);
     *result = cur ? y : x;
+    if (sweeps) *sweeps = iters;
     return resid;
 }
 

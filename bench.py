@@ -927,6 +927,7 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
     stream = torch.cuda.ExternalStream(a.stream_handle())
     ph0, w0, tot0 = a.solve_phases(), a.solve_phase_waits(), a.solve_totals()
     rp0 = a.relax_passes()
+    rs0 = a.solve_relax_split()
     k0 = a.launch_count()
     sampler = ClockSampler(local)
     barrier()
@@ -960,6 +961,8 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
         "phases_per_step": {k: v["count"] / args.steps for k, v in d.items()},
         "barrier_ms_per_step": {k: round((w1[k] - w0[k]) / args.steps, 4) for k in ph1},
         "level_sum_ms_per_step": round((w1["level_sum"] - w0["level_sum"]) / args.steps, 4)}
+    rs1 = a.solve_relax_split()
+    res["persistent"]["relax_split_per_step"] = {k: round((rs1[k] - rs0[k]) / args.steps, 3) for k in rs1}
     lv = a.get_tree()["level"]
     nl = int(lv.max()) + 1
     res["persistent"]["bricks_by_level"] = [int((lv == l).sum()) for l in range(nl)]
@@ -1132,6 +1135,7 @@ def roofline_persistent(res, traffic=None):
             "level_sum_ms_per_step": p.get("level_sum_ms_per_step"),
             "bricks_by_level": p.get("bricks_by_level"),
             "relax_passes_per_step_by_level": p.get("relax_passes_per_step_by_level"),
+            "relax_split_per_step": p.get("relax_split_per_step"),
             "note": "latency-bound: the reference's V-cycle is a chain of dependent per-level steps "
                     "(%d grid barriers per step here); the relaxation sweeps run in shared memory"
                     % round(sum(p["phases_per_step"].values()))}

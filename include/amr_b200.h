@@ -330,6 +330,12 @@ int amr_set_wait_limit(amr_ctx* ctx, int polls);
  * The captured graphs are re-captured at their next call.  Needs
  * amr_config.persistent_solve > 0. */
 int amr_set_solve_layout(amr_ctx* ctx, int layout, int blocks_per_sm);
+/* The persistent solve's shared-memory relaxation loops as its block 0 sees
+ * them (that block holds a brick of every level): ms[0..3] = time waiting
+ * for the neighbours' passes, computing passes (ghosts and sweeps), waiting
+ * for the loop decision, publishing; the passes and Jacobi sweeps it
+ * computed.  Accumulated since the context started. */
+int amr_solve_relax_split(amr_ctx* ctx, double* ms, long long* passes, long long* sweeps);
 int amr_get_solve_layout(amr_ctx* ctx, int* layout, int* blocks_per_sm, int* threads, int* blocks, int* count);
 /* Autotuner of the persistent solve: times a solve to L1 tolerance tol from
  * the context's current potential in every layout with 1, 2 and as many
