@@ -469,6 +469,20 @@ struct Solver {
         CT d1[K];
         const unsigned seq0 = pass_seq + 1;  // pass word of pass 0
         const unsigned arr0 = arrivals;
+        if (!mine && !server) {
+            // a block without a brick has no part in the loop: it goes to
+            // the closing barrier (one polled word instead of the loop's
+            // published sums) and takes the loop's length from the server,
+            // which stores it before it arrives there
+            if (!sync(PH_RELAX, 0)) return false;
+            const unsigned k = *(volatile const unsigned*)&a.bar->relax_done_k;
+            relax_par ^= (1 + k) & 1;
+            lsum_gen += 1 + k;
+            relax_calls += k + 1;
+            pass_seq = seq0 + k;
+            arrivals = arr0 + n * (k + 1);
+            return true;
+        }
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
         if (mine) {
             // pass 0: the ghost faces are in dphi (filled by the face phase)
@@ -555,6 +569,7 @@ struct Solver {
                 D[gi] = B[gi];
             }
         }
+        if (server && threadIdx.x == 0) a.bar->relax_done_k = k;  // the loop's length for the blocks without a brick
         pass_seq = seq0 + k;
         arrivals = arr0 + n * (k + 1);
         return sync(PH_RELAX, n * (k + 1));
