@@ -417,7 +417,7 @@ struct Solver {
         }
         __syncthreads();
         int sw;
-        const double r = relax_sweeps_in<NX, TPB, CT>(x, y, sm[0].sq, threadIdx.x, c, d1, res, BlockSync{}, &sw);
+        const double r = relax_sweeps_in<NX, TPB, CT>(x, y, &sm[0].red[0][0], threadIdx.x, c, d1, res, BlockSync{}, &sw);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             rsplit[4]++;
             rsplit[5] += sw;
@@ -495,7 +495,7 @@ struct Solver {
             relax_cells<NX, TPB, CT>(threadIdx.x, Corr<CT>::dphi1(a.st) + (size_t)b * P3, c, d1);
             __syncthreads();
             CT* res;
-            const double r = relax_sweeps_in<NX, TPB, CT>(bufs[0], bufs[1], sm[0].sq, threadIdx.x, c, d1,
+            const double r = relax_sweeps_in<NX, TPB, CT>(bufs[0], bufs[1], &sm[0].red[0][0], threadIdx.x, c, d1,
                                                           &res, BlockSync{});
             ib = res == bufs[0] ? 0 : 1;
             resident_publish(b, res, c, snap, pres, r, seq0);

@@ -310,12 +310,6 @@ void launch_vdown(const Geom& g, const BrickTable& bt, const DevState& st, const
 int launch_relax(const Geom& g, const DevState& st, const int* slots, int n, double* out, cudaStream_t s) {
     if (n <= 0) return 0;
     const bool f32 = g.precision == AMR_PREC_MIXED;
-    // the staged 12^3 brick in FP64 with its squares takes more than the 48 KB
-    // of dynamic shared memory a kernel gets without asking (host call, made
-    // outside any capture: the plain form is not captured)
-    if (g.nx == 12 && !f32)
-        cudaFuncSetAttribute((const void*)k_relax<12, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)sizeof(RelaxSmem<12, double>));
     if (g.nx == 8) {
         if (f32)
             launch_k(k_relax<8, float>, n, RelaxThreads<8>::value, sizeof(RelaxSmem<8, float>), s, g, st, slots, out);

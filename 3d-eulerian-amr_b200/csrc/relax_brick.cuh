@@ -4,23 +4,18 @@
 // Each sweep computes tmp0 = dphi1 + lap(dphi)/6 for every cell from the
 // previous sweep's values and adds it; the sweep's sum of tmp0^2 decides the
 // loop (ratio to the first sweep's > 0.5, at most 16 sweeps).  The two shared
-// buffers alternate; the squares go to shared memory, and after a barrier
-// the first warp forms their sum along a fixed tree and publishes it for a
-// second barrier, so every thread takes the same loop decision.  (The
-// reference adds the squares sequentially; the sums differ in the last bits
-// only.)
-//
-// The tree: the interior cells (index t = x + NX (y + NX z)) fall into
-// groups of 32 consecutive ones; a group's sum adds cells t and t + 16 of the
-// group, then those pairs at distance 8, 4, 2, 1 (the order of a warp's
-// xor-shuffle reduction over lanes t % 32); the NW = NX^3 / 32 group sums are
-// added neighbours first, then pairs of pairs and so on.  The tree depends on
-// cell indices only, so every thread layout gives the same sums bit for bit.
+// buffers alternate so one barrier per sweep suffices; every thread adds the
+// per-warp partial sums itself along the same fixed pairwise tree, so all
+// threads take the same loop decision.  (The reference adds the squares
+// sequentially; the sums differ in the last bits only.)
 //
 // Thread layout: TH threads (a multiple of 32 that divides NX^3) relax one
-// brick, K = NX^3 / TH cells each; thread lt owns interior cells lt + r TH,
-// r < K: a whole block of 512 threads on an 8^3 brick, two bricks of 256
-// threads each in one block, 576 or 864 or 288 threads on a 12^3 brick.
+// brick, K = NX^3 / TH cells each; thread lt owns interior cells
+// lt + r TH, r < K, counted x fastest.  Cell c's square enters the partial
+// of its 32-cell group c / 32 at lane c % 32 whatever TH is, so the warp
+// partials, their pairwise sum and every loop decision are the same bit for
+// bit for every layout: a whole block of 512 threads on an 8^3 brick, two
+// bricks of 256 threads each in one block, 576 threads on a 12^3 brick.
 #pragma once
 
 namespace amr {
@@ -28,12 +23,8 @@ namespace amr {
 template <int NX, typename CT = double>
 struct RelaxSmem {
     static constexpr int P = NX + 2, P3 = P * P * P, NT = NX * NX * NX, NW = NT / 32;
-    // the sweep's squares, group g at [33 g, 33 g + 32) (one pad entry per
-    // group keeps the first warp's reads to two-way bank conflicts), then
-    // the published sum
-    static constexpr int SQ = NT + NW + 2;
     CT buf[2][P3];
-    double sq[SQ];
+    double red[2][NW];
 };
 
 // Threads of a whole block relaxing one brick of NX^3 interior cells.
@@ -72,34 +63,22 @@ __device__ __forceinline__ int relax_cell(int t) {
     return ((t / (NX * NX) + 1) * P + (t / NX) % NX + 1) * P + t % NX + 1;
 }
 
-// Sum of the 32 squares of group g (sq[33 g + i], i < 32) in the group's
-// tree order: the leaves in bit-reversed order make the tree's pairs
-// neighbours, and a binary counter over them adds exactly the tree's
-// operands in its order (left first), with at most six partial sums live.
-__device__ __forceinline__ double group_sum(const double* sq, int g) {
-    double stk[6];
-    int top = 0;
-#pragma unroll
-    for (int j = 0; j < 32; j++) {
-        double v = sq[33 * g + (__brev(j) >> 27)];
-#pragma unroll
-        for (int m = j; m & 1; m >>= 1) v = stk[--top] + v;
-        stk[top++] = v;
-    }
-    return stk[0];
-}
-
-// Sum of the brick's squares by the first warp (lanes q: groups q and
-// 32 + q), the group sums added along the pairwise tree with a shuffle
-// butterfly: lane q adds the partial of lane q ^ s, which is q + s's for q a
-// multiple of 2s, and an absent group adds +0.0, which leaves a non-negative
-// value unchanged; the other lanes add the same pairs in swapped order,
-// which IEEE addition does not distinguish.  Lane 0 stores the sum.
+// Sum of the NW warp partials p[0..NW-1] (NW <= 64; every partial is a sum
+// of squares, so >= 0) along a fixed pairwise tree, identical in every
+// thread: at span s = 1, 2, 4, ... every partial q that is a multiple of 2s
+// takes q + s when that exists, left operand first.  Each warp forms it with
+// a shuffle butterfly over lanes holding partials q and 32 + q (0 where
+// there is none): lane q adds the partial of lane q ^ s, which is q + s's
+// for q a multiple of 2s, and an absent partner adds +0.0, which leaves a
+// non-negative value unchanged; the other lanes add the same pairs in
+// swapped order, which IEEE addition does not distinguish.  So every lane
+// ends with the tree's sum bit for bit, from two shared loads per lane.
 template <int NW>
-__device__ __forceinline__ void brick_sum(double* sq, int q) {
-    static_assert(NW <= 64, "at most 64 groups");
-    double lo = q < NW ? group_sum(sq, q) : 0.0;
-    double hi = (NW > 32 && 32 + q < NW) ? group_sum(sq, 32 + q) : 0.0;
+__device__ __forceinline__ double pairwise_sum(const double* p) {
+    static_assert(NW <= 64, "at most 64 warp partials");
+    const int q = threadIdx.x & 31;
+    double lo = q < NW ? p[q] : 0.0;
+    double hi = (NW > 32 && 32 + q < NW) ? p[32 + q] : 0.0;
 #pragma unroll
     for (int s = 1; s < 32; s <<= 1) {
         const double a = __shfl_xor_sync(0xffffffffu, lo, s);
@@ -109,37 +88,44 @@ __device__ __forceinline__ void brick_sum(double* sq, int q) {
             hi = (q & s) ? b + hi : hi + b;
         }
     }
-    if (q == 0) sq[NW * 33] = NW > 32 ? lo + hi : lo;
+    return NW > 32 ? lo + hi : lo;
 }
 
 // The sweeps on a brick staged in two buffers x, y (x holds every cell,
 // ghosts included; y the same ghost faces): thread lt owns the K cells c[r]
-// with dphi1 values d1[r]; sq is the squares' shared array
-// (RelaxSmem::SQ doubles).  Returns the last sweep's sum and the buffer that
-// holds the relaxed brick.
+// with dphi1 values d1[r]; red holds the per-sweep warp partials
+// (2 x NX^3 / 32).  Returns the last sweep's sum and the buffer that holds
+// the relaxed brick.
 template <int NX, int TH, typename CT, typename Sync>
-__device__ __forceinline__ double relax_sweeps_in(CT* x, CT* y, double* sq, int lt, const int* c, const CT* d1,
+__device__ __forceinline__ double relax_sweeps_in(CT* x, CT* y, double* red, int lt, const int* c, const CT* d1,
                                                   CT** result, Sync sync, int* sweeps = nullptr) {
-    constexpr int P = NX + 2, NW = NX * NX * NX / 32, K = NX * NX * NX / TH;
+    constexpr int P = NX + 2, NW = NX * NX * NX / 32, K = NX * NX * NX / TH, WT = TH / 32;
     static_assert((NX * NX * NX) % TH == 0 && TH % 32 == 0, "relaxation layout");
     double resid0 = 0.0, resid = 0.0;
     int iters = 0, cur = 0;
     do {
         const CT* d = cur ? y : x;
         CT* w_ = cur ? x : y;
+        double sq[K];
 #pragma unroll
         for (int r = 0; r < K; r++) {
             const int cc = c[r];
             const CT div = (d[cc + 1] + d[cc - 1] + d[cc + P] + d[cc - P] + d[cc + P * P] + d[cc - P * P]) - (d[cc] * CT(6.0));
             const CT tmp0 = d1[r] + div * (CT(1.0) / CT(6.0));
             w_[cc] = d[cc] + tmp0;
-            const int t = lt + r * TH;
-            sq[t + (t >> 5)] = double(tmp0) * double(tmp0);
+            sq[r] = double(tmp0) * double(tmp0);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int r = 0; r < K; r++) sq[r] += __shfl_xor_sync(0xffffffffu, sq[r], o);
+        double* rd = red + cur * NW;
+        if ((lt & 31) == 0) {
+#pragma unroll
+            for (int r = 0; r < K; r++) rd[r * WT + (lt >> 5)] = sq[r];
         }
         sync();
-        if (lt < 32) brick_sum<NW>(sq, lt);
-        sync();
-        resid = sq[NW * 33];
+        resid = pairwise_sum<NW>(rd);
         if (iters == 0) resid0 = resid;
         iters++;
         cur ^= 1;
@@ -156,7 +142,7 @@ __device__ __forceinline__ double relax_sweeps(RelaxSmem<NX, CT>& sm, int lt, co
                                                Sync sync) {
     constexpr int K = NX * NX * NX / TH;
     CT* res;
-    const double r = relax_sweeps_in<NX, TH, CT>(sm.buf[0], sm.buf[1], sm.sq, lt, c, d1, &res, sync);
+    const double r = relax_sweeps_in<NX, TH, CT>(sm.buf[0], sm.buf[1], &sm.red[0][0], lt, c, d1, &res, sync);
 #pragma unroll
     for (int q = 0; q < K; q++) out[q] = res[c[q]];
     return r;
