@@ -138,6 +138,25 @@ __device__ __forceinline__ void relax_layer_put(CT* sw, int t, CT v) {
     if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v;
 }
 
+// relax_layer_put for a snapshot of tagged entries (64 bits: the FP32 value
+// in the low half, the pass word `tag` in the high half), each written with
+// one relaxed 64-bit store: a reader that sees the tag it waits for sees
+// that pass's value, with no fence and no flag between them.
+__device__ __forceinline__ void tagged_put(unsigned long long* p, float v, unsigned tag) {
+    const unsigned long long w = ((unsigned long long)tag << 32) | __float_as_uint(v);
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
+}
+template <int NX>
+__device__ __forceinline__ void relax_layer_put_tagged(unsigned long long* sw, int t, float v, unsigned tag) {
+    const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
+    if (ci == 1) tagged_put(sw + (0 * NX + (cj - 1)) * NX + (ck - 1), v, tag);
+    if (ci == NX) tagged_put(sw + (1 * NX + (cj - 1)) * NX + (ck - 1), v, tag);
+    if (cj == 1) tagged_put(sw + (2 * NX + (ci - 1)) * NX + (ck - 1), v, tag);
+    if (cj == NX) tagged_put(sw + (3 * NX + (ci - 1)) * NX + (ck - 1), v, tag);
+    if (ck == 1) tagged_put(sw + (4 * NX + (ci - 1)) * NX + (cj - 1), v, tag);
+    if (ck == NX) tagged_put(sw + (5 * NX + (ci - 1)) * NX + (cj - 1), v, tag);
+}
+
 // Writes a relaxed interior value of cell t to dphi and to the snapshot.
 template <int NX, typename CT>
 __device__ __forceinline__ void relax_put(CT* D, CT* sw, int t, CT v) {

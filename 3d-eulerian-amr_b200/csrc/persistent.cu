@@ -380,21 +380,65 @@ struct Solver {
         return s_ok != 0;
     }
 
+    // The FP32 correction publishes its face layers as tagged entries (each
+    // value with its pass word in one 64-bit store, tagged_put): a neighbour
+    // waits on the very values it reads, so a pass needs neither a block
+    // barrier nor a release fence before its layers are visible, nor a
+    // separate pass word.  The FP64 correction has no room for a tag in a
+    // 64-bit store and publishes through the pass words.
+    static constexpr bool TAGGED = sizeof(CT) == 4;
+    // snapshot buffer p of tagged entries (their own allocation, zeroed
+    // before every launch; pass words start at 1)
+    __device__ unsigned long long* tagged_snap(int p) const { return a.tsnap + (size_t)p * a.snap_half; }
+
     // Publishes the relaxed brick `res` as a pass: its first interior layers
-    // to snapshot `wr`, its sum to pres[b]; then brick b's pass word is
-    // released as `seq` and the level's arrival count raised.
-    __device__ void resident_publish(int b, const CT* res, const int* c, CT* wr, double* pres, double resid,
+    // to snapshot buffer `wpar`, its sum to pres[b]; then (untagged) brick
+    // b's pass word is released as `seq`; the level's arrival count is raised.
+    __device__ void resident_publish(int b, const CT* res, const int* c, int wpar, double* pres, double resid,
                                      unsigned seq) {
         constexpr int K = NX * NX * NX / TPB;
-        CT* sw = wr + (size_t)b * a.stride;
+        if constexpr (TAGGED) {
+            unsigned long long* sw = tagged_snap(wpar) + (size_t)b * a.stride;
 #pragma unroll
-        for (int r = 0; r < K; r++) relax_layer_put<NX, CT>(sw, threadIdx.x + r * TPB, res[c[r]]);
-        if (threadIdx.x == 0) pres[b] = resid;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(a.rpub + b), "r"(seq) : "memory");
-            asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&a.bar->relax_arrivals), "r"(1u)
-                         : "memory");
+            for (int r = 0; r < K; r++) relax_layer_put_tagged<NX>(sw, threadIdx.x + r * TPB, float(res[c[r]]), seq);
+            if (threadIdx.x == 0) {
+                pres[b] = resid;
+                // the release orders this thread's sum before the arrival
+                asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&a.bar->relax_arrivals), "r"(1u)
+                             : "memory");
+            }
+        } else {
+            CT* sw = reinterpret_cast<CT*>(a.snap) + (size_t)wpar * a.snap_half + (size_t)b * a.stride;
+#pragma unroll
+            for (int r = 0; r < K; r++) relax_layer_put<NX, CT>(sw, threadIdx.x + r * TPB, res[c[r]]);
+            if (threadIdx.x == 0) pres[b] = resid;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(a.rpub + b), "r"(seq) : "memory");
+                asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&a.bar->relax_arrivals), "r"(1u)
+                             : "memory");
+            }
+        }
+    }
+
+    // A same-level neighbour's tagged layer value: waits until the entry
+    // carries pass word `tag`; false when the solve aborted or the wait ran
+    // out.
+    __device__ bool tagged_get(const unsigned long long* p, unsigned tag, CT& v) {
+        unsigned long long spins = 0;
+        for (;;) {
+            unsigned long long w;
+            asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w) : "l"(p) : "memory");
+            if ((unsigned)(w >> 32) == tag) {
+                v = CT(__uint_as_float((unsigned)w));
+                return true;
+            }
+            if ((spins & 63) == 63 && ld_volatile(&a.bar->abort)) return false;
+            if (++spins > spin_limit) {
+                give_up(a.bar, &a.ctl->status);
+                return false;
+            }
+            if (spins > 8) __nanosleep(20);
         }
     }
 
@@ -403,19 +447,33 @@ struct Solver {
     // `base` across z = 0, 0 on outflow faces), swept in x and y; nothing is
     // written outside shared memory.  Returns the sum and the buffer with the
     // relaxed brick (x or y).
-    __device__ double resident_pass(int b, CT* base, CT* x, CT* y, const CT* rd, const int* c, const CT* d1,
-                                    CT** res) {
+    __device__ double resident_pass(int b, CT* base, CT* x, CT* y, int rpar, unsigned want, const int* c,
+                                    const CT* d1, CT** res, bool& ok) {
         constexpr int K = NX * NX * NX / TPB, F = NX * NX;
 #pragma unroll
         for (int r = 0; r < K; r++) x[c[r]] = base[c[r]];
+        const CT* rd = reinterpret_cast<const CT*>(a.snap) + (size_t)rpar * a.snap_half;
+        int bad = 0;
         for (int q = threadIdx.x; q < 6 * F; q += TPB) {
             int face, t1, t2;
             const int gi = relax_ghost_cell<NX>(q, face, t1, t2);
-            const CT v = ghost_dphi<NX, CT>(a.g, a.bt, a.st, rd, a.stride, b, face, t1, t2, base);
+            CT v;
+            if (TAGGED && a.bt.ftype[6 * b + face] == FACE_SIB) {
+                const int nbr = a.bt.fnbr[6 * b + face];
+                const unsigned long long* p =
+                    tagged_snap(rpar) + (size_t)nbr * a.stride + ((face ^ 1) * NX + (t1 - 1)) * NX + (t2 - 1);
+                if (!tagged_get(p, want, v)) {
+                    bad = 1;
+                    v = CT(0);
+                }
+            } else {
+                v = ghost_dphi<NX, CT>(a.g, a.bt, a.st, rd, a.stride, b, face, t1, t2, base);
+            }
             x[gi] = v;
             y[gi] = v;
         }
-        __syncthreads();
+        ok = !__syncthreads_or(bad);
+        if (!ok) return 0.0;
         int sw;
         const double r = relax_sweeps_in<NX, TPB, CT>(x, y, &sm[0].red[0][0], threadIdx.x, c, d1, res, BlockSync{}, &sw);
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -498,7 +556,7 @@ struct Solver {
             const double r = relax_sweeps_in<NX, TPB, CT>(bufs[0], bufs[1], &sm[0].red[0][0], threadIdx.x, c, d1,
                                                           &res, BlockSync{});
             ib = res == bufs[0] ? 0 : 1;
-            resident_publish(b, res, c, snap, pres, r, seq0);
+            resident_publish(b, res, c, 0, pres, r, seq0);
         }
         count_pass(l);
         // pass 1 runs whatever the first sum; that sum is formed meanwhile
@@ -510,11 +568,14 @@ struct Solver {
             ++lsum_gen;
             if (server && !serve_sum(l, done, arr0 + n)) return false;
             if (mine) {
-                if (!wait_neighbours(b, seq0)) return false;
+                if (!TAGGED && !wait_neighbours(b, seq0)) return false;
                 CT* res;
-                const double r = resident_pass(b, bufs[ib], bufs[(ib + 1) % 3], bufs[(ib + 2) % 3], snap, c, d1, &res);
+                bool ok;
+                const double r =
+                    resident_pass(b, bufs[ib], bufs[(ib + 1) % 3], bufs[(ib + 2) % 3], 0, seq0, c, d1, &res, ok);
+                if (!ok) return false;
                 ib = res == bufs[(ib + 1) % 3] ? (ib + 1) % 3 : (ib + 2) % 3;
-                resident_publish(b, bufs[ib], c, snap + a.snap_half, pres, r, seq0 + 1);
+                resident_publish(b, bufs[ib], c, 1, pres, r, seq0 + 1);
             }
             if (!wait_sum(r0)) return false;
             count_pass(l);
@@ -532,10 +593,12 @@ struct Solver {
             double rr = 0.0;
             unsigned long long tt = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
             if (mine) {
-                if (!wait_neighbours(b, seq0 + k)) return false;
+                if (!TAGGED && !wait_neighbours(b, seq0 + k)) return false;
                 split(0, tt);
-                rr = resident_pass(b, bufs[ib], bufs[(ib + 1) % 3], bufs[(ib + 2) % 3], snap + (size_t)par * a.snap_half,
-                                   c, d1, &res);
+                bool ok;
+                rr = resident_pass(b, bufs[ib], bufs[(ib + 1) % 3], bufs[(ib + 2) % 3], par, seq0 + k, c, d1, &res,
+                                   ok);
+                if (!ok) return false;
                 split(1, tt);
             }
             double r;
@@ -549,7 +612,7 @@ struct Solver {
             if (!again) break;
             if (mine) {
                 ib = res == bufs[(ib + 1) % 3] ? (ib + 1) % 3 : (ib + 2) % 3;
-                resident_publish(b, bufs[ib], c, snap + (size_t)(par ^ 1) * a.snap_half, pres, rr, seq0 + k + 1);
+                resident_publish(b, bufs[ib], c, par ^ 1, pres, rr, seq0 + k + 1);
                 split(3, tt);
             }
             par ^= 1;

@@ -50,6 +50,7 @@ struct SolveArgs {
     double* nest;  // [blocks][cap] per-block nested-sum scratch
     void* snap;    // [2][cap][stride] face snapshots (CT entries)
     unsigned* rpub;  // [cap] last pass a brick published in the shared-memory relaxation loops (zero per launch)
+    unsigned long long* tsnap;  // [2][cap][stride] tagged face snapshots of the FP32 correction (zero per launch)
     size_t stride;
     size_t snap_half;
     GridBarrier* bar;
