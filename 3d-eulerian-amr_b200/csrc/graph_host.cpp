@@ -73,6 +73,7 @@ struct GraphState {
     GridBarrier* d_bar = nullptr;
     unsigned* d_rpub = nullptr;  // [cap] relaxation pass words of the persistent solve
     unsigned long long* d_tsnap = nullptr;  // [2][cap][6][nx][nx] tagged face snapshots (FP32 correction)
+    unsigned long long* d_tpres = nullptr;  // [2][cap][2] tagged per-brick relaxation sums (FP32 correction)
     cudaEvent_t ev_ps[2] = {nullptr, nullptr};  // around the last persistent launch
     double ps_ms_total = 0.0;                   // persistent launches of amr_graph_solve: device time, count
     long long ps_count = 0;
@@ -117,8 +118,10 @@ int ensure_state(amr_ctx* c) {
         CUDA_TRY(cudaMalloc(&g->d_pnest, sizeof(double) * (size_t)g->pnest_blocks * c->cap));
         CUDA_TRY(cudaMalloc(&g->d_bar, sizeof(GridBarrier)));
         CUDA_TRY(cudaMalloc(&g->d_rpub, sizeof(unsigned) * (size_t)c->cap));
-        if (c->geom.precision == AMR_PREC_MIXED)
+        if (c->geom.precision == AMR_PREC_MIXED) {
             CUDA_TRY(cudaMalloc(&g->d_tsnap, sizeof(unsigned long long) * 2 * snap_stride(c) * (size_t)c->cap));
+            CUDA_TRY(cudaMalloc(&g->d_tpres, sizeof(unsigned long long) * 4 * (size_t)c->cap));
+        }
         CUDA_TRY(cudaEventCreate(&g->ev_ps[0]));
         CUDA_TRY(cudaEventCreate(&g->ev_ps[1]));
     }
@@ -321,8 +324,11 @@ int rec_persistent(amr_ctx* c, cudaStream_t s, double tol) {
     a.rpub = g->d_rpub;
     CUDA_TRY(cudaMemsetAsync(g->d_rpub, 0, sizeof(unsigned) * (size_t)c->cap, s));
     a.tsnap = g->d_tsnap;
-    if (g->d_tsnap)
+    a.tpres = g->d_tpres;
+    if (g->d_tsnap) {
         CUDA_TRY(cudaMemsetAsync(g->d_tsnap, 0, sizeof(unsigned long long) * 2 * snap_stride(c) * (size_t)c->cap, s));
+        CUDA_TRY(cudaMemsetAsync(g->d_tpres, 0, sizeof(unsigned long long) * 4 * (size_t)c->cap, s));
+    }
     // event nodes bracketing the launch: the elapsed time of the latest
     // replay is the kernel's duration on this stream
     CUDA_TRY(cudaEventRecordWithFlags(g->ev_ps[0], s, cudaEventRecordExternal));
@@ -526,6 +532,7 @@ void graph_release(amr_ctx* c) {
     if (g->d_bar) cudaFree(g->d_bar);
     if (g->d_rpub) cudaFree(g->d_rpub);
     if (g->d_tsnap) cudaFree(g->d_tsnap);
+    if (g->d_tpres) cudaFree(g->d_tpres);
     for (cudaEvent_t e : g->ev_ps)
         if (e) cudaEventDestroy(e);
     delete g;

@@ -402,10 +402,12 @@ struct Solver {
 #pragma unroll
             for (int r = 0; r < K; r++) relax_layer_put_tagged<NX>(sw, threadIdx.x + r * TPB, float(res[c[r]]), seq);
             if (threadIdx.x == 0) {
-                pres[b] = resid;
-                // the release orders this thread's sum before the arrival
-                asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&a.bar->relax_arrivals), "r"(1u)
-                             : "memory");
+                // the FP64 sum as two tagged halves (pres buffer of this pass)
+                const int pp = (int)((pres - a.pres) / a.L.cap);
+                unsigned long long* w = a.tpres + ((size_t)pp * a.L.cap + b) * 2;
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(resid);
+                tagged_put(w, __uint_as_float((unsigned)(bits >> 32)), seq);
+                tagged_put(w + 1, __uint_as_float((unsigned)bits), seq);
             }
         } else {
             CT* sw = reinterpret_cast<CT*>(a.snap) + (size_t)wpar * a.snap_half + (size_t)b * a.stride;
@@ -495,11 +497,33 @@ struct Solver {
     // The server's part of a pass: waits until the level's bricks have all
     // released `target` arrivals, forms the level sum of `done` and publishes
     // it as generation lsum_gen.
-    __device__ bool serve_sum(int l, const double* done, unsigned target) {
+    __device__ bool serve_sum(int l, const double* done, unsigned target, unsigned tag) {
         __shared__ int s_ok;
-        if (threadIdx.x == 0) s_ok = wait_word(&a.bar->relax_arrivals, target);
-        __syncthreads();
-        if (!s_ok) return false;
+        if constexpr (TAGGED) {
+            // the bricks' tagged sums of this pass: wait on each, write it
+            // back whole to the pres buffer the level sum reads
+            const int* sl = level(l);
+            const int n = a.L.cnt[l];
+            const int pp = (int)((done - a.pres) / a.L.cap);
+            int bad = 0;
+            for (int q = threadIdx.x; q < n; q += TPB) {
+                const int b = sl[q];
+                const unsigned long long* w = a.tpres + ((size_t)pp * a.L.cap + b) * 2;
+                CT hi, lo;
+                if (!tagged_get(w, tag, hi) || !tagged_get(w + 1, tag, lo)) {
+                    bad = 1;
+                    continue;
+                }
+                const unsigned long long bits = ((unsigned long long)__float_as_uint(float(hi)) << 32) |
+                                                __float_as_uint(float(lo));
+                const_cast<double*>(done)[b] = __longlong_as_double((long long)bits);
+            }
+            if (__syncthreads_or(bad)) return false;
+        } else {
+            if (threadIdx.x == 0) s_ok = wait_word(&a.bar->relax_arrivals, target);
+            __syncthreads();
+            if (!s_ok) return false;
+        }
         const double r = level_sum(l, done);
         if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
         return true;
@@ -566,7 +590,7 @@ struct Solver {
             relax_par ^= 1;
             pres = a.pres + (size_t)relax_par * a.L.cap;
             ++lsum_gen;
-            if (server && !serve_sum(l, done, arr0 + n)) return false;
+            if (server && !serve_sum(l, done, arr0 + n, seq0)) return false;
             if (mine) {
                 if (!TAGGED && !wait_neighbours(b, seq0)) return false;
                 CT* res;
@@ -588,7 +612,7 @@ struct Solver {
             relax_par ^= 1;
             pres = a.pres + (size_t)relax_par * a.L.cap;
             ++lsum_gen;
-            if (server && !serve_sum(l, done, arr0 + n * (k + 1))) return false;
+            if (server && !serve_sum(l, done, arr0 + n * (k + 1), seq0 + k)) return false;
             CT* res = nullptr;
             double rr = 0.0;
             unsigned long long tt = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;

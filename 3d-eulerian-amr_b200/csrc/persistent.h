@@ -51,6 +51,7 @@ struct SolveArgs {
     void* snap;    // [2][cap][stride] face snapshots (CT entries)
     unsigned* rpub;  // [cap] last pass a brick published in the shared-memory relaxation loops (zero per launch)
     unsigned long long* tsnap;  // [2][cap][stride] tagged face snapshots of the FP32 correction (zero per launch)
+    unsigned long long* tpres;  // [2][cap][2] tagged halves of the per-brick relaxation sums (zero per launch)
     size_t stride;
     size_t snap_half;
     GridBarrier* bar;
