@@ -79,6 +79,16 @@ __device__ inline double nested_sum_smem(const LevelLists& L, const double* leaf
     return r;
 }
 
+// Entry of a snapshot layer: face f's first-interior layer, at face
+// coordinates t1 (along the lower of the two other axes) and t2 (the
+// higher), 1..NX.  t1 runs fastest, so the cells a warp relaxes (x fastest)
+// write neighbouring entries of every face, and the ghost faces a warp
+// fetches (relax_ghost_cell, t1 fastest) read neighbouring entries.
+template <int NX>
+__device__ __forceinline__ int layer_entry(int f, int t1, int t2) {
+    return (f * NX + (t2 - 1)) * NX + (t1 - 1);
+}
+
 // `self`, when given, holds the brick's own values before this pass (a
 // brick kept in shared memory); else they are read from dphi.
 template <int NX, typename CT>
@@ -89,7 +99,7 @@ __device__ __forceinline__ CT ghost_dphi(const Geom& g, const BrickTable& bt, co
     const int kind = bt.ftype[6 * b + face];
     const int nbr = bt.fnbr[6 * b + face];
     const CT* D = Corr<CT>::dphi(st);
-    if (kind == FACE_SIB) return __ldcg(snap_rd + (size_t)nbr * stride + ((face ^ 1) * NX + (t1 - 1)) * NX + (t2 - 1));
+    if (kind == FACE_SIB) return __ldcg(snap_rd + (size_t)nbr * stride + layer_entry<NX>(face ^ 1, t1, t2));
     if (kind == FACE_OUTFLOW) return CT(0);
     const int ax = face >> 1;
     const int qa = (face & 1) ? 1 : P - 2;  // the source layer along the face normal
@@ -130,12 +140,12 @@ __device__ __forceinline__ int relax_ghost_cell(int q, int& face, int& t1, int& 
 template <int NX, typename CT>
 __device__ __forceinline__ void relax_layer_put(CT* sw, int t, CT v) {
     const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
-    if (ci == 1) sw[(0 * NX + (cj - 1)) * NX + (ck - 1)] = v;
-    if (ci == NX) sw[(1 * NX + (cj - 1)) * NX + (ck - 1)] = v;
-    if (cj == 1) sw[(2 * NX + (ci - 1)) * NX + (ck - 1)] = v;
-    if (cj == NX) sw[(3 * NX + (ci - 1)) * NX + (ck - 1)] = v;
-    if (ck == 1) sw[(4 * NX + (ci - 1)) * NX + (cj - 1)] = v;
-    if (ck == NX) sw[(5 * NX + (ci - 1)) * NX + (cj - 1)] = v;
+    if (ci == 1) sw[layer_entry<NX>(0, cj, ck)] = v;
+    if (ci == NX) sw[layer_entry<NX>(1, cj, ck)] = v;
+    if (cj == 1) sw[layer_entry<NX>(2, ci, ck)] = v;
+    if (cj == NX) sw[layer_entry<NX>(3, ci, ck)] = v;
+    if (ck == 1) sw[layer_entry<NX>(4, ci, cj)] = v;
+    if (ck == NX) sw[layer_entry<NX>(5, ci, cj)] = v;
 }
 
 // relax_layer_put for a snapshot of tagged entries (64 bits: the FP32 value
@@ -149,12 +159,12 @@ __device__ __forceinline__ void tagged_put(unsigned long long* p, float v, unsig
 template <int NX>
 __device__ __forceinline__ void relax_layer_put_tagged(unsigned long long* sw, int t, float v, unsigned tag) {
     const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
-    if (ci == 1) tagged_put(sw + (0 * NX + (cj - 1)) * NX + (ck - 1), v, tag);
-    if (ci == NX) tagged_put(sw + (1 * NX + (cj - 1)) * NX + (ck - 1), v, tag);
-    if (cj == 1) tagged_put(sw + (2 * NX + (ci - 1)) * NX + (ck - 1), v, tag);
-    if (cj == NX) tagged_put(sw + (3 * NX + (ci - 1)) * NX + (ck - 1), v, tag);
-    if (ck == 1) tagged_put(sw + (4 * NX + (ci - 1)) * NX + (cj - 1), v, tag);
-    if (ck == NX) tagged_put(sw + (5 * NX + (ci - 1)) * NX + (cj - 1), v, tag);
+    if (ci == 1) tagged_put(sw + layer_entry<NX>(0, cj, ck), v, tag);
+    if (ci == NX) tagged_put(sw + layer_entry<NX>(1, cj, ck), v, tag);
+    if (cj == 1) tagged_put(sw + layer_entry<NX>(2, ci, ck), v, tag);
+    if (cj == NX) tagged_put(sw + layer_entry<NX>(3, ci, ck), v, tag);
+    if (ck == 1) tagged_put(sw + layer_entry<NX>(4, ci, cj), v, tag);
+    if (ck == NX) tagged_put(sw + layer_entry<NX>(5, ci, cj), v, tag);
 }
 
 // Writes a relaxed interior value of cell t to dphi and to the snapshot.

@@ -126,13 +126,19 @@ __device__ __forceinline__ bool lsum_wait(GridBarrier* bar, unsigned g, double& 
 // gives the same results bit for bit).  With 8^3 bricks and 512 threads a
 // block relaxes two bricks at once (one per half) on levels with more
 // bricks than blocks, so it holds two staged bricks; the other layouts take
-// such levels brick by brick.  MINB: blocks per SM the registers are
-// budgeted for.
+// such levels brick by brick.  With 12^3 bricks the FP32 correction's launch
+// holds two bricks' buffers, so that levels of up to twice as many bricks as
+// worker blocks stay in the shared-memory relaxation loop.  MINB: blocks per
+// SM the registers are budgeted for.
 template <int NX, int TPB_>
 struct SolveLayout {
     static constexpr int TPB = TPB_;
     static constexpr bool HALVES = NX == 8 && TPB == 512;
     static constexpr int NSM = HALVES ? 2 : 1;
+    // FP32 corrections of 12^3 bricks: three more brick buffers, for a
+    // second brick per block in the shared-memory relaxation loop
+    static constexpr bool RES2 = NX == 12;
+    static_assert(!RES2 || NSM == 1, "the extra buffers follow the third brick buffer");
     static constexpr int MINB = TPB >= 864 ? 1 : (TPB > 288 ? 2 : (TPB > 256 ? 3 : 4));
     // threads per face in the face-ghost phases
     static constexpr int PF = NX * NX <= TPB / 6 ? NX * NX : TPB / 6;
@@ -315,7 +321,7 @@ struct Solver {
             if (t < 6 * PF) op_dphi_faces<CT>(a.g, a.bt, a.st, a.aux, sl[q], t / PF, t % PF, PF);
         });
         if (!sync(PH_DPHI_FACES, n)) return false;
-        if (n < (int)gridDim.x) return relax_loop_resident(l, ratio, sl, n, snap);
+        if (n <= (RES2 ? 2 * ((int)gridDim.x - 1) : (int)gridDim.x)) return relax_loop_resident(l, ratio, sl, n, snap);
         int par = 0;
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
         relax_pass(sl, n, 0, snap, snap, pres);
@@ -387,6 +393,9 @@ struct Solver {
     // separate pass word.  The FP64 correction has no room for a tag in a
     // 64-bit store and publishes through the pass words.
     static constexpr bool TAGGED = sizeof(CT) == 4;
+    // the launch holds a second brick's three buffers after xbuf, so the
+    // shared-memory loop takes levels of up to two bricks per worker block
+    static constexpr bool RES2 = Lay::RES2 && TAGGED;
     // snapshot buffer p of tagged entries (their own allocation, zeroed
     // before every launch; pass words start at 1)
     __device__ unsigned long long* tagged_snap(int p) const { return a.tsnap + (size_t)p * a.snap_half; }
@@ -463,7 +472,7 @@ struct Solver {
             if (TAGGED && a.bt.ftype[6 * b + face] == FACE_SIB) {
                 const int nbr = a.bt.fnbr[6 * b + face];
                 const unsigned long long* p =
-                    tagged_snap(rpar) + (size_t)nbr * a.stride + ((face ^ 1) * NX + (t1 - 1)) * NX + (t2 - 1);
+                    tagged_snap(rpar) + (size_t)nbr * a.stride + layer_entry<NX>(face ^ 1, t1, t2);
                 if (!tagged_get(p, want, v)) {
                     bad = 1;
                     v = CT(0);
@@ -529,26 +538,48 @@ struct Solver {
         return true;
     }
 
-    // The relaxation loop of a level with fewer bricks than blocks: one
-    // brick per block, the brick kept in shared memory for the whole loop,
-    // the last block (which has no brick) forming the level sums.  No grid
-    // barrier between passes: a brick waits only for its same-level
-    // neighbours' published face layers (their pass words), computes the
-    // next pass from shared memory while the server forms the last pass's
-    // nested sum, and publishes it (snapshot layers, sum, pass word) once
-    // the sum says the loop goes on -- else the pass is dropped.  The loop
-    // ends with one write of each brick (interior and ghost faces) back to
-    // dphi and one grid barrier.  Passes written, their values, the sums
-    // and every loop decision are those of the loop in relax_until.
+    // Brick buffer i (0..2) of the shared-memory loop's brick j (0, 1).
+    __device__ CT* resident_buf(int j, int i) const {
+        constexpr int P3 = (NX + 2) * (NX + 2) * (NX + 2);
+        if (RES2 && j) return xbuf + (size_t)(1 + i) * P3;
+        return i == 0 ? sm[0].buf[0] : i == 1 ? sm[0].buf[1] : xbuf;
+    }
+
+    // The relaxation loop of a level the blocks can hold in shared memory:
+    // one brick per block, the last block (the server) forming the level
+    // sums; or, where the level has more bricks than blocks and the launch
+    // holds a second set of brick buffers (RES2), two bricks in the first
+    // worker blocks and none in the server.  The bricks stay in shared
+    // memory for the whole loop.  No grid barrier between passes: a brick
+    // waits only for its same-level neighbours' published face layers,
+    // computes the next pass from shared memory while the server forms the
+    // last pass's nested sum, and publishes it (snapshot layers, sum, pass
+    // word) once the sum says the loop goes on -- else the pass is dropped.
+    // A block with two bricks takes them one after the other in every pass;
+    // a server with a brick (as many bricks as blocks) forms the sum first,
+    // then its pass, so its brick trails the others by the sum's latency --
+    // a smaller delay than a second brick in one block.  The loop ends with
+    // one write of each brick (interior and ghost faces) back to dphi and
+    // one grid barrier.  Passes written, their values, the sums and every
+    // loop decision are those of the loop in relax_until.
     __device__ bool relax_loop_resident(int l, double ratio, const int* sl, int n, CT* snap) {
+        constexpr int NB = RES2 ? 2 : 1;
         constexpr int K = NX * NX * NX / TPB, P3 = (NX + 2) * (NX + 2) * (NX + 2), F = NX * NX;
-        const bool mine = (int)blockIdx.x < n;
-        const bool server = blockIdx.x == gridDim.x - 1;
-        const int b = mine ? sl[blockIdx.x] : -1;
-        CT* bufs[3] = {sm[0].buf[0], sm[0].buf[1], xbuf};
-        int ib = 0;  // buffer holding the committed brick
+        const int W = (int)gridDim.x - 1;
+        const bool server = (int)blockIdx.x == W;
+        // this block's bricks: slot blockIdx.x (the server's too when the
+        // level has as many bricks as blocks), and slot blockIdx.x + W in
+        // the worker blocks when it has more (-1: none)
+        const bool two = n > (int)gridDim.x;
+        const int b0 = (int)blockIdx.x < n && !(two && server) ? sl[blockIdx.x] : -1;
+        const int b1 = RES2 && two && !server && (int)blockIdx.x + W < n ? sl[blockIdx.x + W] : -1;
+        const bool mine = b0 >= 0;
+        // three buffers per brick (resident_buf): its committed values (ib0,
+        // ib1) and two to sweep in.  The brick loops below are not unrolled;
+        // a brick's values are picked by selects so they stay in registers.
+        int ib0 = 0, ib1 = 0;
         int c[K];
-        CT d1[K];
+        CT d1a[K], d1b[K];
         const unsigned seq0 = pass_seq + 1;  // pass word of pass 0
         const unsigned arr0 = arrivals;
         if (!mine && !server) {
@@ -566,23 +597,52 @@ struct Solver {
             return true;
         }
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
-        if (mine) {
+#pragma unroll 1
+        for (int j = 0; j < NB; j++) {
+            const int b = j ? b1 : b0;
+            if (b < 0) continue;
             // pass 0: the ghost faces are in dphi (filled by the face phase)
             const CT* D = Corr<CT>::dphi(a.st) + (size_t)b * P3;
+            CT* x = resident_buf(j, 0);
+            CT* y = resident_buf(j, 1);
             for (int q = threadIdx.x; q < P3; q += TPB) {
                 const CT v = D[q];
-                bufs[0][q] = v;
-                bufs[1][q] = v;
+                x[q] = v;
+                y[q] = v;
             }
+            CT d1[K];
             relax_cells<NX, TPB, CT>(threadIdx.x, Corr<CT>::dphi1(a.st) + (size_t)b * P3, c, d1);
+#pragma unroll
+            for (int r = 0; r < K; r++) {
+                if (j) d1b[r] = d1[r];
+                else d1a[r] = d1[r];
+            }
             __syncthreads();
             CT* res;
-            const double r = relax_sweeps_in<NX, TPB, CT>(bufs[0], bufs[1], &sm[0].red[0][0], threadIdx.x, c, d1,
-                                                          &res, BlockSync{});
-            ib = res == bufs[0] ? 0 : 1;
-            resident_publish(b, res, c, 0, pres, r, seq0);
+            const double rs = relax_sweeps_in<NX, TPB, CT>(x, y, &sm[0].red[0][0], threadIdx.x, c, d1, &res,
+                                                           BlockSync{});
+            const int i = res == x ? 0 : 1;
+            if (j) ib1 = i;
+            else ib0 = i;
+            resident_publish(b, res, c, 0, pres, rs, seq0);
         }
         count_pass(l);
+        // One pass of brick j from its committed buffer, the neighbours'
+        // layers of pass `want` in snapshot buffer `rpar`: the sum, and in
+        // *ri the buffer that holds the result.
+        auto pass = [&](int j, int rpar, unsigned want, int* ri, bool& ok) -> double {
+            const int b = j ? b1 : b0;
+            const int i = j ? ib1 : ib0;
+            CT d1[K];
+#pragma unroll
+            for (int r = 0; r < K; r++) d1[r] = j ? d1b[r] : d1a[r];
+            CT* x = resident_buf(j, (i + 1) % 3);
+            CT* res;
+            const double rs = resident_pass(b, resident_buf(j, i), x, resident_buf(j, (i + 2) % 3), rpar, want, c,
+                                            d1, &res, ok);
+            *ri = res == x ? (i + 1) % 3 : (i + 2) % 3;
+            return rs;
+        };
         // pass 1 runs whatever the first sum; that sum is formed meanwhile
         double r0;
         {
@@ -591,15 +651,18 @@ struct Solver {
             pres = a.pres + (size_t)relax_par * a.L.cap;
             ++lsum_gen;
             if (server && !serve_sum(l, done, arr0 + n, seq0)) return false;
-            if (mine) {
+#pragma unroll 1
+            for (int j = 0; j < NB; j++) {
+                const int b = j ? b1 : b0;
+                if (b < 0) continue;
                 if (!TAGGED && !wait_neighbours(b, seq0)) return false;
-                CT* res;
                 bool ok;
-                const double r =
-                    resident_pass(b, bufs[ib], bufs[(ib + 1) % 3], bufs[(ib + 2) % 3], 0, seq0, c, d1, &res, ok);
+                int ri;
+                const double rs = pass(j, 0, seq0, &ri, ok);
                 if (!ok) return false;
-                ib = res == bufs[(ib + 1) % 3] ? (ib + 1) % 3 : (ib + 2) % 3;
-                resident_publish(b, bufs[ib], c, 1, pres, r, seq0 + 1);
+                if (j) ib1 = ri;
+                else ib0 = ri;
+                resident_publish(b, resident_buf(j, ri), c, 1, pres, rs, seq0 + 1);
             }
             if (!wait_sum(r0)) return false;
             count_pass(l);
@@ -613,16 +676,28 @@ struct Solver {
             pres = a.pres + (size_t)relax_par * a.L.cap;
             ++lsum_gen;
             if (server && !serve_sum(l, done, arr0 + n * (k + 1), seq0 + k)) return false;
-            CT* res = nullptr;
-            double rr = 0.0;
+            // this pass of each brick, held until the sum of the last one
+            // decides whether it is published
+            int ri0 = 0, ri1 = 0;
+            double rr0 = 0.0, rr1 = 0.0;
             unsigned long long tt = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
-            if (mine) {
+#pragma unroll 1
+            for (int j = 0; j < NB; j++) {
+                const int b = j ? b1 : b0;
+                if (b < 0) continue;
                 if (!TAGGED && !wait_neighbours(b, seq0 + k)) return false;
                 split(0, tt);
                 bool ok;
-                rr = resident_pass(b, bufs[ib], bufs[(ib + 1) % 3], bufs[(ib + 2) % 3], par, seq0 + k, c, d1, &res,
-                                   ok);
+                int ri;
+                const double rs = pass(j, par, seq0 + k, &ri, ok);
                 if (!ok) return false;
+                if (j) {
+                    ri1 = ri;
+                    rr1 = rs;
+                } else {
+                    ri0 = ri;
+                    rr0 = rs;
+                }
                 split(1, tt);
             }
             double r;
@@ -635,19 +710,26 @@ struct Solver {
             }
             if (!again) break;
             if (mine) {
-                ib = res == bufs[(ib + 1) % 3] ? (ib + 1) % 3 : (ib + 2) % 3;
-                resident_publish(b, bufs[ib], c, par ^ 1, pres, rr, seq0 + k + 1);
-                split(3, tt);
+                ib0 = ri0;
+                resident_publish(b0, resident_buf(0, ib0), c, par ^ 1, pres, rr0, seq0 + k + 1);
             }
+            if (b1 >= 0) {
+                ib1 = ri1;
+                resident_publish(b1, resident_buf(1, ib1), c, par ^ 1, pres, rr1, seq0 + k + 1);
+            }
+            split(3, tt);
             par ^= 1;
             ++k;
             count_pass(l);
             ++outer;
         }
-        if (mine) {
+#pragma unroll 1
+        for (int j = 0; j < NB; j++) {
+            const int b = j ? b1 : b0;
+            if (b < 0) continue;
             // the committed brick back to dphi: interior and ghost faces
             CT* D = Corr<CT>::dphi(a.st) + (size_t)b * P3;
-            const CT* B = bufs[ib];
+            const CT* B = resident_buf(j, j ? ib1 : ib0);
 #pragma unroll
             for (int r = 0; r < K; r++) D[c[r]] = B[c[r]];
             for (int q = threadIdx.x; q < 6 * F; q += TPB) {
@@ -835,7 +917,9 @@ __global__ void __launch_bounds__(TPB, SolveLayout<NX, TPB>::MINB) k_solve_persi
 template <int NX, int TPB, typename CT>
 constexpr size_t solve_smem() {
     using Lay = SolveLayout<NX, TPB>;
-    return Lay::NSM * sizeof(RelaxSmem<NX, CT>) + (Lay::NSM == 1 ? sizeof(CT) * (NX + 2) * (NX + 2) * (NX + 2) : 0);
+    constexpr size_t P3 = (NX + 2) * (NX + 2) * (NX + 2);
+    return Lay::NSM * sizeof(RelaxSmem<NX, CT>) + (Lay::NSM == 1 ? sizeof(CT) * P3 : 0) +
+           (Lay::RES2 && sizeof(CT) == 4 ? 3 * sizeof(CT) * P3 : 0);
 }
 
 namespace {

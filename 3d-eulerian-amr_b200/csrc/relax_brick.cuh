@@ -65,30 +65,48 @@ __device__ __forceinline__ int relax_cell(int t) {
 
 // Sum of the NW warp partials p[0..NW-1] (NW <= 64; every partial is a sum
 // of squares, so >= 0) along a fixed pairwise tree, identical in every
-// thread: at span s = 1, 2, 4, ... every partial q that is a multiple of 2s
-// takes q + s when that exists, left operand first.  Each warp forms it with
-// a shuffle butterfly over lanes holding partials q and 32 + q (0 where
-// there is none): lane q adds the partial of lane q ^ s, which is q + s's
-// for q a multiple of 2s, and an absent partner adds +0.0, which leaves a
-// non-negative value unchanged; the other lanes add the same pairs in
-// swapped order, which IEEE addition does not distinguish.  So every lane
-// ends with the tree's sum bit for bit, from two shared loads per lane.
+// thread: partials 0..31 and 32..63 (0.0 where there is none) are each
+// added along the xor butterfly (at span s = 1, 2, 4, 8, 16 partial q takes
+// q ^ s), and the two halves' sums added last.  IEEE addition is
+// commutative and an absent partner adds +0.0, which leaves a non-negative
+// value unchanged, so every lane ends with the tree's sum bit for bit.
+// With two halves the first span is taken for both at once: even lanes keep
+// the low half's pair sum (q, q ^ 1) and odd lanes the high half's, one
+// shuffle carrying the half each lane gives away; spans 2..16 then add
+// within the same parity, and one more shuffle at span 1 adds the halves --
+// 6 shuffles instead of 10.
 template <int NW>
 __device__ __forceinline__ double pairwise_sum(const double* p) {
     static_assert(NW <= 64, "at most 64 warp partials");
     const int q = threadIdx.x & 31;
-    double lo = q < NW ? p[q] : 0.0;
-    double hi = (NW > 32 && 32 + q < NW) ? p[32 + q] : 0.0;
+    const double lo = q < NW ? p[q] : 0.0;
+    if constexpr (NW <= 32) {
+        double v = lo;
 #pragma unroll
-    for (int s = 1; s < 32; s <<= 1) {
-        const double a = __shfl_xor_sync(0xffffffffu, lo, s);
-        lo = (q & s) ? a + lo : lo + a;
-        if (NW > 32) {
-            const double b = __shfl_xor_sync(0xffffffffu, hi, s);
-            hi = (q & s) ? b + hi : hi + b;
-        }
+        for (int s = 1; s < 32; s <<= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+        return v;
+    } else {
+        const double hi = 32 + q < NW ? p[32 + q] : 0.0;
+        const bool odd = q & 1;
+        double v = (odd ? hi : lo) + __shfl_xor_sync(0xffffffffu, odd ? lo : hi, 1);
+#pragma unroll
+        for (int s = 2; s < 32; s <<= 1) v += __shfl_xor_sync(0xffffffffu, v, s);
+        return v + __shfl_xor_sync(0xffffffffu, v, 1);
     }
-    return NW > 32 ? lo + hi : lo;
+}
+
+// resid / resid0 > 0.5, the sweep loop's test, without the division.  For
+// resid0 >= 2^-1021 (so that 0.5 resid0 is a normal double, exact) the
+// correctly rounded quotient exceeds 0.5 exactly when resid > 0.5 resid0:
+// rounding is monotonic and 0.5 is a double, so the two can differ only if
+// the exact quotient lay in (0.5, 0.5 + 2^-54], which would need
+// 0 < resid - 0.5 resid0 <= 2^-54 resid0; but two different doubles differ
+// by at least one unit in the last place of the smaller, here of
+// 0.5 resid0, which is more than 2^-53 (0.5 resid0) = 2^-54 resid0.  Zero, subnormal, infinite and NaN values
+// give the same answer both ways (any resid0 below the bound takes the
+// division).
+__device__ __forceinline__ bool above_half(double resid, double resid0) {
+    return resid0 >= 0x1p-1021 ? resid > 0.5 * resid0 : resid / resid0 > 0.5;
 }
 
 // The sweeps on a brick staged in two buffers x, y (x holds every cell,
@@ -115,21 +133,34 @@ __device__ __forceinline__ double relax_sweeps_in(CT* x, CT* y, double* red, int
             w_[cc] = d[cc] + tmp0;
             sq[r] = double(tmp0) * double(tmp0);
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-            for (int r = 0; r < K; r++) sq[r] += __shfl_xor_sync(0xffffffffu, sq[r], o);
+        // warp partials: cells r and r + 1 of this thread lie in groups
+        // r WT + warp and (r + 1) WT + warp, whose butterflies (spans 16, 8,
+        // 4, 2, 1) are taken together: at span 16 the lower lanes keep group
+        // r's pair sums and the upper ones group r + 1's, one shuffle
+        // carrying the value each lane gives away; spans 8..1 stay within a
+        // half.  Same pairs, so the same sums, with 5 shuffles instead of 10.
         double* rd = red + cur * NW;
-        if ((lt & 31) == 0) {
+        const int lane = lt & 31, wp = lt >> 5;
 #pragma unroll
-            for (int r = 0; r < K; r++) rd[r * WT + (lt >> 5)] = sq[r];
+        for (int r = 0; r + 1 < K; r += 2) {
+            const bool up = lane & 16;
+            double v = (up ? sq[r + 1] : sq[r]) + __shfl_xor_sync(0xffffffffu, up ? sq[r] : sq[r + 1], 16);
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if ((lane & 15) == 0) rd[(r + (up ? 1 : 0)) * WT + wp] = v;
+        }
+        if constexpr (K & 1) {
+            double v = sq[K - 1];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) rd[(K - 1) * WT + wp] = v;
         }
         sync();
         resid = pairwise_sum<NW>(rd);
         if (iters == 0) resid0 = resid;
         iters++;
         cur ^= 1;
-    } while (resid / resid0 > 0.5 && iters < 16);
+    } while (above_half(resid, resid0) && iters < 16);
     *result = cur ? y : x;
     if (sweeps) *sweeps = iters;
     return resid;

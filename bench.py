@@ -708,6 +708,7 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL, n
            "binary": dict(ini.BINARY), "regrid": "every 8 steps (binary_driver.cpp:426)"}
     finals = {}
     snaps = {}  # state after steps 1 and 10, for the growth of the mixed form's error
+    layouts = {}  # the persistent forms' autotuned solve layouts
     for name, prec, pers in forms:
         a = ztwd_context(amr, ini, helm_mod, table, ZT_LEVELS, prec, pers, nx=nx)
         stream = torch.cuda.ExternalStream(a.stream_handle())
@@ -718,6 +719,8 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL, n
             if s > 0:
                 dt = min(1.25 * last, dt)
             timed = warmup <= s < warmup + steps
+            if s == warmup and pers:
+                layouts[name] = autotune_solve(a)
             if s == warmup:
                 ph0 = a.solve_phases() if pers else None
                 w0 = a.solve_phase_waits() if pers else None
@@ -729,15 +732,15 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL, n
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 e0.record(stream)
             last = a.ztwd_step(dt, ZT_TOL, DYNAMIC_RANGE, s)
-            if s + 1 in (1, 10) and name in ("fp64", "mixed"):
-                t = a.get_tree()
-                snaps[(name, s + 1)] = {"U": a.download_state(), "phi": a.download_poisson()[0], "level": t["level"],
-                                        "loc": t["loc"], "h": t["h"], "child_mask": t["child_mask"]}
             if timed:
                 e1.record(stream)
                 e1.synchronize()
                 times.append(e0.elapsed_time(e1))
                 cells += n
+            if s + 1 in (1, 10) and name in ("fp64", "mixed"):
+                t = a.get_tree()
+                snaps[(name, s + 1)] = {"U": a.download_state(), "phi": a.download_poisson()[0], "level": t["level"],
+                                        "loc": t["loc"], "h": t["h"], "child_mask": t["child_mask"]}
             if s == warmup + steps - 1:
                 st1 = a.stats()
                 if pers:
@@ -756,6 +759,7 @@ def run_ztwd(amr, ini, torch, steps, warmup, cpu_sample, total=ZT_STEPS_TOTAL, n
                      "relax_calls_per_step": (st1["relax_calls"] - st0["relax_calls"]) / steps}
         if pers:
             res[name]["persistent"] = phase_split
+            res[name]["autotune"] = {k: layouts[name][k] for k in ("layout", "blocks_per_sm", "threads", "blocks")}
         a.close()
     res["metric_unit"] = UNIT
     res["speedup_mixed_vs_fp64"] = res["fp64"]["ms_per_step"] / res["mixed"]["ms_per_step"]
@@ -867,6 +871,24 @@ def run_error_study(amr, ini, torch, nx=ZT_NX, total=ZT_STEPS_TOTAL, snaps=(1, 1
     return out
 
 
+def autotune_solve(a):
+    """Runs the persistent solve's autotuner on a representative solve of the
+    binary -- from the potential of the step's start (phi0) to the current
+    density, as the third substep solves -- and keeps the fastest layout;
+    returns the trials and the choice."""
+    P = a.download_poisson()
+    Pk = P.copy()
+    Pk[0] = P[1]
+    a.upload_poisson(Pk)
+    ms, best = a.autotune_solve(ZT_TOL, reps=2)
+    a.upload_poisson(P)
+    lay = a.solve_layout()
+    return {"trials_ms": [None if m is None else round(m, 4) for m in ms], "best_trial": best,
+            "layout": lay[0], "blocks_per_sm": lay[1], "threads": lay[2], "blocks": lay[3], "layouts": lay[4],
+            "trial": "layout = trial // 3, blocks per SM = (1, 2, all)[trial % 3]; one persistent solve from the "
+                     "step's starting potential, mean of 2 after 1 untimed"}
+
+
 def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
     """The headline: W untimed then K timed BinaryDriver steps of the 5-level
     ZTWD binary in the mixed persistent form (L2 flushed between timed steps,
@@ -905,20 +927,7 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
         for _ in range(args.warmup):
             one_step()
         if not tuned and not args.no_autotune:
-            # a representative solve: from the potential of the step's start
-            # (phi0) to the current density, as the third substep solves
-            P = a.download_poisson()
-            Pk = P.copy()
-            Pk[0] = P[1]
-            a.upload_poisson(Pk)
-            ms, best = a.autotune_solve(ZT_TOL, reps=2)
-            a.upload_poisson(P)
-            lay = a.solve_layout()
-            tuned.update({"trials_ms": [None if m is None else round(m, 4) for m in ms], "best_trial": best,
-                          "layout": lay[0], "blocks_per_sm": lay[1], "threads": lay[2], "blocks": lay[3],
-                          "layouts": lay[4],
-                          "trial": "layout = trial // 3, blocks per SM = (1, 2, all)[trial % 3]; one persistent "
-                                   "solve from the step's starting potential, mean of 2 after 1 untimed"})
+            tuned.update(autotune_solve(a))
         elif tuned:
             a.set_solve_layout(tuned["layout"], tuned["blocks_per_sm"])
         return a, one_step
