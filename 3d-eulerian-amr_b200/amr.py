@@ -142,6 +142,7 @@ def load_library(path=LIB_PATH):
             lib.amr_solve_relax_split.argtypes = [P, dp, ctypes.POINTER(ctypes.c_longlong),
                                                   ctypes.POINTER(ctypes.c_longlong)]
             lib.amr_get_solve_layout.argtypes = [P, ip, ip, ip, ip, ip]
+            lib.amr_solve_relax_level_ms.argtypes = [P, dp, I]
             lib.amr_autotune_solve.argtypes = [P, D, I, I, dp, I, ip, ip]
         _lib = lib
     return _lib
@@ -449,6 +450,12 @@ class AMR:
         n = ctypes.c_longlong()
         self._check(self.lib.amr_solve_totals(self.ctx, ctypes.byref(ms), ctypes.byref(n)))
         return ms.value, n.value
+
+    def solve_relax_level_ms(self, n=16):
+        """Block 0's ms in the persistent solve's relaxation loops per level."""
+        ms = np.zeros(n)
+        self._check(self.lib.amr_solve_relax_level_ms(self.ctx, _dptr(ms), n))
+        return ms
 
     def solve_relax_split(self):
         """Block 0's view of the shared-memory relaxation loops: ms waiting

@@ -63,6 +63,9 @@ struct Control {
     // waiting for the loop decision, publishing; passes and sweeps counted
     unsigned long long relax_split_ns[4];
     unsigned long long relax_split_passes, relax_split_sweeps;
+    // block 0's time in the relaxation loops of each level (from the dphi
+    // ghost faces to the loop's closing barrier)
+    unsigned long long relax_level_ns[MAX_LEVELS];
 };
 
 // phase classes of the persistent solve

@@ -595,6 +595,15 @@ int amr_solve_relax_split(amr_ctx* c, double* ms, long long* passes, long long* 
     return AMR_OK;
 }
 
+// Block 0's time (ms) in the persistent solve's relaxation loops of each
+// level since the context started; levels past n are not written.
+int amr_solve_relax_level_ms(amr_ctx* c, double* ms, int n) {
+    if (!c || !ms || n < 0) return AMR_ERR_ARG;
+    if (c->gs) TRY(read_ctl(c));
+    for (int l = 0; l < n; l++) ms[l] = c->gs && l < MAX_LEVELS ? c->gs->h_ctl->relax_level_ns[l] * 1e-6 : 0.0;
+    return AMR_OK;
+}
+
 // Device time and number of the persistent solve launches made by
 // amr_graph_solve (CUDA events around each launch on its stream).
 int amr_solve_totals(amr_ctx* c, double* ms, long long* count) {

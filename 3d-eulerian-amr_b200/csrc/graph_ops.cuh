@@ -51,13 +51,23 @@ __device__ inline double nested_sum_block(const LevelLists& L, const int* __rest
 // S(c1)) + ... in child order, own = leaf[p] when withown, else 0.  Same
 // additions in the same order as nested_sum_block; the result is returned
 // to every thread.  Needs L.max_cnt <= NEST_SMEM.
+__device__ inline double nested_sum_smem_in(const LevelLists& L, const double* leaf, int top, bool withown,
+                                            double* buf);
 __device__ inline double nested_sum_smem(const LevelLists& L, const double* leaf, int top, bool withown,
                                          double* buf) {
+    for (int q = threadIdx.x; q < L.cnt[top]; q += blockDim.x) buf[q] = __ldcg(leaf + L.slots[L.off[top] + q]);
+    __syncthreads();
+    return nested_sum_smem_in(L, leaf, top, withown, buf);
+}
+
+// nested_sum_smem with level `top`'s values already in buf[0 .. cnt[top])
+// (level list order, made visible to the block); leaf is read only for the
+// own values of the levels above (withown).
+__device__ inline double nested_sum_smem_in(const LevelLists& L, const double* leaf, int top, bool withown,
+                                            double* buf) {
     double* vb = buf;
     double* ub = buf + NEST_SMEM;
     const int e0 = L.off[0];
-    for (int q = threadIdx.x; q < L.cnt[top]; q += blockDim.x) vb[q] = __ldcg(leaf + L.slots[L.off[top] + q]);
-    __syncthreads();
     for (int m = top - 1; m >= 0; m--) {
         for (int q = threadIdx.x; q < L.cnt[m]; q += blockDim.x) {
             const int* cp = L.cpos + 8 * (L.off[m] - e0 + q);

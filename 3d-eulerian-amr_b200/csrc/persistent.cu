@@ -170,6 +170,7 @@ struct Solver {
     double* ph_bytes;
     unsigned long long* ph_wait;  // [PH_COUNT], then level-sum time and count
     unsigned* lvl_n;              // relaxation passes per level
+    unsigned long long* lvl_ns;   // block 0's time in each level's relaxation loops
     unsigned long long* rsplit;   // block 0: the resident loops' time split [4], passes, sweeps
 
     __device__ static unsigned long long now() {
@@ -300,7 +301,24 @@ struct Solver {
     // time it waits for it)
     __device__ bool wait_sum(double& r) {
         const unsigned long long t0 = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
-        const bool ok = lsum_wait(a.bar, lsum_gen, r, spin_limit, &a.ctl->status);
+        bool ok;
+        if constexpr (TAGGED) {
+            // the two tagged halves: each carries the generation it belongs
+            // to, so a half of an older sum is never taken for this one
+            __shared__ double s_r;
+            __shared__ int s_ok;
+            if (threadIdx.x == 0) {
+                CT hi, lo;
+                const int good = tagged_get2(a.bar->lsum_tag, lsum_gen, hi, lo);
+                s_r = good ? join_halves(hi, lo) : 0.0;
+                s_ok = good;
+            }
+            __syncthreads();
+            r = s_r;
+            ok = s_ok != 0;
+        } else {
+            ok = lsum_wait(a.bar, lsum_gen, r, spin_limit, &a.ctl->status);
+        }
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             ph_wait[PH_COUNT] += now() - t0;
             ph_wait[PH_COUNT + 1]++;
@@ -312,6 +330,12 @@ struct Solver {
     // with ghosts from the previous pass's snapshot until the level sum has
     // fallen to `ratio` of the first
     __device__ bool relax_until(int l, double ratio) {
+        const unsigned long long t0 = (blockIdx.x == 0 && threadIdx.x == 0) ? now() : 0;
+        const bool ok = relax_until_(l, ratio);
+        if (blockIdx.x == 0 && threadIdx.x == 0) lvl_ns[l] += now() - t0;
+        return ok;
+    }
+    __device__ bool relax_until_(int l, double ratio) {
         const int* sl = level(l);
         const int n = a.L.cnt[l];
         const int t = threadIdx.x;
@@ -432,6 +456,36 @@ struct Solver {
         }
     }
 
+    // Two adjacent tagged entries (the halves of an FP64 value): waits until
+    // both carry pass word `tag`, loading the two together in every poll.
+    __device__ bool tagged_get2(const unsigned long long* p, unsigned tag, CT& hi, CT& lo) {
+        unsigned long long spins = 0;
+        for (;;) {
+            unsigned long long w0, w1;
+            asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w0) : "l"(p) : "memory");
+            asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(w1) : "l"(p + 1) : "memory");
+            if ((unsigned)(w0 >> 32) == tag && (unsigned)(w1 >> 32) == tag) {
+                hi = CT(__uint_as_float((unsigned)w0));
+                lo = CT(__uint_as_float((unsigned)w1));
+                return true;
+            }
+            if ((spins & 63) == 63 && ld_volatile(&a.bar->abort)) return false;
+            if (++spins > spin_limit) {
+                give_up(a.bar, &a.ctl->status);
+                return false;
+            }
+            if (spins > 8) __nanosleep(20);
+        }
+    }
+
+    // The FP64 value whose high and low 32 bits were sent as the bit
+    // patterns of two tagged FP32 entries.
+    __device__ static double join_halves(CT hi, CT lo) {
+        const unsigned long long bits = ((unsigned long long)__float_as_uint(float(hi)) << 32) |
+                                        __float_as_uint(float(lo));
+        return __longlong_as_double((long long)bits);
+    }
+
     // A same-level neighbour's tagged layer value: waits until the entry
     // carries pass word `tag`; false when the solve aborted or the wait ran
     // out.
@@ -509,33 +563,47 @@ struct Solver {
     __device__ bool serve_sum(int l, const double* done, unsigned target, unsigned tag) {
         __shared__ int s_ok;
         if constexpr (TAGGED) {
-            // the bricks' tagged sums of this pass: wait on each, write it
-            // back whole to the pres buffer the level sum reads
+            // the bricks' tagged sums of this pass: wait on each and take it
+            // straight into the shared buffer of the nested sum (or, for a
+            // level too large for it, write it back whole to the pres
+            // buffer the level sum reads); the sum goes out as two tagged
+            // halves, so neither side needs a fence or a flag
             const int* sl = level(l);
             const int n = a.L.cnt[l];
             const int pp = (int)((done - a.pres) / a.L.cap);
+            const bool in_smem = a.L.max_cnt <= NEST_SMEM;
             int bad = 0;
             for (int q = threadIdx.x; q < n; q += TPB) {
                 const int b = sl[q];
                 const unsigned long long* w = a.tpres + ((size_t)pp * a.L.cap + b) * 2;
                 CT hi, lo;
-                if (!tagged_get(w, tag, hi) || !tagged_get(w + 1, tag, lo)) {
+                if (!tagged_get2(w, tag, hi, lo)) {
                     bad = 1;
                     continue;
                 }
-                const unsigned long long bits = ((unsigned long long)__float_as_uint(float(hi)) << 32) |
-                                                __float_as_uint(float(lo));
-                const_cast<double*>(done)[b] = __longlong_as_double((long long)bits);
+                if (in_smem)
+                    nbuf[q] = join_halves(hi, lo);
+                else
+                    const_cast<double*>(done)[b] = join_halves(hi, lo);
             }
             if (__syncthreads_or(bad)) return false;
+            const double r = !in_smem ? level_sum(l, done) : l == 0 ? nbuf[0] : nested_sum_smem_in(a.L, done, l, false, nbuf);
+            if (threadIdx.x == 0) {
+                const unsigned long long bits = (unsigned long long)__double_as_longlong(r);
+                tagged_put(&a.bar->lsum_tag[0], __uint_as_float((unsigned)(bits >> 32)), lsum_gen);
+                tagged_put(&a.bar->lsum_tag[1], __uint_as_float((unsigned)bits), lsum_gen);
+            }
+            // the shared buffer is read again by the next pass's sum
+            __syncthreads();
+            return true;
         } else {
             if (threadIdx.x == 0) s_ok = wait_word(&a.bar->relax_arrivals, target);
             __syncthreads();
             if (!s_ok) return false;
+            const double r = level_sum(l, done);
+            if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
+            return true;
         }
-        const double r = level_sum(l, done);
-        if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
-        return true;
     }
 
     // Brick buffer i (0..2) of the shared-memory loop's brick j (0, 1).
@@ -853,10 +921,15 @@ __global__ void __launch_bounds__(TPB, SolveLayout<NX, TPB>::MINB) k_solve_persi
     }
     __shared__ unsigned s_lvl_n[MAX_LEVELS];
     s.lvl_n = s_lvl_n;
+    __shared__ unsigned long long s_lvl_ns[MAX_LEVELS];
+    s.lvl_ns = s_lvl_ns;
     __shared__ unsigned long long s_rsplit[6];
     s.rsplit = s_rsplit;
     if (threadIdx.x < 6) s_rsplit[threadIdx.x] = 0;
-    if (threadIdx.x < MAX_LEVELS) s_lvl_n[threadIdx.x] = 0;
+    if (threadIdx.x < MAX_LEVELS) {
+        s_lvl_n[threadIdx.x] = 0;
+        s_lvl_ns[threadIdx.x] = 0;
+    }
     s.ph_ns = s_ph_ns;
     s.ph_n = s_ph_n;
     s.ph_bytes = s_ph_bytes;
@@ -904,7 +977,10 @@ __global__ void __launch_bounds__(TPB, SolveLayout<NX, TPB>::MINB) k_solve_persi
             }
             c->level_sum_ns += s.ph_wait[PH_COUNT];
             c->level_sum_n += s.ph_wait[PH_COUNT + 1];
-            for (int l = 0; l < MAX_LEVELS; l++) c->relax_level[l] += s.lvl_n[l];
+            for (int l = 0; l < MAX_LEVELS; l++) {
+                c->relax_level[l] += s.lvl_n[l];
+                c->relax_level_ns[l] += s.lvl_ns[l];
+            }
             for (int q = 0; q < 4; q++) c->relax_split_ns[q] += s.rsplit[q];
             c->relax_split_passes += s.rsplit[4];
             c->relax_split_sweeps += s.rsplit[5];

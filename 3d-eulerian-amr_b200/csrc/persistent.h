@@ -26,6 +26,10 @@ struct GridBarrier {
     // the last pass of the latest shared-memory relaxation loop (stored by
     // the block that forms its sums before the loop's closing barrier)
     unsigned int relax_done_k;
+    // the FP32 correction's level sums: the high and low halves of the FP64
+    // sum, each tagged with its generation (value and tag in one 64-bit
+    // word), on a cache line of their own
+    alignas(128) unsigned long long lsum_tag[2];
 };
 
 struct SolveArgs {

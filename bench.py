@@ -71,12 +71,14 @@ BYTES_PER_BRICK = {
 }
 
 # DRAM bytes (read + write) per launch of the persistent solve on the 5-level
-# ZTWD binary: the mean over the six solve launches of two BinaryDriver steps
-# of `bench.py --case ztwd_mixed_L5`, one ncu capture (dram__bytes_read.sum +
-# dram__bytes_write.sum, caches flushed before each launch); those launches
-# carry 2.72 GB of algorithmic bytes each.  The solve's arrays stay in L2
-# across its V-cycles, so DRAM sees the cold fill and the dirty write-back.
-ZT_SOLVE_DRAM_BYTES_PER_LAUNCH = {8: 16.69e6}
+# ZTWD binary, from ncu (dram__bytes_read.sum + dram__bytes_write.sum, caches
+# flushed before each launch) on `bench.py --case ztwd_mixed_L5`: 8^3 bricks,
+# the mean over the six solve launches of two BinaryDriver steps (2.72 GB of
+# algorithmic bytes each); 12^3 bricks, the seventh solve launch of the case
+# (7.93 GB of algorithmic bytes).  The solve's arrays stay in L2 across its
+# V-cycles, so DRAM sees the cold fill, the per-launch zeroing of the tagged
+# relaxation buffers and the dirty write-back.
+ZT_SOLVE_DRAM_BYTES_PER_LAUNCH = {8: 16.69e6, 12: 215.0e6}
 
 
 def load_amr():
@@ -937,6 +939,7 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
     ph0, w0, tot0 = a.solve_phases(), a.solve_phase_waits(), a.solve_totals()
     rp0 = a.relax_passes()
     rs0 = a.solve_relax_split()
+    rl0 = a.solve_relax_level_ms()
     k0 = a.launch_count()
     sampler = ClockSampler(local)
     barrier()
@@ -977,6 +980,8 @@ def run_ztwd_headline(amr, ini, args, world, local, torch, dist):
     res["persistent"]["bricks_by_level"] = [int((lv == l).sum()) for l in range(nl)]
     res["persistent"]["relax_passes_per_step_by_level"] = [
         round(float(x) / args.steps, 1) for x in (a.relax_passes() - rp0)[:nl]]
+    res["persistent"]["relax_ms_per_step_by_level"] = [
+        round(float(x) / args.steps, 3) for x in (a.solve_relax_level_ms() - rl0)[:nl]]
     a.close()
     t = aggregate(sum(times), cells, world, dist)
     res["ms_total"], res["cells"] = t
@@ -1145,6 +1150,7 @@ def roofline_persistent(res, traffic=None):
             "bricks_by_level": p.get("bricks_by_level"),
             "relax_passes_per_step_by_level": p.get("relax_passes_per_step_by_level"),
             "relax_split_per_step": p.get("relax_split_per_step"),
+            "relax_ms_per_step_by_level": p.get("relax_ms_per_step_by_level"),
             "note": "latency-bound: the reference's V-cycle is a chain of dependent per-level steps "
                     "(%d grid barriers per step here); the relaxation sweeps run in shared memory"
                     % round(sum(p["phases_per_step"].values()))}

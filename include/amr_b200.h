@@ -336,6 +336,10 @@ int amr_set_solve_layout(amr_ctx* ctx, int layout, int blocks_per_sm);
  * for the loop decision, publishing; the passes and Jacobi sweeps it
  * computed.  Accumulated since the context started. */
 int amr_solve_relax_split(amr_ctx* ctx, double* ms, long long* passes, long long* sweeps);
+/* The persistent solve's block 0 time (ms) in the relaxation loops of each
+ * level 0..n-1 (from the level's dphi ghost faces to the loop's closing
+ * barrier), accumulated since the context started. */
+int amr_solve_relax_level_ms(amr_ctx* ctx, double* ms, int n);
 int amr_get_solve_layout(amr_ctx* ctx, int* layout, int* blocks_per_sm, int* threads, int* blocks, int* count);
 /* Autotuner of the persistent solve: times a solve to L1 tolerance tol from
  * the context's current potential in every layout with 1, 2 and as many
