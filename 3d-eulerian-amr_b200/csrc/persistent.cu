@@ -161,7 +161,6 @@ struct Solver {
     unsigned bar_target = 0;    // thread 0: arrivals that complete the next barrier
     unsigned lsum_gen = 0;      // level sums published so far in this launch
     unsigned pass_seq = 0;      // last pass word used by the shared-memory relaxation loops
-    unsigned arrivals = 0;      // their arrivals released so far in this launch
     unsigned long long spin_limit = BARRIER_SPINS;  // polls per bounded wait
     unsigned long long t_last;  // block 0: global time at the last barrier exit
     // block 0's phase accounting, in shared memory
@@ -425,8 +424,8 @@ struct Solver {
     __device__ unsigned long long* tagged_snap(int p) const { return a.tsnap + (size_t)p * a.snap_half; }
 
     // Publishes the relaxed brick `res` as a pass: its first interior layers
-    // to snapshot buffer `wpar`, its sum to pres[b]; then (untagged) brick
-    // b's pass word is released as `seq`; the level's arrival count is raised.
+    // to snapshot buffer `wpar`, its sum to pres[b] (tagged: both as tagged
+    // entries; untagged: then brick b's pass word is released as `seq`).
     __device__ void resident_publish(int b, const CT* res, const int* c, int wpar, double* pres, double resid,
                                      unsigned seq) {
         constexpr int K = NX * NX * NX / TPB;
@@ -448,11 +447,8 @@ struct Solver {
             for (int r = 0; r < K; r++) relax_layer_put<NX, CT>(sw, threadIdx.x + r * TPB, res[c[r]]);
             if (threadIdx.x == 0) pres[b] = resid;
             __syncthreads();
-            if (threadIdx.x == 0) {
+            if (threadIdx.x == 0)
                 asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(a.rpub + b), "r"(seq) : "memory");
-                asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(&a.bar->relax_arrivals), "r"(1u)
-                             : "memory");
-            }
         }
     }
 
@@ -557,11 +553,13 @@ struct Solver {
         }
     }
 
-    // The server's part of a pass: waits until the level's bricks have all
-    // released `target` arrivals, forms the level sum of `done` and publishes
-    // it as generation lsum_gen.
-    __device__ bool serve_sum(int l, const double* done, unsigned target, unsigned tag) {
-        __shared__ int s_ok;
+    // The server's part of a pass: waits until every brick of the level has
+    // published pass word `tag`, forms the level sum of `done` (that pass's
+    // sums) and publishes it as generation lsum_gen.  The wait is per brick:
+    // pass 1 goes out before the sum of pass 0 is known, so a count of the
+    // level's publications could be complete for pass 0 while a slow
+    // brick's pass 0 is still missing and a fast one's pass 1 is in.
+    __device__ bool serve_sum(int l, const double* done, unsigned tag) {
         if constexpr (TAGGED) {
             // the bricks' tagged sums of this pass: wait on each and take it
             // straight into the shared buffer of the nested sum (or, for a
@@ -597,9 +595,14 @@ struct Solver {
             __syncthreads();
             return true;
         } else {
-            if (threadIdx.x == 0) s_ok = wait_word(&a.bar->relax_arrivals, target);
-            __syncthreads();
-            if (!s_ok) return false;
+            // the bricks' pass words (a brick one pass further has put that
+            // pass's sum in the other buffer, so `done` is intact)
+            const int* sl = level(l);
+            const int n = a.L.cnt[l];
+            int bad = 0;
+            for (int q = threadIdx.x; q < n; q += TPB)
+                if (!wait_word(a.rpub + sl[q], tag)) bad = 1;
+            if (__syncthreads_or(bad)) return false;
             const double r = level_sum(l, done);
             if (threadIdx.x == 0) lsum_publish(a.bar, lsum_gen, r);
             return true;
@@ -649,7 +652,6 @@ struct Solver {
         int c[K];
         CT d1a[K], d1b[K];
         const unsigned seq0 = pass_seq + 1;  // pass word of pass 0
-        const unsigned arr0 = arrivals;
         if (!mine && !server) {
             // a block without a brick has no part in the loop: it goes to
             // the closing barrier (one polled word instead of the loop's
@@ -661,7 +663,6 @@ struct Solver {
             lsum_gen += 1 + k;
             relax_calls += k + 1;
             pass_seq = seq0 + k;
-            arrivals = arr0 + n * (k + 1);
             return true;
         }
         double* pres = a.pres + (size_t)relax_par * a.L.cap;
@@ -718,7 +719,7 @@ struct Solver {
             relax_par ^= 1;
             pres = a.pres + (size_t)relax_par * a.L.cap;
             ++lsum_gen;
-            if (server && !serve_sum(l, done, arr0 + n, seq0)) return false;
+            if (server && !serve_sum(l, done, seq0)) return false;
 #pragma unroll 1
             for (int j = 0; j < NB; j++) {
                 const int b = j ? b1 : b0;
@@ -743,7 +744,7 @@ struct Solver {
             relax_par ^= 1;
             pres = a.pres + (size_t)relax_par * a.L.cap;
             ++lsum_gen;
-            if (server && !serve_sum(l, done, arr0 + n * (k + 1), seq0 + k)) return false;
+            if (server && !serve_sum(l, done, seq0 + k)) return false;
             // this pass of each brick, held until the sum of the last one
             // decides whether it is published
             int ri0 = 0, ri1 = 0;
@@ -808,7 +809,6 @@ struct Solver {
         }
         if (server && threadIdx.x == 0) a.bar->relax_done_k = k;  // the loop's length for the blocks without a brick
         pass_seq = seq0 + k;
-        arrivals = arr0 + n * (k + 1);
         return sync(PH_RELAX, n * (k + 1));
     }
 

@@ -20,9 +20,7 @@ struct GridBarrier {
     unsigned int lsum_gen;
     unsigned int pad1;
     double lsum_val[2];
-    // passes published by the bricks of the shared-memory relaxation loops
-    // (one release add per brick and pass); grows over the launch
-    unsigned int relax_arrivals;
+    unsigned int pad2;
     // the last pass of the latest shared-memory relaxation loop (stored by
     // the block that forms its sums before the loop's closing barrier)
     unsigned int relax_done_k;

@@ -199,3 +199,41 @@ def test_ztwd_configured_size_matches_reference(gpu, table_path, tmp_path):
     fo = a.flow_off()
     np.testing.assert_allclose(fo, g["final_FO"], rtol=1e-10, atol=1e-13 * max(1.0, np.abs(g["final_FO"]).max()))
     a.close()
+
+
+@pytest.mark.gpu
+def test_persistent_forms_bitwise_on_the_headline_tree(gpu, table_path, tmp_path):
+    """The persistent solve on the headline tree (5 levels of 12^3 bricks,
+    309 bricks, 148 on the finest level): two BinaryDriver steps in the FP64
+    form give the plain form's state and potential bit for bit in every
+    block layout and blocks-per-SM cap (one block per SM: the finest level
+    has as many bricks as blocks and the last block holds one; two: the
+    shared-memory loops leave blocks idle), and the mixed form gives the
+    same bits in each of them.  Bricks of a level reach pass 1 at different
+    times here, which the smaller trees of the other tests do not show."""
+    from cases import live_initial_state
+    g = load_golden("ztwd12_L5")
+    levels = int(g["args"][0])
+    d0 = live_initial_state("ztwd12", ["ztwd", levels, 0], str(tmp_path), table_path)
+    init = {"init_level": d0.level, "init_loc": d0.loc, "init_age": d0.age, "extra": g["extra"],
+            "init_U": d0.U[:, :, 3:-3, 3:-3, 3:-3], "nx": g["nx"]}
+
+    def final(prec, pers, layout=None):
+        a = make(gpu, init, table_path, max_bricks=2048, precision=prec, persistent_solve=pers)
+        if layout is not None:
+            a.set_solve_layout(*layout)
+        run(a, 2)
+        out = (interior(a), a.download_poisson()[0])
+        a.close()
+        return out
+
+    U0, phi0 = final(gpu.PREC_FP64, 0)
+    mixed = None
+    for layout in ((0, 1), (0, 2), (1, 1), (2, 2)):
+        U, phi = final(gpu.PREC_FP64, 2, layout)
+        assert np.array_equal(U, U0) and np.array_equal(phi, phi0), layout
+        m = final(gpu.PREC_MIXED, 2, layout)
+        if mixed is None:
+            mixed = m
+        else:
+            assert np.array_equal(m[0], mixed[0]) and np.array_equal(m[1], mixed[1]), layout
