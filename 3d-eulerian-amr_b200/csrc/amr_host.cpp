@@ -420,12 +420,17 @@ int dev_alloc(amr_ctx* c, T** p, size_t count) {
     return AMR_OK;
 }
 
+// The staging buffer of the host copies (gather / scatter of the bricks'
+// arrays), sized on first use for the whole brick pool (its largest user,
+// the state of every slot): a tree that grows later never makes a copy
+// reallocate it, which cost from 5 ms to half a second per call (the free
+// and allocation of a few hundred MB) on the copy after a regrid.
 int ensure_stage(amr_ctx* c, size_t count) {
     if (count <= c->stage_cap) return AMR_OK;
     if (c->d_stage) cudaFree(c->d_stage);
     c->d_stage = nullptr;
-    c->stage_cap = count;
-    return dev_alloc(c, &c->d_stage, count);
+    c->stage_cap = std::max(count, (size_t)c->cap * (size_t)std::max(c->geom.ucount, c->geom.pnx3));
+    return dev_alloc(c, &c->d_stage, c->stage_cap);
 }
 
 int check_slots(amr_ctx* c) {
@@ -438,6 +443,10 @@ int check_slots(amr_ctx* c) {
 }
 
 }  // namespace
+
+namespace amr {
+int stage_reserve(amr_ctx* c, size_t count) { return ensure_stage(c, count); }
+}  // namespace amr
 
 // ===========================================================================
 // C ABI

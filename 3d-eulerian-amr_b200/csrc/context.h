@@ -112,4 +112,6 @@ int zt_check(amr_ctx* c);  // reads and clears the EOS-failure word
 int rebuild_topology(amr_ctx* c);
 int alloc_slot(amr_ctx* c);
 void graph_release(amr_ctx* c);
+// the staging buffer of the host copies holds at least `count` doubles
+int stage_reserve(amr_ctx* c, size_t count);
 }  // namespace amr

@@ -299,11 +299,7 @@ int amr_upload_poisson(amr_ctx* c, const double* P) {
     const int n = nall(c);
     const size_t per = (size_t)n * c->geom.pnx3;
     double* arr[8] = {c->st.phi, c->st.phi0, c->st.dphi, c->st.dphi1, c->st.S, c->st.fx, c->st.fy, c->st.fz};
-    if (c->stage_cap < per) {
-        if (c->d_stage) cudaFree(c->d_stage);
-        c->stage_cap = std::max(per, (size_t)n * c->geom.ucount);
-        CUDA_TRY(cudaMalloc(&c->d_stage, sizeof(double) * c->stage_cap));
-    }
+    TRY(stage_reserve(c, per));
     for (int a = 0; a < 8; a++) {
         CUDA_TRY(cudaMemcpyAsync(c->d_stage, P + a * per, sizeof(double) * per, cudaMemcpyHostToDevice, c->stream));
         launch_scatter(c->d_stage, all(c), n, c->geom.pnx3, arr[a], c->stream);
@@ -318,11 +314,7 @@ int amr_download_poisson(amr_ctx* c, double* P) {
     const int n = nall(c);
     const size_t per = (size_t)n * c->geom.pnx3;
     double* arr[8] = {c->st.phi, c->st.phi0, c->st.dphi, c->st.dphi1, c->st.S, c->st.fx, c->st.fy, c->st.fz};
-    if (c->stage_cap < per) {
-        if (c->d_stage) cudaFree(c->d_stage);
-        c->stage_cap = std::max(per, (size_t)n * c->geom.ucount);
-        CUDA_TRY(cudaMalloc(&c->d_stage, sizeof(double) * c->stage_cap));
-    }
+    TRY(stage_reserve(c, per));
     for (int a = 0; a < 8; a++) {
         launch_gather(arr[a], all(c), n, c->geom.pnx3, c->d_stage, c->stream);
         TRY(check_launch(c));
