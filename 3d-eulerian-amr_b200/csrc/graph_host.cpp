@@ -702,10 +702,30 @@ int amr_autotune_solve(amr_ctx* c, double tol, int max_cycles, int reps, double*
     const int caps[3] = {1, 2, 0};
     const int nt = 3 * nl;
     if (ntrials) *ntrials = nt;
-    const size_t bytes = sizeof(double) * (size_t)c->cap * c->geom.pnx3;
+    // the trials run whole solves, which write the Poisson arrays and, for
+    // the ZTWD state, the potential field and the parents' covered cells of
+    // the state: all of them are saved here and put back after every trial
+    // and at the end, so tuning leaves the run's trajectory unchanged
+    const size_t pbytes = sizeof(double) * (size_t)c->cap * c->geom.pnx3;
+    const size_t ubytes = sizeof(double) * (size_t)c->cap * c->geom.ucount;
+    double* arr[9] = {c->st.phi, c->st.phi0, c->st.dphi, c->st.dphi1, c->st.S, c->st.fx, c->st.fy, c->st.fz, c->st.U};
     double* saved = nullptr;
-    CUDA_TRY(cudaMalloc(&saved, bytes));
-    CUDA_TRY(cudaMemcpyAsync(saved, c->st.phi, bytes, cudaMemcpyDeviceToDevice, c->stream));
+    CUDA_TRY(cudaMalloc(&saved, 8 * pbytes + ubytes));
+    auto copy_all = [&](bool save) {
+        for (int q = 0; q < 9; q++) {
+            double* keep = saved + (size_t)q * (pbytes / sizeof(double));
+            const size_t nb = q < 8 ? pbytes : ubytes;
+            if (cudaMemcpyAsync(save ? keep : arr[q], save ? arr[q] : keep, nb, cudaMemcpyDeviceToDevice,
+                                c->stream) != cudaSuccess)
+                return false;
+        }
+        return true;
+    };
+    if (!copy_all(true)) {
+        cudaFree(saved);
+        c->err = "autotuner: saving the state failed";
+        return AMR_ERR_CUDA;
+    }
     const int l0 = g->layout, p0 = g->per_sm;
     double best_ms = 1e300;
     int best_t = -1;
@@ -722,7 +742,7 @@ int amr_autotune_solve(amr_ctx* c, double tol, int max_cycles, int reps, double*
             rc = amr_set_solve_layout(c, l, cap);
             double sum = 0.0;
             for (int r = 0; r <= reps && rc == AMR_OK; r++) {
-                if (cudaMemcpyAsync(c->st.phi, saved, bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess) {
+                if (!copy_all(false)) {
                     rc = AMR_ERR_CUDA;
                     break;
                 }
@@ -739,8 +759,7 @@ int amr_autotune_solve(amr_ctx* c, double tol, int max_cycles, int reps, double*
         }
         if (ms && t < ms_cap) ms[t] = mean;
     }
-    if (cudaMemcpyAsync(c->st.phi, saved, bytes, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess && rc == AMR_OK)
-        rc = AMR_ERR_CUDA;
+    if (!copy_all(false) && rc == AMR_OK) rc = AMR_ERR_CUDA;
     cudaStreamSynchronize(c->stream);
     cudaFree(saved);
     if (rc != AMR_OK) {

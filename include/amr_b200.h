@@ -343,9 +343,10 @@ int amr_solve_relax_level_ms(amr_ctx* ctx, double* ms, int n);
 int amr_get_solve_layout(amr_ctx* ctx, int* layout, int* blocks_per_sm, int* threads, int* blocks, int* count);
 /* Autotuner of the persistent solve: times a solve to L1 tolerance tol from
  * the context's current potential in every layout with 1, 2 and as many
- * blocks per SM as fit (reps timed solves after an untimed one, the
- * potential restored before each), keeps the fastest and leaves the
- * potential as it was.  ms[t] (t < ms_cap) receives trial t's mean device
+ * blocks per SM as fit (reps timed solves after an untimed one, the state
+ * and the Poisson arrays restored before each: a solve of the ZTWD state
+ * also writes its potential field and restricts it), keeps the fastest and
+ * leaves the state and the Poisson arrays as they were.  ms[t] (t < ms_cap) receives trial t's mean device
  * time (layout t / 3, blocks per SM 1, 2, all for t % 3; -1 where the trial
  * repeats an earlier launch), *ntrials the number of trials, *best the one
  * kept. */

@@ -146,9 +146,10 @@ def test_persistent_wait_limit_times_out_and_context_recovers(gpu):
 @pytest.mark.parametrize("case", ["poisson_poly_L2", "ztwd12_L2"])
 def test_solve_layouts_bitwise_and_autotuner(gpu, table_path, case):
     """Every block layout of the persistent solve kernel (threads per block,
-    cells per thread, blocks per SM) gives the plain form's potential bit for
-    bit; the autotuner times them all on the context's own solve, keeps one
-    and leaves the potential unchanged."""
+    cells per thread, blocks per SM) gives the same potential bit for bit;
+    the autotuner times them all on the context's own solve, keeps one and
+    leaves the state and every Poisson array unchanged (a ZTWD solve also
+    writes the state's potential field and restricts the state)."""
     if case.startswith("ztwd"):
         from test_ztwd_gpu import make as make_ztwd
         g = load_golden(case)
@@ -176,10 +177,12 @@ def test_solve_layouts_bitwise_and_autotuner(gpu, table_path, case):
                 assert (e, n) == ref[:2], (layout, per_sm)
                 assert np.array_equal(phi, ref[2]), (layout, per_sm)
     a.upload_poisson(P0)
+    U0 = a.download_state()
     ms, best = a.autotune_solve(tol, reps=1)
     assert 0 <= best < len(ms) and ms[best] is not None and ms[best] > 0
     assert all(m is None or m >= ms[best] for m in ms)
-    assert np.array_equal(a.download_poisson()[0], P0[0])
+    assert np.array_equal(a.download_poisson(), P0)
+    assert np.array_equal(a.download_state(), U0)
     lay = a.solve_layout()
     assert lay[0] == best // 3
     a.close()
