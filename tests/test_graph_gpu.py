@@ -148,8 +148,10 @@ def test_solve_layouts_bitwise_and_autotuner(gpu, table_path, case):
     """Every block layout of the persistent solve kernel (threads per block,
     cells per thread, blocks per SM) gives the same potential bit for bit;
     the autotuner times them all on the context's own solve, keeps one and
-    leaves the state and every Poisson array unchanged (a ZTWD solve also
-    writes the state's potential field and restricts the state)."""
+    leaves the state and the Poisson arrays unchanged (a ZTWD solve also
+    writes the state's potential field and restricts the state).  The
+    source S is the exception: every call of the graph API recomputes it
+    from the density first, and so does the autotuner's last one."""
     if case.startswith("ztwd"):
         from test_ztwd_gpu import make as make_ztwd
         g = load_golden(case)
@@ -181,7 +183,9 @@ def test_solve_layouts_bitwise_and_autotuner(gpu, table_path, case):
     ms, best = a.autotune_solve(tol, reps=1)
     assert 0 <= best < len(ms) and ms[best] is not None and ms[best] > 0
     assert all(m is None or m >= ms[best] for m in ms)
-    assert np.array_equal(a.download_poisson(), P0)
+    P1 = a.download_poisson()
+    for q in (0, 1, 2, 3, 5, 6, 7):  # phi, phi0, dphi, dphi1, fx, fy, fz
+        assert np.array_equal(P1[q], P0[q]), q
     assert np.array_equal(a.download_state(), U0)
     lay = a.solve_layout()
     assert lay[0] == best // 3
