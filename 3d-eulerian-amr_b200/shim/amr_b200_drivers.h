@@ -151,9 +151,17 @@ class GpuBinaryDriver : public BinaryDriver {
     amr_binary_header hdr_{};
 
 public:
-    explicit GpuBinaryDriver(Binary* r, const char* table = "helmholtz.table") : BinaryDriver(r), root_(r) {
+    // precision / persistent_solve: AMR_PREC_FP64 and 0 (the defaults) step
+    // as the reference does, to round-off; AMR_PREC_MIXED_SOLVE and 1 is the
+    // benchmark's form (FP32 multigrid correction, each solve one
+    // cooperative kernel)
+    explicit GpuBinaryDriver(Binary* r, const char* table = "helmholtz.table", int precision = AMR_PREC_FP64,
+                             int persistent_solve = 0)
+        : BinaryDriver(r), root_(r) {
         amr_config cfg = amr_b200_bind::reference_config(AMR_PHYSICS_ZTWD, STATE_NF);
         cfg.rho_floor = State::rho_floor;
+        cfg.precision = precision;
+        cfg.persistent_solve = persistent_solve;
         if (amr_create(&cfg, &ctx_) != AMR_OK) amr_b200_bind::fail(nullptr, "amr_create");
         if (helm_create(table, &eos_) != 0) amr_b200_bind::fail(ctx_, "helm_create");
         helm_set_cgs_units(eos_, Binary::Ucm, Binary::Ug, Binary::Us, 1.0);  // Binary::set_units
