@@ -110,12 +110,19 @@ int amr_poisson_boundaries_noalloc(amr_ctx* c) {
     // so nothing has to be cleared between calls
     const int* order = c->d_slots + c->off_all[0];
     const int n = (int)c->all_slots.size();
-    const long long t0 = g_launch_tally;
-    launch_set_source(c->geom, c->st, order, n, c->stream);
-    launch_source_sums(c->geom, c->bt, c->st, order, n, c->d_msrc, c->d_allref, c->stream);
-    const int rc = launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, order, phys_walk(c), c->d_msrc,
-                                     c->d_allref, c->d_bphi, scratch, NOALLOC_SCRATCH_DOUBLES, c->stream);
-    c->prof.kernels += g_launch_tally - t0;
+    // the same profile classes as amr_poisson_boundaries (the scopes record
+    // events only and count the launches; no device memory is allocated)
+    {
+        ProfScope ps_(c->prof, KC_SOURCE, c->stream);
+        launch_set_source(c->geom, c->st, order, n, c->stream);
+        launch_source_sums(c->geom, c->bt, c->st, order, n, c->d_msrc, c->d_allref, c->stream);
+    }
+    int rc;
+    {
+        ProfScope ps_(c->prof, KC_PHYS_BOUND, c->stream);
+        rc = launch_phys_bound(c->geom, c->bt, c->d_bfaces, c->n_bfaces, order, phys_walk(c), c->d_msrc,
+                               c->d_allref, c->d_bphi, scratch, NOALLOC_SCRATCH_DOUBLES, c->stream);
+    }
     if (rc) {
         c->err = "static scratch too small for one point";
         return AMR_ERR_RANGE;

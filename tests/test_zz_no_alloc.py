@@ -62,3 +62,36 @@ def test_noalloc_boundaries_match_two_calls(gpu):
         np.testing.assert_allclose(e_var, e_ref, rtol=1e-12)
     ref.close()
     var.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_boundaries_bitwise_on_the_4_level_star(gpu, tmp_path):
+    """The 4-level single star (the reference's configured size; its initial
+    state from a zero-step run of the reference harness): the boundary
+    points and subtree sums are many times those of the 2-level case, so the
+    variant's static scratch is walked in batches of points.  The points are
+    batched, not the sums of one point, so the domain-face potential -- and
+    the V-cycle that carries it into phi -- must equal the ordinary entry
+    point's bit for bit."""
+    from cases import live_initial_state
+    from test_poisson_gpu import load_state, make as make_grav
+    g = load_golden("grav_poly_L4")
+    ic, maxlevel, _, tol = [x for x in g["args"]]
+    d0 = live_initial_state("g05", ["grav", ic, int(maxlevel), 0, float(tol)], str(tmp_path))
+    b = d0.bw
+    init = {"init_level": d0.level, "init_loc": d0.loc, "init_age": d0.age, "init_U": d0.U[:, :, b:-b, b:-b, b:-b]}
+    ref, var = make_grav(gpu, int(maxlevel)), make_grav(gpu, int(maxlevel))
+    for a in (ref, var):
+        load_state(a, init)
+    fn = var.lib.amr_poisson_boundaries_noalloc
+    fn.argtypes = [ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    assert var.lib.amr_poisson_set_source(var.ctx) == 0
+    ref.poisson_boundaries()
+    rc = fn(var.ctx)
+    assert rc == 0, var.lib.amr_last_error(var.ctx)
+    e_ref, e_var = ref.vcycle(), var.vcycle()
+    assert e_ref == e_var
+    assert np.array_equal(ref.download_poisson()[0], var.download_poisson()[0])
+    ref.close()
+    var.close()
