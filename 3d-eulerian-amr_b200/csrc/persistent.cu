@@ -34,7 +34,6 @@ namespace {
 constexpr unsigned long long BARRIER_SPINS = 1ull << 22;
 
 __device__ __forceinline__ int ld_volatile(const int* p) { return *(const volatile int*)p; }
-__device__ __forceinline__ unsigned ld_volatile(const unsigned* p) { return *(const volatile unsigned*)p; }
 
 // Grid-wide barrier of a cooperative launch; false when the solve aborted.
 // The arrival counter only grows: barrier k of the launch completes when it
@@ -171,6 +170,8 @@ struct Solver {
     unsigned* lvl_n;              // relaxation passes per level
     unsigned long long* lvl_ns;   // block 0's time in each level's relaxation loops
     unsigned long long* rsplit;   // block 0: the resident loops' time split [4], passes, sweeps
+    unsigned mbar = 0;            // shared-memory address of the staging mbarrier (bulk copies)
+    unsigned mbar_parity = 0;     // phase parity of its next completion (the same in every thread)
 
     __device__ static unsigned long long now() {
         unsigned long long t;
@@ -544,6 +545,77 @@ struct Solver {
         return r;
     }
 
+    // Waits (every thread) until the staging mbarrier completes its current
+    // phase; false when the wait ran out (the solve is then aborted, and
+    // the wait goes on, again bounded, so that no copy is still landing in
+    // shared memory when the block leaves).
+    __device__ bool wait_staged() {
+        unsigned long long spins = 0;
+        bool ok = true;
+        for (;;) {
+            unsigned done;
+            asm volatile(
+                "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                : "=r"(done)
+                : "r"(mbar), "r"(mbar_parity)
+                : "memory");
+            if (done) break;
+            if (++spins > spin_limit) {
+                if (!ok) break;
+                ok = false;
+                spins = 0;
+                if (threadIdx.x == 0) give_up(a.bar, &a.ctl->status);
+            }
+        }
+        mbar_parity ^= 1;
+        return ok;
+    }
+
+    // Brick b's (NX+2)^3 correction values from dphi into the two sweep
+    // buffers x and y: two bulk copies (the TMA engine, from this GPU's own
+    // memory, no multicast) issued by one thread and completed on the
+    // staging mbarrier, so the other threads load their dphi1 meanwhile.
+    // A brick is one contiguous block of P3 values whose size is a multiple
+    // of 16 bytes; where an address is not 16-byte aligned (never for the
+    // slot pool and the shared buffers, but checked) plain loads stage it.
+    // Returns whether bulk copies were issued (then wait_staged follows).
+    __device__ bool stage_brick(const CT* D, CT* x, CT* y) {
+        constexpr int P3 = (NX + 2) * (NX + 2) * (NX + 2);
+        constexpr unsigned BYTES = P3 * sizeof(CT);
+        static_assert(BYTES % 16 == 0, "bulk copies move multiples of 16 bytes");
+        const bool aligned = ((reinterpret_cast<size_t>(D) | reinterpret_cast<size_t>(x) |
+                               reinterpret_cast<size_t>(y)) & 15) == 0;
+        if (!aligned) {
+            for (int q = threadIdx.x; q < P3; q += TPB) {
+                const CT v = D[q];
+                x[q] = v;
+                y[q] = v;
+            }
+            return false;
+        }
+        // the buffers' last generic uses are over before the copies start
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned xs = (unsigned)__cvta_generic_to_shared(x);
+            const unsigned ys = (unsigned)__cvta_generic_to_shared(y);
+            // order this block's generic accesses (and, through the grid
+            // barrier before, the other blocks' writes of dphi) before the
+            // copies of the async proxy
+            asm volatile("fence.proxy.async;" ::: "memory");
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(2 * BYTES)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(xs),
+                "l"(D), "r"(BYTES), "r"(mbar)
+                : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(ys),
+                "l"(D), "r"(BYTES), "r"(mbar)
+                : "memory");
+        }
+        return true;
+    }
+
     // block 0, thread 0: adds the time since *t to split s and restarts *t
     __device__ void split(int s, unsigned long long& t) {
         if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -670,15 +742,12 @@ struct Solver {
         for (int j = 0; j < NB; j++) {
             const int b = j ? b1 : b0;
             if (b < 0) continue;
-            // pass 0: the ghost faces are in dphi (filled by the face phase)
+            // pass 0: the ghost faces are in dphi (filled by the face phase);
+            // the brick is staged by bulk copies while dphi1 is loaded
             const CT* D = Corr<CT>::dphi(a.st) + (size_t)b * P3;
             CT* x = resident_buf(j, 0);
             CT* y = resident_buf(j, 1);
-            for (int q = threadIdx.x; q < P3; q += TPB) {
-                const CT v = D[q];
-                x[q] = v;
-                y[q] = v;
-            }
+            const bool bulk = stage_brick(D, x, y);
             CT d1[K];
             relax_cells<NX, TPB, CT>(threadIdx.x, Corr<CT>::dphi1(a.st) + (size_t)b * P3, c, d1);
 #pragma unroll
@@ -686,6 +755,7 @@ struct Solver {
                 if (j) d1b[r] = d1[r];
                 else d1a[r] = d1[r];
             }
+            if (bulk && !wait_staged()) return false;
             __syncthreads();
             CT* res;
             const double rs = relax_sweeps_in<NX, TPB, CT>(x, y, &sm[0].red[0][0], threadIdx.x, c, d1, &res,
@@ -925,6 +995,14 @@ __global__ void __launch_bounds__(TPB, SolveLayout<NX, TPB>::MINB) k_solve_persi
     s.lvl_ns = s_lvl_ns;
     __shared__ unsigned long long s_rsplit[6];
     s.rsplit = s_rsplit;
+    // the mbarrier of the bulk brick copies: one arrival (the issuing
+    // thread's, with the bytes it expects) completes a phase
+    __shared__ __align__(8) unsigned long long s_mbar;
+    s.mbar = (unsigned)__cvta_generic_to_shared(&s_mbar);
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(s.mbar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
     if (threadIdx.x < 6) s_rsplit[threadIdx.x] = 0;
     if (threadIdx.x < MAX_LEVELS) {
         s_lvl_n[threadIdx.x] = 0;
