@@ -88,7 +88,7 @@ BYTES_PER_BRICK = {
 # (7.93 GB of algorithmic bytes).  The solve's arrays stay in L2 across its
 # V-cycles, so DRAM sees the cold fill, the per-launch zeroing of the tagged
 # relaxation buffers and the dirty write-back.
-ZT_SOLVE_DRAM_BYTES_PER_LAUNCH = {8: 16.69e6, 12: 218.8e6}
+ZT_SOLVE_DRAM_BYTES_PER_LAUNCH = {8: 16.69e6, 12: 185.0e6}
 
 
 def load_amr():
