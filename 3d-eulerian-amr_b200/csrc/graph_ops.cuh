@@ -166,15 +166,18 @@ __device__ __forceinline__ void tagged_put(unsigned long long* p, float v, unsig
     const unsigned long long w = ((unsigned long long)tag << 32) | __float_as_uint(v);
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(w) : "memory");
 }
+// Only the faces in `faces` (bit f for face f) are written: a layer is read
+// only by the same-level neighbour across that face.
 template <int NX>
-__device__ __forceinline__ void relax_layer_put_tagged(unsigned long long* sw, int t, float v, unsigned tag) {
+__device__ __forceinline__ void relax_layer_put_tagged(unsigned long long* sw, int t, float v, unsigned tag,
+                                                       unsigned faces) {
     const int ci = t % NX + 1, cj = (t / NX) % NX + 1, ck = t / (NX * NX) + 1;
-    if (ci == 1) tagged_put(sw + layer_entry<NX>(0, cj, ck), v, tag);
-    if (ci == NX) tagged_put(sw + layer_entry<NX>(1, cj, ck), v, tag);
-    if (cj == 1) tagged_put(sw + layer_entry<NX>(2, ci, ck), v, tag);
-    if (cj == NX) tagged_put(sw + layer_entry<NX>(3, ci, ck), v, tag);
-    if (ck == 1) tagged_put(sw + layer_entry<NX>(4, ci, cj), v, tag);
-    if (ck == NX) tagged_put(sw + layer_entry<NX>(5, ci, cj), v, tag);
+    if ((faces & 1u) && ci == 1) tagged_put(sw + layer_entry<NX>(0, cj, ck), v, tag);
+    if ((faces & 2u) && ci == NX) tagged_put(sw + layer_entry<NX>(1, cj, ck), v, tag);
+    if ((faces & 4u) && cj == 1) tagged_put(sw + layer_entry<NX>(2, ci, ck), v, tag);
+    if ((faces & 8u) && cj == NX) tagged_put(sw + layer_entry<NX>(3, ci, ck), v, tag);
+    if ((faces & 16u) && ck == 1) tagged_put(sw + layer_entry<NX>(4, ci, cj), v, tag);
+    if ((faces & 32u) && ck == NX) tagged_put(sw + layer_entry<NX>(5, ci, cj), v, tag);
 }
 
 // Writes a relaxed interior value of cell t to dphi and to the snapshot.

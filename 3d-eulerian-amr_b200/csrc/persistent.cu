@@ -432,8 +432,14 @@ struct Solver {
         constexpr int K = NX * NX * NX / TPB;
         if constexpr (TAGGED) {
             unsigned long long* sw = tagged_snap(wpar) + (size_t)b * a.stride;
+            // the layers a same-level neighbour reads (the other faces' ghosts
+            // come from the parent, the mirror or the outflow value)
+            unsigned sib = 0;
 #pragma unroll
-            for (int r = 0; r < K; r++) relax_layer_put_tagged<NX>(sw, threadIdx.x + r * TPB, float(res[c[r]]), seq);
+            for (int f = 0; f < 6; f++) sib |= a.bt.ftype[6 * b + f] == FACE_SIB ? 1u << f : 0u;
+#pragma unroll
+            for (int r = 0; r < K; r++)
+                relax_layer_put_tagged<NX>(sw, threadIdx.x + r * TPB, float(res[c[r]]), seq, sib);
             if (threadIdx.x == 0) {
                 // the FP64 sum as two tagged halves (pres buffer of this pass)
                 const int pp = (int)((pres - a.pres) / a.L.cap);
