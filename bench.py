@@ -91,6 +91,12 @@ BYTES_PER_BRICK = {
 ZT_SOLVE_DRAM_BYTES_PER_LAUNCH = {8: 16.69e6, 12: 185.0e6}
 
 
+# the keys of the roofline object on the bench line (the rest of the solve's
+# breakdown is written to the --json-out sidecar)
+ROOFLINE_LINE_KEYS = ("bound", "kernel", "achieved", "peak", "unit", "frac", "peak_source", "traffic",
+                      "algorithmic_bytes_per_launch", "ms_per_launch", "note", "traffic_note")
+
+
 def load_amr():
     import importlib.util
     spec = importlib.util.spec_from_file_location("amr_b200", os.path.join(PKG, "amr.py"))
@@ -1283,6 +1289,12 @@ def main():
     if rank == 0:
         cpu = ztwd.get("cpu_baseline") if ztwd else None
         traffic = ZT_SOLVE_DRAM_BYTES_PER_LAUNCH.get(nx)
+        # the line keeps the roofline's figures; the solve's per-phase and
+        # per-level splits go to the sidecar
+        roofline = dict(roofline_persistent(head, traffic),
+                        traffic_note=None if traffic is None else
+                        "ncu DRAM read+write per solve launch on this workload (L2-resident arrays: far "
+                        "below the algorithmic bytes)")
         out = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "ms_steps": head["ms_steps"],
@@ -1295,10 +1307,7 @@ def main():
                        "timed_steps": [args.warmup, args.warmup + args.steps - 1],
                        "regrids_in_timed_steps": sum(1 for q in range(args.warmup, args.warmup + args.steps)
                                                      if q % 8 == 0)},
-            "roofline": dict(roofline_persistent(head, traffic),
-                             traffic_note=None if traffic is None else
-                             "ncu DRAM read+write per solve launch on this workload (L2-resident arrays: far "
-                             "below the algorithmic bytes)"),
+            "roofline": {k: v for k, v in roofline.items() if k in ROOFLINE_LINE_KEYS},
             "cpu_baseline": cpu, "e2e": head["e2e"],
             "autotune": {k: head["autotune"].get(k) for k in ("layout", "blocks_per_sm", "threads", "blocks",
                                                             "trials_ms")} if head.get("autotune") else None,
@@ -1309,13 +1318,17 @@ def main():
             out["fp64_persistent"] = {k: ztwd["fp64_persistent"][k] for k in ("value", "ms_per_step")}
             out["mixed_100_steps"] = {k: ztwd["mixed"][k] for k in ("value", "ms_per_step")}
             out["speedup_vs_fp64_plain"] = ztwd["fp64"]["ms_per_step"] / head["ms_per_step"]
-            out["errors_vs_fp64"] = ztwd["errors_mixed_vs_fp64"]
+            # the errors after the 100 steps (their growth after 1 and 10 steps
+            # is in the sidecar's ztwd_binary)
+            out["errors_vs_fp64"] = {k: v for k, v in ztwd["errors_mixed_vs_fp64"].items() if k != "growth"}
+            f32 = ztwd["errors_mixed_flux32_vs_fp64"]
             out["mixed_flux32_100_steps"] = dict({k: ztwd["mixed_flux32"][k] for k in ("value", "ms_per_step")},
-                                                 errors_vs_fp64=ztwd["errors_mixed_flux32_vs_fp64"])
+                                                 phi_rel_l2=f32.get("phi_rel_l2"), rho_rel_l1=f32.get("rho_rel_l1"))
         line = json.dumps(out)
         print(line)
         if args.json_out:
             side = dict(out, ztwd_binary=ztwd, **sections)
+            side["roofline"] = roofline
             with open(args.json_out, "w") as f:
                 f.write(json.dumps(side) + "\n")
     if world > 1:
