@@ -85,3 +85,25 @@ def test_bench_line_keeps_the_contract(tmp_path, monkeypatch, capsys):
     s = json.loads(side.read_text())
     assert s["roofline"]["relax_ms_per_step_by_level"] == [1.0, 2.0, 3.0]
     assert s["ztwd_binary"]["errors_mixed_vs_fp64"]["growth"]
+
+
+def test_reference_arm_line(monkeypatch, capsys):
+    """--impl reference: the line of the reference's own CPU build, on the
+    same metric and workload, with its CPU description and an end-to-end
+    figure that copies nothing; without the harness it says why in one
+    line."""
+    bench = _bench()
+    sample = {"seconds": [25.0, 25.5], "leaf_cells": [467424, 467424], "threads": 16, "bricks": 309}
+    monkeypatch.setattr(bench, "run_reference_ztwd", lambda *a, **k: sample)
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--impl", "reference"])
+    assert bench.main() == 0
+    line = json.loads([x for x in capsys.readouterr().out.splitlines() if x.startswith("{")][-1])
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert abs(line["value"] - 2 * 467424 / 50.5) < 1e-9
+    assert line["cpu_baseline"]["kind"] == "reference" and line["cpu_baseline"]["cores"] == 16
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["value"] == line["value"]
+    assert line["config"]["workload"] == bench.ZT_WORKLOAD % bench.ZT_NX
+    monkeypatch.setattr(bench, "run_reference_ztwd", lambda *a, **k: None)
+    assert bench.main() == 0
+    line = json.loads([x for x in capsys.readouterr().out.splitlines() if x.startswith("{")][-1])
+    assert line["impl"] == "reference" and "unavailable" in line
